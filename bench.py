@@ -1,0 +1,468 @@
+"""Benchmark: fwd+VJP events/s of the batched LOITS sampler on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload uniform|single|ragged|precision]
+
+One step = forward (normalise, CDF, Philox, inverse-CDF search +
+interpolation, stable compaction) + VJP of the whole density batch.  The
+default workload is 64 densities on a 1024-knot uniform grid over [1e-3, 1]
+with 1e6 events each (6.4e7 events per step), seeded synthetic densities
+(sums of 1-3 x^a (1-x)^b components); no dataset is involved.
+
+Arms:
+  --impl b200       (default) the persistent, CUDA-graph-captured form; the
+                    plain one-launch-per-density form is measured beside it.
+  --impl reference  the reference's own openmp core (oracle/_ref, compiled
+                    from the reference sources) on the host cores, on the exact
+                    embedding of the same workload, a bounded sample per step.
+
+Under torchrun each rank (one GPU) samples its own 64 densities of a global
+batch (density_base = rank * 64, same Philox slot stride): weak scaling, no
+collective on the data path; the step time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "fwd+VJP events/s on 1 B200 (batched vs plain), %HBM peak, CDF err vs FP64"
+PEAKS = ROOT / "MEASURED_PEAKS.json"
+TRAFFIC = ROOT / "profiles" / "traffic.json"
+FALLBACK_HBM_GBS = 6650.0
+# algorithmic bytes per event: the forward writes the event (4 B), the VJP
+# reads its cotangent (4 B); per knot the forward reads grid + value (8 B), the
+# VJP reads them again and writes the gradient (12 B)
+FWD_B_PER_EVENT, BWD_B_PER_EVENT = 4, 4
+FWD_B_PER_KNOT, BWD_B_PER_KNOT = 8, 12
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def workload_spec(name: str):
+    from quantom_loits_b200 import workloads
+
+    return workloads.WORKLOADS[name]()
+
+
+def describe(spec) -> dict:
+    g = np.diff(spec.knot_offsets)
+    return {"workload": spec.name, "densities": spec.n_densities,
+            "knots_min": int(g.min()), "knots_max": int(g.max()),
+            "events_per_step": spec.total_events,
+            "x_cut": spec.x_cut is not None}
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        import tempfile
+
+        self.index = index
+        self.proc = None
+        self.out = None
+        self.path = os.path.join(tempfile.gettempdir(), f"loits_bench_clocks_{os.getpid()}.csv")
+
+    def __enter__(self):
+        try:
+            self.out = open(self.path, "w")
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.out:
+            self.out.close()
+
+    def summary(self) -> dict:
+        try:
+            lines = [l.split(",") for l in open(self.path) if l.strip()]
+        except Exception:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        if not lines:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(l[1]) for l in lines if l[1].strip().replace(".", "").isdigit()]
+        mx = [float(l[2]) for l in lines if l[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for l in lines for i in range(4)
+                          if len(l) > 5 + i and "Active" in l[5 + i] and "Not" not in l[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(lines)}
+
+
+def hbm_peak() -> tuple[float, str]:
+    try:
+        return float(json.loads(PEAKS.read_text())["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def cpu_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+# --------------------------------------------------------------- reference
+
+def reference_sample(spec, n_dens: int):
+    """The reference openmp core on the exact embedding of the first n_dens
+    densities (full event counts).  Returns (events, seconds fwd+bwd)."""
+    from oracle import oracle as O
+
+    ref = O.Reference("openmp")
+    ref.set_threads(cpu_cores())
+    koff = spec.knot_offsets[:n_dens + 1]
+    grid = spec.grid[:koff[-1]]
+    values = spec.values[:koff[-1]]
+    counts = spec.event_counts[:n_dens]
+    *arrs, n_events = O.embed_densities(koff, grid, values, counts)
+    t0 = time.perf_counter()
+    st = ref.forward(*arrs, n_events, spec.seed, spec.sequence)
+    g = np.zeros_like(st["events"])
+    g[:, 0] = 1.0
+    ref.backward(g, st, arrs[0], arrs[1], arrs[2], arrs[3], arrs[5])
+    dt = time.perf_counter() - t0
+    return int(counts.sum()), dt
+
+
+def run_reference(args, spec) -> dict:
+    # calibrate on one density, then take a sample of ~args.ref_seconds per step
+    n1, t1 = reference_sample(spec, 1)
+    per_density = max(t1, 1e-6)
+    n_dens = int(max(1, min(spec.n_densities, args.ref_seconds / per_density)))
+    for _ in range(max(args.warmup, 0) if n_dens * per_density < 5 else 1):
+        reference_sample(spec, n_dens)
+    times, evs = [], 0
+    for _ in range(args.steps):
+        ev, dt = reference_sample(spec, n_dens)
+        times.append(dt)
+        evs = ev
+    t = float(np.mean(times))
+    value = evs / t
+    sample = (f"first {n_dens} of {spec.n_densities} densities ({evs} events, "
+              f"{spec.knot_offsets[1] - spec.knot_offsets[0]} knots) per step, exact embedding "
+              f"into the reference tuple; forward + backward wall clock")
+    return {"metric": METRIC, "value": value, "unit": "events/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": describe(spec),
+            "cpu_baseline": {"value": value, "unit": "events/s", "cores": cpu_cores(),
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+# ------------------------------------------------------------------- b200
+
+def run_b200(args, spec, rank, world, dist) -> dict:
+    import torch
+
+    from quantom_loits_b200 import batched as B
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    nmax = int(spec.event_counts.max())
+    cfg = B.make_config(threads=args.threads, blocks_per_item=args.blocks,
+                        density_base=rank * spec.n_densities, slot_stride=nmax)
+    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev)
+    step = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None)
+    step.grid.copy_(torch.from_numpy(spec.grid))
+    step.values.copy_(torch.from_numpy(spec.values))
+    if spec.x_cut is not None:
+        step.x_cut.copy_(torch.from_numpy(spec.x_cut))
+    gen = torch.Generator(device=dev).manual_seed(1000 + rank)
+    step.grad_events.normal_(generator=gen)
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # ---- per-kernel durations (forward and backward launches, eager)
+    for _ in range(max(args.warmup, 3)):
+        step.forward()
+        step.backward()
+    torch.cuda.synchronize(dev)
+    step.check_status()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd_ms, bwd_ms = [], []
+    for _ in range(args.steps):
+        ev[0].record(stream)
+        step.forward()
+        ev[1].record(stream)
+        step.backward()
+        ev[2].record(stream)
+        ev[2].synchronize()
+        fwd_ms.append(ev[0].elapsed_time(ev[1]))
+        bwd_ms.append(ev[1].elapsed_time(ev[2]))
+
+    # ---- batched form: persistent kernels, fwd+bwd captured in one graph
+    step.capture()
+    for _ in range(args.warmup):
+        step.step()
+    barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        barrier()
+        t0.record(stream)
+        for _ in range(args.steps):
+            step.step()
+        t1.record(stream)
+        barrier()
+    step.check_status()
+    ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    events_step = spec.total_events * world
+    value = events_step / (ms * 1e-3)
+    valid = int(step.row_offsets[-1].item())
+
+    # ---- plain form: one launch per density for forward and for backward
+    plain_cfg = B.make_config(threads=args.threads, blocks_per_item=args.blocks, plain=1,
+                              density_base=rank * spec.n_densities, slot_stride=nmax)
+    pplan = B.BatchPlan(spec.knot_offsets, spec.event_counts, plain_cfg, dev)
+    pstep = B.BatchStep(pplan, seed=spec.seed, with_cut=spec.x_cut is not None)
+    pstep.grid.copy_(step.grid); pstep.values.copy_(step.values)
+    if spec.x_cut is not None:
+        pstep.x_cut.copy_(step.x_cut)
+    pstep.grad_events.copy_(step.grad_events)
+    for _ in range(args.warmup):
+        pstep.step()
+    barrier()
+    t0.record(stream)
+    for _ in range(args.steps):
+        pstep.step()
+    t1.record(stream)
+    barrier()
+    pstep.check_status()
+    plain_ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        tt = torch.tensor([plain_ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        plain_ms = float(tt.item())
+    plain_value = events_step / (plain_ms * 1e-3)
+    same = torch.equal(pstep.events[:valid], step.events[:valid])
+    del pstep, pplan
+
+    # ---- end to end through the public autograd API, host buffers
+    e2e = run_e2e(args, spec, dev, rank, world, dist)
+
+    # ---- roofline of the dominant kernel
+    f_ms, b_ms = float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
+    knots = spec.total_knots
+    fwd_bytes = FWD_B_PER_EVENT * spec.total_events + FWD_B_PER_KNOT * knots
+    bwd_bytes = BWD_B_PER_EVENT * spec.total_events + BWD_B_PER_KNOT * knots
+    kname, k_ms, k_bytes = (("batch_forward_kernel", f_ms, fwd_bytes) if f_ms >= b_ms
+                            else ("batch_backward_kernel", b_ms, bwd_bytes))
+    peak, peak_kind = hbm_peak()
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        t = json.loads(TRAFFIC.read_text())
+        entry = t.get(spec.name, {}).get(kname)
+        if entry:
+            traffic = entry["bytes_per_event"] * spec.total_events
+    except Exception:
+        pass
+    cdf_err = cdf_error(plan, step, spec) if rank == 0 else None
+
+    out = {
+        "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic",
+        "config": {**describe(spec), "form": "persistent forward + backward, one CUDA graph",
+                   "parallelism": f"density-sharded x{world} (no collective on the data path)",
+                   "l2": "per step 256 MB of events written and 256 MB of cotangents read, "
+                         "both larger than the 126 MB L2 (no flush)",
+                   "launch": plan.config, "accepted_events_per_step": valid * world},
+        "plain": {"value": plain_value, "ms_per_step": plain_ms,
+                  "form": "one forward + one backward launch per density, no graph",
+                  "batched_over_plain": value / plain_value, "events_identical": bool(same)},
+        "kernels_ms": {"batch_forward_kernel": f_ms, "batch_backward_kernel": b_ms},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": traffic,
+                     "algorithmic_bytes": k_bytes},
+        "step_hbm_frac": (fwd_bytes + bwd_bytes) / (ms * 1e-3) / 1e9 / peak,
+        "cdf_err_vs_fp64": cdf_err,
+        "e2e": e2e,
+        "gpu_launches": 2 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    return out
+
+
+def cdf_error(plan, step, spec):
+    """max |CDF - FP64 oracle CDF| over every knot of the workload."""
+    try:
+        from oracle import oracle as O
+
+        cdf, _ = plan.cdf(step.workspace)
+        _, ocdf, _ = O.Oracle().d_cdf(spec.knot_offsets, spec.grid, spec.values)
+        return float(np.abs(cdf.cpu().numpy() - ocdf).max())
+    except Exception as exc:  # pragma: no cover
+        return f"unavailable: {exc}"
+
+
+def run_e2e(args, spec, dev, rank, world, dist) -> dict:
+    """The user-facing call with host data: pinned host -> device copies of the
+    step's inputs (density values, grid, cotangent), BatchedLOITS.sample +
+    autograd backward, device -> host copies of the events and the gradient."""
+    import torch
+
+    from quantom_loits_b200 import batched as B
+
+    nmax = int(spec.event_counts.max())
+    sampler = B.BatchedLOITS(dev, seed=spec.seed,
+                             config=B.make_config(threads=args.threads,
+                                                  blocks_per_item=args.blocks,
+                                                  density_base=rank * spec.n_densities,
+                                                  slot_stride=nmax))
+    h_vals = torch.from_numpy(spec.values).pin_memory()
+    h_grid = torch.from_numpy(spec.grid).pin_memory()
+    h_cut = None if spec.x_cut is None else torch.from_numpy(spec.x_cut).pin_memory()
+    h_cot = torch.randn(spec.total_events, generator=torch.Generator().manual_seed(5)).pin_memory()
+    h_events = torch.empty(spec.total_events, dtype=torch.float32).pin_memory()
+    h_grad = torch.empty(spec.total_knots, dtype=torch.float32).pin_memory()
+    stream = torch.cuda.current_stream(dev)
+
+    def one():
+        values = h_vals.to(dev, non_blocking=True).requires_grad_(True)
+        grid = h_grid.to(dev, non_blocking=True)
+        cut = None if h_cut is None else h_cut.to(dev, non_blocking=True)
+        cot = h_cot.to(dev, non_blocking=True)
+        batch = B.DensityBatch(grid, values, spec.knot_offsets, spec.event_counts, cut)
+        events, rows = sampler.sample(batch, sequence=0)
+        n = events.shape[0]
+        h_events[:n].copy_(events.detach(), non_blocking=True)
+        events.backward(cot[:n])
+        h_grad.copy_(values.grad, non_blocking=True)
+        return n
+
+    for _ in range(max(2, args.warmup // 2)):
+        one()
+    torch.cuda.synchronize(dev)
+    if dist is not None:
+        dist.barrier()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    steps = max(3, args.steps // 2)
+    t0.record(stream)
+    n = 0
+    for _ in range(steps):
+        n = one()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    ms = t0.elapsed_time(t1) / steps
+    if dist is not None:
+        tt = torch.tensor([ms], device=dev)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms = float(tt.item())
+    h2d = 4 * (spec.total_knots * 2 + spec.total_events + (spec.n_densities if h_cut is not None else 0))
+    d2h = 4 * (n + spec.total_knots)
+    return {"value": spec.total_events * world / (ms * 1e-3), "unit": "events/s",
+            "ms_per_step": ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+            "api": "BatchedLOITS.sample + autograd backward"}
+
+
+def cpu_baseline_leg(args, spec) -> dict:
+    """The reference openmp core on a bounded sample, rank 0 / N=1 only."""
+    try:
+        n1, t1 = reference_sample(spec, 1)
+        n_dens = int(max(1, min(spec.n_densities, args.ref_seconds / max(t1, 1e-6))))
+        ev, dt = reference_sample(spec, n_dens)
+        return {"value": ev / dt, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
+                "sample": f"first {n_dens} of {spec.n_densities} densities ({ev} events), "
+                          "reference openmp core on the exact embedding, fwd + bwd wall clock"}
+    except Exception as exc:
+        return {"value": None, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
+                "sample": f"unavailable: {exc}"}
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--workload", choices=["uniform", "single", "ragged", "precision"],
+                    default="uniform")
+    ap.add_argument("--threads", type=int, default=0)
+    ap.add_argument("--blocks", type=int, default=0)
+    ap.add_argument("--ref-seconds", type=float, default=3.0,
+                    help="CPU seconds per reference step (bounded sample)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args(argv)
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    world, rank, local = dist_env()
+    spec = workload_spec(args.workload)
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        print(json.dumps(run_reference(args, spec)), flush=True)
+        return 0
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch
+        import torch.distributed as tdist
+
+        torch.cuda.set_device(local)
+        tdist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                 device_id=torch.device("cuda", local))
+        dist = tdist
+    try:
+        out = run_b200(args, spec, rank, world, dist)
+        if rank == 0:
+            if world == 1 and not args.no_cpu_baseline:
+                out["cpu_baseline"] = cpu_baseline_leg(args, spec)
+            print(json.dumps(out), flush=True)
+    finally:
+        if dist is not None:
+            dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

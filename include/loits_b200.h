@@ -1,0 +1,193 @@
+/*
+ * loits_b200.h -- C ABI of the B200 LOITS sampler (libloits_b200.so).
+ *
+ * Plain pointers and sizes only.  Every buffer is caller-owned DEVICE memory
+ * unless a comment says "host"; nothing in the library allocates or frees a
+ * caller buffer.  Every launching entry point takes the CUDA stream to launch
+ * on as `void* stream` (a cudaStream_t; NULL = legacy default stream), returns
+ * immediately (asynchronous), and returns a loits_status code for errors it
+ * can see on the host.  Errors seen on the device (a bounded wait that ran
+ * out, an output that would not fit) are written to a device int32 status
+ * word that the caller reads after synchronising.
+ *
+ * Two input modes share the kernels' building blocks:
+ *
+ *  - "tuple": the reference's own 2-D theory tuple (x_bins, xsec_x, q_bins,
+ *    xsec_q, weights, acceptance), fp64, one x curve and one q curve per cell.
+ *    This is the drop-in for the reference's native pybind module
+ *    (cpp/bindings.cpp:24-208, openmp/bindings.cpp); results are those of the
+ *    reference cpp core: same Philox counters, same compaction order, same
+ *    int16 intervals, same epsilon.
+ *  - "batch": B independent 1-D densities of ragged size described by offset
+ *    tables, fp32 storage, per-density event counts and an optional
+ *    per-density cut x > x_cut.  A batch is exactly the reference's x curve
+ *    of a one-cell theory per density (nx = ny = 1), so slot s of density b
+ *    uses Philox counter b * nmax + s on stream 2 * sequence, nmax = max n_b.
+ */
+#ifndef LOITS_B200_H
+#define LOITS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------- status */
+
+enum loits_status {
+  LOITS_OK = 0,
+  LOITS_ERR_INVALID = 1,     /* bad pointer, shape, size or argument */
+  LOITS_ERR_UNSUPPORTED = 2, /* outside the supported range (e.g. K > 32767) */
+  LOITS_ERR_CUDA = 3,        /* a CUDA runtime call failed */
+  LOITS_ERR_TIMEOUT = 4,     /* a bounded device-side wait ran out */
+  LOITS_ERR_CAPACITY = 5,    /* an output buffer or workspace is too small */
+  LOITS_ERR_EPSILON = 6      /* epsilon other than the reference's 1e-5 */
+};
+
+/* Human-readable name of a status code (static string). */
+const char* loits_status_string(int status);
+
+/* Library ABI version (major * 10000 + minor * 100 + patch). */
+int loits_version(void);
+
+/* ------------------------------------------------------------ uniforms */
+
+/* values[p] = uniform of word (p & 3) of Philox4x32-10 block p >> 2 on
+ * (stream, seed), p in [0, count): top 24 bits * 2^-24, in [0, 1).
+ * Replaces cpp/loits_core.cpp:39-53 fill_uniform (rng/philox.hpp:17-61). */
+int loits_fill_uniform(float* values, int64_t count, uint64_t seed, uint64_t stream_id,
+                       void* stream);
+
+/* ------------------------------------------------------ tuple (fp64, 2-D) */
+
+/* {batch, nx, ny, kx, kq}; cells = nx * ny (cpp/bindings.cpp:36-37). */
+typedef struct loits_shape {
+  int64_t batch, nx, ny, kx, kq;
+} loits_shape;
+
+/* Stages allocation + density + cdf of cpp/bindings.cpp:39-77
+ * (allocate_counts cpp/loits_core.cpp:22-37, density_x/q :55-109,
+ * cdf_x/q :111-165).
+ *   weights, acceptance (uint8 0/1): batch * cells, index (b*nx+ix)*ny+iy
+ *   counts:       batch * cells int64, trunc(|w * n_events|)
+ *   cell_offsets: batch * cells + 1 int64, exclusive prefix of counts
+ *   norm_x: (batch, ny, nx), cdf_x like xsec_x; norm_q: (batch, nx, ny),
+ *   cdf_q like xsec_q
+ *   alloc: 2 int64 {nmax, active}; the caller reads it back to size the
+ *   sampling outputs. */
+int loits_tuple_prepare(const loits_shape* shape, const double* x_bins, const double* xsec_x,
+                        const double* q_bins, const double* xsec_q, const double* weights,
+                        const uint8_t* acceptance, int64_t n_events, int64_t* counts,
+                        int64_t* cell_offsets, double* norm_x, double* norm_q, double* cdf_x,
+                        double* cdf_q, int64_t* alloc, void* stream);
+
+/* Bytes of scratch loits_tuple_sample needs for `active` slots. */
+size_t loits_tuple_sample_workspace(int64_t active);
+
+/* Stages random_x/q + interpolation_x/q + stream_compaction of
+ * cpp/bindings.cpp:79-124 fused in one kernel (fill_uniform
+ * cpp/loits_core.cpp:39-53, interpolate_x/q :167-237, compact :239-266):
+ * Philox uniforms are generated in registers for active slots only.
+ *   events: capacity `active` rows of (x, q); packed: padded slot index of
+ *   each kept row; interval_x / interval_q (may be NULL): int16 interval of
+ *   each kept row; valid: 1 int64, the number of kept rows;
+ *   status: 1 int32 device status word (LOITS_OK or a device error). */
+int loits_tuple_sample(const loits_shape* shape, const double* x_bins, const double* q_bins,
+                       const double* cdf_x, const double* cdf_q, const int64_t* cell_offsets,
+                       int64_t nmax, int64_t active, uint64_t seed, uint64_t sequence,
+                       double* events, int64_t* packed, int16_t* interval_x, int16_t* interval_q,
+                       int64_t* valid, int32_t* status, void* workspace, size_t workspace_bytes,
+                       void* stream);
+
+/* Replaces the pybind backward of cpp/bindings.cpp:132-208
+ * (interpolation_vjp_x/q cpp/loits_core.cpp:268-338, cdf_vjp_x/q :340-398,
+ * density_vjp_x/q :400-472).  grad_events: nvalid rows of 2; packed: the
+ * forward's packed rows (ascending); uniforms and intervals are recomputed
+ * from (seed, sequence) instead of being stored.  Writes every entry of
+ * grad_xsec_x / grad_xsec_q (same shapes as xsec_x / xsec_q). */
+int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
+                         const int64_t* packed, int64_t nvalid, int64_t nmax, uint64_t seed,
+                         uint64_t sequence, const double* x_bins, const double* xsec_x,
+                         const double* q_bins, const double* xsec_q, const uint8_t* acceptance,
+                         const double* norm_x, const double* norm_q, const double* cdf_x,
+                         const double* cdf_q, double* grad_xsec_x, double* grad_xsec_q,
+                         void* stream);
+
+/* ------------------------------------------------ batch (fp32, ragged 1-D) */
+
+typedef struct loits_batch_plan loits_batch_plan; /* opaque, host object */
+
+/* Launch geometry of the batched kernels.  Zero fields take defaults. */
+typedef struct loits_batch_config {
+  int32_t threads;         /* threads per CTA of the sampling kernels: 256 or 512 */
+  int32_t blocks_per_item; /* Philox blocks (4 slots each) per thread per tile: 2,4,8,16 */
+  int32_t scan_knots;      /* knots per thread in the CDF scan: 1..16 */
+  int32_t ctas_per_sm;     /* persistent CTAs per SM (0 = as many as fit) */
+  int32_t plain;           /* 1 = one launch per density (no persistent queue) */
+  int64_t density_base;    /* global index of density 0 of this plan (sharding) */
+  int64_t slot_stride;     /* Philox slots per density, >= max n_b (0 = max n_b) */
+} loits_batch_config;
+
+/* Slot s of (plan-local) density b uses Philox counter
+ * (density_base + b) * slot_stride + s.  A batch split into shards, each
+ * planned with its first density's global index as density_base and the
+ * whole batch's max n_b as slot_stride, samples bit-identically to the
+ * unsplit batch. */
+
+/* Build a plan for B densities.  Host arrays: knot_offsets (B+1, knots of
+ * density b are [knot_offsets[b], knot_offsets[b+1]), at least 2 each) and
+ * event_counts (B, >= 0).  cfg may be NULL (defaults).  The plan owns a
+ * small device table (cudaMalloc at creation, cudaFree at destroy). */
+int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_offsets,
+                            const int64_t* event_counts, const loits_batch_config* cfg,
+                            loits_batch_plan** plan);
+void loits_batch_plan_destroy(loits_batch_plan* plan);
+
+/* Sizes of the caller buffers of a plan. */
+int64_t loits_batch_capacity(const loits_batch_plan* plan);      /* sum n_b: events rows */
+int64_t loits_batch_total_knots(const loits_batch_plan* plan);   /* knot_offsets[B] */
+size_t loits_batch_workspace_bytes(const loits_batch_plan* plan); /* state + scratch */
+/* Offset (bytes) of the int32 device status word inside the workspace. */
+size_t loits_batch_status_offset(const loits_batch_plan* plan);
+/* The config the plan resolved (defaults filled in). */
+int loits_batch_plan_config(const loits_batch_plan* plan, loits_batch_config* cfg);
+
+/* Forward: per-density normalisation, trapezoid CDF (compensated fp32 scan,
+ * fp64 carries and normaliser), in-kernel Philox, inverse-CDF search and
+ * interpolation, acceptance and stable compaction in (density, slot) order.
+ *   grid, values: total_knots fp32; x_cut: B fp32 or NULL (no cut);
+ *   events: capacity fp32 rows; row_offsets: B+1 int64, kept rows of
+ *   density b are [row_offsets[b], row_offsets[b+1]);
+ *   intervals: capacity int32 (may be NULL), interval of each kept row.
+ * The workspace keeps the CDF state the backward needs.  Replaces, for a
+ * batch, cpp/bindings.cpp:24-130 on the embedded tuple. */
+int loits_batch_forward(const loits_batch_plan* plan, const float* grid, const float* values,
+                        const float* x_cut, uint64_t seed, uint64_t sequence, float* events,
+                        int64_t* row_offsets, int32_t* intervals, void* workspace, void* stream);
+
+/* Backward: d(sum_r g_r * x_r)/d(values), with the uniforms, intervals and
+ * compaction recomputed from (seed, sequence) and the forward's workspace.
+ *   grad_events: capacity fp32 (first row_offsets[B] used);
+ *   grad_values: total_knots fp32, every entry written. */
+int loits_batch_backward(const loits_batch_plan* plan, const float* grid, const float* values,
+                         const float* x_cut, uint64_t seed, uint64_t sequence,
+                         const float* grad_events, float* grad_values, void* workspace,
+                         void* stream);
+
+/* The forward's CDF of every knot as fp64 (hi + lo), total_knots entries;
+ * norm: B fp64 normalisers (may be NULL). */
+int loits_batch_cdf(const loits_batch_plan* plan, const void* workspace, double* cdf,
+                    double* norm, void* stream);
+
+/* Inverse CDF of density b at n caller uniforms (fp32 in [0,1)), using the
+ * forward's CDF state: x and (optional) interval per uniform, no acceptance. */
+int loits_batch_quantile(const loits_batch_plan* plan, const void* workspace, int64_t density,
+                         const float* u, int64_t n, float* x, int32_t* intervals, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LOITS_B200_H */

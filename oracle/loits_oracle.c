@@ -343,14 +343,21 @@ static int d_accept(double x, const double* x_cut, int64_t b) {
   return x_cut == NULL || x > x_cut[b];
 }
 
+/* Philox slots per density: slot_stride if given (> 0), else max n_b. */
+static int64_t d_stride(int64_t nd, const int64_t* eoff, int64_t slot_stride) {
+  return slot_stride > 0 ? slot_stride : oracle_d_nmax(nd, eoff);
+}
+
 /* Sample every density; rows in (density, slot) order.  row_offsets has nd+1
    entries.  intervals / u_rows / slots (each may be NULL) receive the
-   interval, the uniform and the slot of each kept row.  Returns kept rows. */
+   interval, the uniform and the slot of each kept row.  Slot s of density b
+   draws counter (density_base + b) * stride + s.  Returns kept rows. */
 int64_t oracle_d_sample(int64_t nd, const int64_t* koff, const int64_t* eoff, const double* grid,
                         const double* cdf, const uint8_t* monotone, const double* x_cut,
-                        uint64_t seed, uint64_t sequence, double* events, int64_t* row_offsets,
+                        uint64_t seed, uint64_t sequence, int64_t density_base,
+                        int64_t slot_stride, double* events, int64_t* row_offsets,
                         int32_t* intervals, float* u_rows, int64_t* slots) {
-  const int64_t nmax = oracle_d_nmax(nd, eoff);
+  const int64_t nmax = d_stride(nd, eoff, slot_stride);
   int64_t row = 0;
   for (int64_t b = 0; b < nd; ++b) {
     row_offsets[b] = row;
@@ -358,7 +365,7 @@ int64_t oracle_d_sample(int64_t nd, const int64_t* koff, const int64_t* eoff, co
     const int64_t n = eoff[b + 1] - eoff[b];
     const int mono = monotone ? monotone[b] : is_nondecreasing(cdf + o, k);
     for (int64_t slot = 0; slot < n; ++slot) {
-      const float u32 = slot_uniform(b * nmax + slot, seed, 2 * sequence);
+      const float u32 = slot_uniform((density_base + b) * nmax + slot, seed, 2 * sequence);
       const double u = (double)u32;
       const int64_t j = d_interval(cdf + o, k, u, mono);
       const double x = curve_value(grid + o, cdf + o, j, u);
@@ -390,8 +397,9 @@ void oracle_d_quantile(int64_t b, const int64_t* koff, const double* grid, const
 void oracle_d_backward(int64_t nd, const int64_t* koff, const int64_t* eoff, const double* grid,
                        const double* values, const double* norm, const double* cdf,
                        const uint8_t* monotone, const double* x_cut, uint64_t seed,
-                       uint64_t sequence, const double* grad_events, double* grad_values) {
-  const int64_t nmax = oracle_d_nmax(nd, eoff);
+                       uint64_t sequence, int64_t density_base, int64_t slot_stride,
+                       const double* grad_events, double* grad_values) {
+  const int64_t nmax = d_stride(nd, eoff, slot_stride);
   int64_t kmax = 2;
   for (int64_t b = 0; b < nd; ++b) if (koff[b + 1] - koff[b] > kmax) kmax = koff[b + 1] - koff[b];
   double* gcdf = (double*)malloc((size_t)kmax * sizeof(double));
@@ -403,7 +411,7 @@ void oracle_d_backward(int64_t nd, const int64_t* koff, const int64_t* eoff, con
     const int mono = monotone ? monotone[b] : is_nondecreasing(cdf + o, k);
     memset(gcdf, 0, (size_t)k * sizeof(double));
     for (int64_t slot = 0; slot < n; ++slot) {
-      const double u = (double)slot_uniform(b * nmax + slot, seed, 2 * sequence);
+      const double u = (double)slot_uniform((density_base + b) * nmax + slot, seed, 2 * sequence);
       const int64_t j = d_interval(cdf + o, k, u, mono);
       const double x = curve_value(grid + o, cdf + o, j, u);
       if (!d_accept(x, x_cut, b)) continue;

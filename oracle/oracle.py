@@ -93,12 +93,12 @@ class Oracle:
         lib.oracle_d_nmax.argtypes = [_i64, _lp]
         lib.oracle_d_nmax.restype = _i64
         lib.oracle_d_cdf.argtypes = [_i64, _lp, _dp, _dp, _dp, _dp, _bp]
-        lib.oracle_d_sample.argtypes = [_i64, _lp, _lp, _dp, _dp, _bp, _dp, _u64, _u64, _dp, _lp,
-                                        _ip, _fp, _lp]
+        lib.oracle_d_sample.argtypes = [_i64, _lp, _lp, _dp, _dp, _bp, _dp, _u64, _u64, _i64, _i64,
+                                        _dp, _lp, _ip, _fp, _lp]
         lib.oracle_d_sample.restype = _i64
         lib.oracle_d_quantile.argtypes = [_i64, _lp, _dp, _dp, _dp, _i64, _dp, _ip]
         lib.oracle_d_backward.argtypes = [_i64, _lp, _lp, _dp, _dp, _dp, _dp, _bp, _dp, _u64, _u64,
-                                          _dp, _dp]
+                                          _i64, _i64, _dp, _dp]
         lib.oracle_d_fd.argtypes = [_i64, _i64, _i64, C.c_double, _lp, _lp, _dp, _dp, _dp, _u64,
                                     _u64, _dp, _lp]
         lib.oracle_d_fd.restype = C.c_double
@@ -170,8 +170,11 @@ class Oracle:
                               _ptr(norm, _dp), _ptr(cdf, _dp), _ptr(mono, _bp))
         return norm, cdf, mono
 
-    def d_forward(self, knot_offsets, event_offsets, grid, values, x_cut, seed, sequence):
-        """Returns dict(events, row_offsets, intervals, u, slots, norm, cdf, monotone)."""
+    def d_forward(self, knot_offsets, event_offsets, grid, values, x_cut, seed, sequence,
+                  density_base=0, slot_stride=0):
+        """Returns dict(events, row_offsets, intervals, u, slots, norm, cdf, monotone).
+        Slot s of density b draws counter (density_base + b) * stride + s,
+        stride = slot_stride or max n_b."""
         koff = _i64a(knot_offsets); eoff = _i64a(event_offsets)
         grid = _f64(grid); values = _f64(values)
         nd = len(koff) - 1
@@ -183,13 +186,14 @@ class Oracle:
         xc = None if x_cut is None else _f64(x_cut)
         valid = self.lib.oracle_d_sample(nd, _ptr(koff, _lp), _ptr(eoff, _lp), _ptr(grid, _dp),
                                          _ptr(cdf, _dp), _ptr(mono, _bp), _ptr(xc, _dp), seed,
-                                         sequence, _ptr(events, _dp), _ptr(rows, _lp),
+                                         sequence, int(density_base), int(slot_stride),
+                                         _ptr(events, _dp), _ptr(rows, _lp),
                                          _ptr(ints, _ip), _ptr(u, _fp), _ptr(slots, _lp))
         return dict(events=events[:valid], row_offsets=rows, intervals=ints[:valid], u=u[:valid],
                     slots=slots[:valid], norm=norm, cdf=cdf, monotone=mono)
 
     def d_backward(self, knot_offsets, event_offsets, grid, values, x_cut, seed, sequence,
-                   grad_events, fwd=None):
+                   grad_events, fwd=None, density_base=0, slot_stride=0):
         koff = _i64a(knot_offsets); eoff = _i64a(event_offsets)
         grid = _f64(grid); values = _f64(values)
         nd = len(koff) - 1
@@ -203,7 +207,8 @@ class Oracle:
         self.lib.oracle_d_backward(nd, _ptr(koff, _lp), _ptr(eoff, _lp), _ptr(grid, _dp),
                                    _ptr(values, _dp), _ptr(_f64(norm), _dp), _ptr(_f64(cdf), _dp),
                                    _ptr(np.ascontiguousarray(mono), _bp), _ptr(xc, _dp), seed,
-                                   sequence, _ptr(g, _dp), _ptr(out, _dp))
+                                   sequence, int(density_base), int(slot_stride), _ptr(g, _dp),
+                                   _ptr(out, _dp))
         return out
 
     def d_fd(self, density, knot, h, knot_offsets, event_offsets, grid, values, x_cut, seed,

@@ -1,0 +1,90 @@
+"""Build libloits_b200.so (the CUDA product library) in-tree for sm_100a.
+
+    python -m quantom_loits_b200.build [--force]
+
+Every ``csrc/*.cu`` translation unit is compiled with nvcc for
+``-gencode arch=compute_100a,code=sm_100a`` (in parallel), then linked into
+``quantom_loits_b200/libloits_b200.so`` with the CUDA runtime linked
+statically, so the library does not depend on which libcudart another module
+of the process loaded.  The build is skipped when the library is newer than
+every source and header.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import shutil
+import subprocess
+import sys
+from concurrent.futures import ThreadPoolExecutor
+from pathlib import Path
+
+PKG = Path(__file__).resolve().parent
+ROOT = PKG.parent
+CSRC = PKG / "csrc"
+INCLUDE = ROOT / "include"
+BUILD = ROOT / "_build"
+LIB = PKG / "libloits_b200.so"
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INCLUDE}"]
+# The reference-tuple kernels must round every fp64 product and sum on its
+# own, in source order, like the reference's C++ built without contraction.
+PER_FILE = {"tuple_kernels.cu": ["-fmad=false"]}
+# batch_plan.cu includes batch_kernels.cu (one translation unit).
+SOURCES = ["capi.cu", "tuple_kernels.cu", "batch_plan.cu"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and Path(cand).exists():
+            return cand
+    raise RuntimeError("nvcc not found: the CUDA toolkit is required to build libloits_b200.so")
+
+
+def _stale() -> bool:
+    if not LIB.exists():
+        return True
+    t = LIB.stat().st_mtime
+    deps = list(CSRC.glob("*.cu")) + list(CSRC.glob("*.cuh")) + list(INCLUDE.glob("*.h"))
+    return any(p.stat().st_mtime > t for p in deps) or Path(__file__).stat().st_mtime > t
+
+
+def build(force: bool = False, verbose: bool = False) -> Path:
+    if not force and not _stale():
+        return LIB
+    BUILD.mkdir(exist_ok=True)
+    exe = nvcc()
+
+    def compile_one(src: str) -> Path:
+        obj = BUILD / (Path(src).stem + ".o")
+        cmd = [exe, *ARCH, *COMMON, *PER_FILE.get(src, []), "-c", str(CSRC / src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), flush=True)
+        res = subprocess.run(cmd, capture_output=True, text=True)
+        if res.returncode != 0:
+            raise RuntimeError(f"nvcc failed on {src}:\n{res.stdout}\n{res.stderr}")
+        return obj
+
+    with ThreadPoolExecutor(max_workers=len(SOURCES)) as pool:
+        objs = list(pool.map(compile_one, SOURCES))
+    tmp = LIB.with_suffix(".so.tmp")
+    cmd = [exe, *ARCH, "-shared", "-o", str(tmp), *map(str, objs)]
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")
+    tmp.replace(LIB)
+    return LIB
+
+
+def main(argv=None) -> int:
+    ap = argparse.ArgumentParser(description=__doc__)
+    ap.add_argument("--force", action="store_true")
+    ap.add_argument("-v", "--verbose", action="store_true")
+    args = ap.parse_args(argv)
+    print(build(force=args.force, verbose=args.verbose))
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,880 @@
+// batch_kernels.cu -- batched ragged 1-D LOITS on sm_100a (fp32 storage).
+//
+// One persistent forward kernel and one persistent backward kernel serve a
+// whole batch of densities.  CTAs take work items from an atomic ticket in a
+// fixed order, so every item an item waits on was handed out earlier to a
+// CTA that is already running (no deadlock), and every wait is bounded.
+//
+// Forward items, in ticket order:
+//   1. CDF scan tiles (density, knot range): trapezoid areas of fp32 knots as
+//      double-float pairs (error-free transforms), a compensated fp32 prefix
+//      per thread, fp64 block scan of thread totals, fp64 carries between
+//      tiles of one density (chained look-back).  A density that fits one
+//      tile is finalised in the same item.
+//   2. CDF finalize items for densities spanning several tiles.
+//      Finalising = clamp the prefix to be non-decreasing (unless an area is
+//      negative: then the exact count semantics of cpp/loits_core.cpp:12-18
+//      are used at sampling time), divide by the fp64 normaliser, store the
+//      CDF as (hi, lo) fp32 pairs with the slope of every interval.
+//   3. Sampling tiles (density, run of Philox blocks): in-register Philox
+//      (rng/philox.hpp), exact search of u against the double-float CDF with
+//      fp32 compares, linear interpolation (cpp/loits_core.cpp:193-196),
+//      acceptance (finite, non-zero, x > x_cut), block scan + decoupled
+//      look-back for a stable (density, slot) compaction, coalesced 16-byte
+//      stores through shared memory.
+// Backward items:
+//   1. Chunks (density, run of sampling tiles): recompute uniforms, intervals
+//      and the compaction ranks of the forward, read the cotangents of the
+//      kept rows, scatter the interpolation VJP (cpp/loits_core.cpp:293-300)
+//      into a shared-memory grad-CDF, write it as the chunk's partial.
+//   2. Density finalize: sum the partials in chunk order (fp64,
+//      deterministic), reverse suffix scan (cdf_vjp, :340-368) and the
+//      normaliser VJP (density_vjp, :400-435), fp32 output.
+#include <cmath>
+#include <cstdint>
+
+#include "batch_kernels.cuh"
+#include "lookback.cuh"
+
+namespace loits_dev {
+
+constexpr double kEps = 1e-5;
+constexpr double kNegInf = -__builtin_huge_val();
+
+// Largest b in [lo, hi) with table[b] <= idx (table non-decreasing).
+__device__ __forceinline__ int find_owner(const int32_t* __restrict__ table, int lo, int hi,
+                                          int32_t idx) {
+  while (hi - lo > 1) {
+    const int mid = (lo + hi) >> 1;
+    if (__ldg(&table[mid]) <= idx) lo = mid; else hi = mid;
+  }
+  return lo;
+}
+
+// ------------------------------------------------------------------ search
+
+// (u >= c) for the double-float knot c = (hi, lo), exactly, for fp32 u.
+__device__ __forceinline__ bool ge_knot(float u, float2 c) {
+  return u > c.x || (u == c.x && c.y <= 0.0f);
+}
+
+__device__ __forceinline__ float2 hilo(const float4* rec, int i) {
+  return *reinterpret_cast<const float2*>(&rec[i]);
+}
+
+// Interval of u: (#knots t with u >= c_t) - 1, clamped to [0, G-2].
+// Non-decreasing CDF: the guide bucket k of u (top m bits of its Philox word)
+// bounds the count to [L[k], L[k+1]]; with M >= G buckets the range is
+// usually empty or one knot wide, decided by at most one compare, else
+// finished by binary search.  Otherwise the full count over every knot
+// (cpp/loits_core.cpp:12-18).
+__device__ __forceinline__ int interval_in_range(const float4* __restrict__ rec, int lo, int hi,
+                                                 float u, int G) {
+  if (lo < hi && ge_knot(u, hilo(rec, lo))) {
+    ++lo;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if (ge_knot(u, hilo(rec, mid))) lo = mid + 1; else hi = mid;
+    }
+  }
+  int j = lo - 1;
+  j = j < 0 ? 0 : j;
+  return j > G - 2 ? G - 2 : j;
+}
+
+__device__ __forceinline__ int interval_count_all(const float4* __restrict__ rec, float u, int G) {
+  int cnt = 0;
+  for (int t = 0; t < G; ++t) cnt += ge_knot(u, hilo(rec, t)) ? 1 : 0;
+  int j = cnt - 1;
+  j = j < 0 ? 0 : j;
+  return j > G - 2 ? G - 2 : j;
+}
+
+// Inverse CDF on interval j: g_j + m_j * ((u - c_hi) - c_lo), fp32.
+__device__ __forceinline__ float interval_value(float4 r, float u, float& t) {
+  t = __fsub_rn(__fsub_rn(u, r.x), r.y);
+  return __fmaf_rn(r.w, t, r.z);
+}
+
+__device__ __forceinline__ bool accept_event(float x, float cut) {
+  // reference predicate (finite, x * q != 0 with q finite non-zero) + cut
+  return isfinite(x) && x != 0.0f && x > cut;
+}
+
+// ------------------------------------------------------------- CDF phase
+
+struct CdfShared {
+  double dscan[33];
+  double dmax[33];
+  double cfirst[512];
+  double tile_excl, norm, mprev, cnext;
+  int nonmono, has_next;
+};
+
+// Double-float prefix step for knot t of density (g, f): adds the area of
+// interval [t-1, t] (t >= 1).  Returns false if that area is negative/NaN.
+__device__ __forceinline__ bool add_area(const float* __restrict__ g, const float* __restrict__ f,
+                                         int64_t t, float& ph, float& pl) {
+  if (t < 1) return true;
+  float ah, al;
+  trapezoid_df(__ldg(&g[t - 1]), __ldg(&g[t]), __ldg(&f[t - 1]), __ldg(&f[t]), ah, al);
+  df_add(ph, pl, ah, al);
+  return ah >= 0.0f;
+}
+
+// Pass 1 over this thread's knots [my_lo, my_hi): local total and max prefix.
+__device__ __forceinline__ void cdf_pass1(const float* g, const float* f, int64_t my_lo,
+                                          int64_t my_hi, double& total, double& maxp, bool& neg) {
+  float ph = 0.0f, pl = 0.0f;
+  maxp = kNegInf;
+  neg = false;
+  for (int64_t t = my_lo; t < my_hi; ++t) {
+    neg |= !add_area(g, f, t, ph, pl);
+    const double p = static_cast<double>(ph) + static_cast<double>(pl);
+    maxp = p > maxp ? p : maxp;
+  }
+  total = static_cast<double>(ph) + static_cast<double>(pl);
+}
+
+// First guide bucket k with k / M >= key (0 .. M + 1).
+__device__ __forceinline__ int32_t bucket_start(float key, int m) {
+  const float scaled = ldexpf(key, m);  // exact: M is a power of two
+  if (!(scaled > 0.0f)) return 0;
+  const int32_t M = 1 << m;
+  if (scaled > static_cast<float>(M)) return M + 1;
+  return static_cast<int32_t>(ceilf(scaled));
+}
+
+// Write the per-knot records of knot t given c_t and (if has_next) c_{t+1},
+// and the guide buckets whose knot count becomes t + 1 at this knot.
+// gd (guide of the density, nullptr when the CDF is not non-decreasing).
+__device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, int64_t t, double c,
+                                            bool has_next, double c_next, uint16_t* gd, int m) {
+  const float2 h = split_df(c);
+  const float gt = __ldg(&a.grid[k0 + t]);
+  float m_slope = 0.0f, inv = 0.0f;
+  float2 hn = make_float2(0.0f, 0.0f);
+  if (has_next) {
+    hn = split_df(c_next);
+    const double C = static_cast<double>(h.x) + static_cast<double>(h.y);
+    const double Cn = static_cast<double>(hn.x) + static_cast<double>(hn.y);
+    const double inv_d = 1.0 / (Cn - C + kEps);
+    const double md = (static_cast<double>(__ldg(&a.grid[k0 + t + 1])) - static_cast<double>(gt)) * inv_d;
+    m_slope = __double2float_rn(md);
+    inv = __double2float_rn(inv_d);
+  }
+  a.rec[k0 + t] = make_float4(h.x, h.y, gt, m_slope);
+  a.invd[k0 + t] = inv;
+  if (gd) {
+    const int32_t M = 1 << m;
+    const int32_t k_lo = bucket_start(knot_key(h), m);
+    const int32_t k_hi = has_next ? bucket_start(knot_key(hn), m) : M + 1;
+    for (int32_t k = k_lo; k < k_hi; ++k) gd[k] = static_cast<uint16_t>(t + 1);
+    if (t == 0)
+      for (int32_t k = 0; k < k_lo; ++k) gd[k] = 0;
+  }
+}
+
+// Pack density b's guide for sampling: gpk[k] = L[k] | L[k+1] << 16.  Every
+// L entry was written (and fenced) before this runs.
+template <int TPB>
+__device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
+  const int M = 1 << __ldg(&a.gbits[b]);
+  const int64_t o = __ldg(&a.goff[b]);
+  const uint16_t* L = a.gl + o;
+  uint32_t* P = a.gpk + o;
+  for (int k = threadIdx.x; k < M; k += TPB)
+    P[k] = static_cast<uint32_t>(__ldcg(&L[k])) | (static_cast<uint32_t>(__ldcg(&L[k + 1])) << 16);
+  __threadfence();
+}
+
+// Pass 2: recompute the prefix, clamp, normalise, emit records for this
+// thread's knots [my_lo, my_hi) of the tile ending at knot `hi`.
+// base = tile_excl + thread exclusive sum; run0 = max of the prefix before
+// this thread (the clamp); tile_next_c is c at knot `hi` when hi < G;
+// gd / m: the density's guide table (nullptr for count semantics).
+template <int TPB>
+__device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_t G, int64_t hi, int64_t my_lo,
+                          int64_t my_hi, double base, double run0, double norm, bool nonmono,
+                          double tile_next_c, uint16_t* gd, int m, CdfShared& sh) {
+  const float* g = a.grid + k0;
+  const float* f = a.values + k0;
+  // first knot of each thread goes to shared memory for its left neighbour
+  double c_first = 0.0;
+  if (my_lo < my_hi) {
+    float ph = 0.0f, pl = 0.0f;
+    add_area(g, f, my_lo, ph, pl);
+    double s = base + (static_cast<double>(ph) + static_cast<double>(pl));
+    if (!nonmono) s = s > run0 ? s : run0;
+    c_first = s / norm;
+  }
+  sh.cfirst[threadIdx.x] = c_first;
+  __syncthreads();
+  if (my_lo < my_hi) {
+    float ph = 0.0f, pl = 0.0f;
+    double run = run0, c_prev = 0.0;
+    for (int64_t t = my_lo; t < my_hi; ++t) {
+      add_area(g, f, t, ph, pl);
+      double s = base + (static_cast<double>(ph) + static_cast<double>(pl));
+      if (!nonmono) {
+        run = s > run ? s : run;
+        s = run;
+      }
+      const double c = s / norm;
+      if (t > my_lo) emit_record(a, k0, t - 1, c_prev, true, c, gd, m);
+      c_prev = c;
+    }
+    // last knot of this thread: end of density, next thread, or next tile
+    const int64_t t = my_hi - 1;
+    if (t == G - 1) emit_record(a, k0, t, c_prev, false, 0.0, gd, m);
+    else if (t + 1 < hi) emit_record(a, k0, t, c_prev, true, sh.cfirst[threadIdx.x + 1], gd, m);
+    else emit_record(a, k0, t, c_prev, true, tile_next_c, gd, m);
+  }
+  // every thread publishes its records before thread 0 signals readiness
+  __threadfence();
+  __syncthreads();
+}
+
+// Chained look-back over the CDF tiles of one density (thread 0 only):
+// returns the fp64 sum of all earlier tiles and publishes this tile's
+// inclusive sum.
+__device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first, int32_t ct, double agg) {
+  double excl = 0.0;
+  if (ct > first) {
+    __stcg(&a.cagg[ct], agg);
+    __threadfence();
+    atomicExch(&a.cflag[ct], 1u);
+    int32_t i = ct - 1;
+    uint32_t polls = 0;
+    while (i >= first) {
+      const uint32_t fl = ld_acquire_u32(&a.cflag[i]);
+      if (fl == 0) {
+        if (++polls >= kSpinLimit) {
+          raise_status(a.status, LOITS_ERR_TIMEOUT);
+          break;
+        }
+        spin_pause(polls);
+        continue;
+      }
+      if (fl == 2) {
+        excl += __ldcg(&a.cinc[i]);
+        break;
+      }
+      excl += __ldcg(&a.cagg[i]);
+      --i;
+    }
+  }
+  __stcg(&a.cinc[ct], excl + agg);
+  __threadfence();
+  atomicExch(&a.cflag[ct], 2u);
+  return excl;
+}
+
+template <int TPB>
+__device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared& sh) {
+  const int b = find_owner(a.cdf_first, a.d_lo, a.d_hi, ct);
+  const int32_t first = __ldg(&a.cdf_first[b]);
+  const int32_t ci = ct - first, nci = __ldg(&a.cdf_first[b + 1]) - first;
+  const int64_t k0 = __ldg(&a.knot_off[b]);
+  const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
+  const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
+  const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
+  const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * a.scan_knots;
+  const int64_t my_lo = my_lo_raw < hi ? my_lo_raw : hi;
+  const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
+  double tot, maxp;
+  bool neg;
+  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg);
+  double tile_tot;
+  const double excl = block_exclusive_sum<double, TPB>(tot, tile_tot, sh.dscan);
+  const double thr_max = my_lo < my_hi ? excl + maxp : kNegInf;
+  double tile_max;
+  const double run0 = block_exclusive_max<double, TPB>(thr_max, kNegInf, tile_max, sh.dmax);
+  const bool any_neg = __syncthreads_or(neg ? 1 : 0) != 0;
+  if (nci == 1) {
+    // whole density in one tile: finalise now
+    uint16_t* gd = any_neg ? nullptr : a.gl + __ldg(&a.goff[b]);
+    cdf_pass2<TPB>(a, k0, G, hi, my_lo, my_hi, excl, run0, tile_tot, any_neg, 0.0, gd,
+                   __ldg(&a.gbits[b]), sh);
+    if (!any_neg) pack_guide<TPB>(a, b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      a.norm[b] = tile_tot;
+      a.dflags[b] = any_neg ? kNonMonotone : 0u;
+      __threadfence();
+      atomicAdd(&a.cdf_ready[b], 1u);
+    }
+    return;
+  }
+  (void)tile_max;
+  (void)run0;
+  if (threadIdx.x == 0) {
+    if (any_neg) atomicOr(&a.dflags[b], kNonMonotone);
+    sh.tile_excl = cdf_lookback(a, first, ct, tile_tot);
+  }
+  __syncthreads();
+  // largest unnormalised prefix of this tile, formed exactly as pass 2 forms
+  // each prefix ((tile_excl + thread_excl) + local), for the clamp of later tiles
+  const double tile_excl = sh.tile_excl;
+  const double my_max = my_lo < my_hi ? (tile_excl + excl) + maxp : kNegInf;
+  double tmax;
+  block_exclusive_max<double, TPB>(my_max, kNegInf, tmax, sh.dmax);
+  if (threadIdx.x == 0) {
+    __stcg(&a.cmax[ct], tmax);
+    if (ci == nci - 1) __stcg(&a.norm[b], tile_excl + tile_tot);
+    __threadfence();
+    atomicAdd(&a.cdf_scanned[b], 1u);
+  }
+  __syncthreads();
+}
+
+template <int TPB>
+__device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi, CdfShared& sh) {
+  const int b = find_owner(a.fin_first, a.d_lo, a.d_hi, fi);
+  const int32_t ci = fi - __ldg(&a.fin_first[b]);
+  const int32_t first = __ldg(&a.cdf_first[b]);
+  const int32_t nci = __ldg(&a.cdf_first[b + 1]) - first;
+  const int32_t ct = first + ci;
+  const int64_t k0 = __ldg(&a.knot_off[b]);
+  const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
+  const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
+  const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
+  if (threadIdx.x == 0) {
+    if (!wait_counter(&a.cdf_scanned[b], static_cast<uint32_t>(nci)))
+      raise_status(a.status, LOITS_ERR_TIMEOUT);
+    sh.norm = __ldcg(&a.norm[b]);
+    sh.nonmono = (ld_acquire_u32(&a.dflags[b]) & kNonMonotone) ? 1 : 0;
+    sh.tile_excl = ci == 0 ? 0.0 : __ldcg(&a.cinc[ct - 1]);
+    double mp = kNegInf;
+    for (int32_t i = first; i < ct; ++i) {
+      const double v = __ldcg(&a.cmax[i]);
+      mp = v > mp ? v : mp;
+    }
+    sh.mprev = mp;
+    sh.has_next = hi < G ? 1 : 0;
+    if (hi < G) {
+      // first knot of the next tile, exactly as that tile's own pass 2 forms it
+      float ph = 0.0f, pl = 0.0f;
+      add_area(a.grid + k0, a.values + k0, hi, ph, pl);
+      double s = (__ldcg(&a.cinc[ct]) + 0.0) + (static_cast<double>(ph) + static_cast<double>(pl));
+      if (!sh.nonmono) {
+        const double m_own = __ldcg(&a.cmax[ct]);
+        const double m = mp > m_own ? mp : m_own;
+        s = s > m ? s : m;
+      }
+      sh.cnext = s / sh.norm;
+    }
+  }
+  __syncthreads();
+  const double norm = sh.norm, tile_excl = sh.tile_excl, mprev = sh.mprev, cnext = sh.cnext;
+  const bool nonmono = sh.nonmono != 0, has_next = sh.has_next != 0;
+  const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * a.scan_knots;
+  const int64_t my_lo = my_lo_raw < hi ? my_lo_raw : hi;
+  const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
+  double tot, maxp;
+  bool neg;
+  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg);
+  double tile_tot;
+  const double excl = block_exclusive_sum<double, TPB>(tot, tile_tot, sh.dscan);
+  const double thr_max = my_lo < my_hi ? (tile_excl + excl) + maxp : kNegInf;
+  double tile_max;
+  double run0 = block_exclusive_max<double, TPB>(thr_max, kNegInf, tile_max, sh.dmax);
+  run0 = run0 > mprev ? run0 : mprev;
+  (void)has_next;
+  uint16_t* gd = nonmono ? nullptr : a.gl + __ldg(&a.goff[b]);
+  cdf_pass2<TPB>(a, k0, G, hi, my_lo, my_hi, tile_excl + excl, run0, norm, nonmono, cnext, gd,
+                 __ldg(&a.gbits[b]), sh);
+  // the last finalize item of the density packs its guide and publishes it
+  if (threadIdx.x == 0) sh.has_next = atomicAdd(&a.fin_done[b], 1u) == static_cast<uint32_t>(nci - 1);
+  __syncthreads();
+  if (sh.has_next) {
+    __threadfence();
+    if (!nonmono) pack_guide<TPB>(a, b);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      a.dflags[b] = nonmono ? kNonMonotone : 0u;
+      __threadfence();
+      atomicAdd(&a.cdf_ready[b], 1u);
+    }
+  }
+  __syncthreads();
+}
+
+// --------------------------------------------------------- sampling phase
+
+// Geometry of sampling tile t of density b: Philox blocks
+// [blk0, blk0 + TPB*R) clipped to the density's slots [P0, P0 + n).
+struct TileGeom {
+  int b;
+  int64_t k0, G, n, P0, blk0;
+};
+
+template <int TPB, int R>
+__device__ __forceinline__ TileGeom tile_geom(const BatchArgs& a, int32_t t) {
+  TileGeom tg;
+  tg.b = find_owner(a.tile_first, a.d_lo, a.d_hi, t);
+  const int32_t si = t - __ldg(&a.tile_first[tg.b]);
+  tg.k0 = __ldg(&a.knot_off[tg.b]);
+  tg.G = __ldg(&a.knot_off[tg.b + 1]) - tg.k0;
+  tg.n = __ldg(&a.n_events[tg.b]);
+  tg.P0 = (a.dbase + tg.b) * a.nmax;
+  tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(si) * TPB * R;
+  return tg;
+}
+
+// A density's sampling state as held in shared memory.
+struct DensView {
+  const float4* rec;
+  const uint32_t* guide;  // packed (L[k], L[k+1]) per bucket
+  int shift;              // 32 - m: bucket of a Philox word = word >> shift
+  int G;
+  bool count_all;
+  float cut;
+};
+
+struct SampleShared {
+  int warp_cnt[16];
+  int64_t base;
+  int nonmono;
+  float cut;
+};
+
+// Wait until density b's CDF is final, then load its records, packed guide
+// and (backward) weights into shared memory.
+__device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
+                                                 float4* rec_s, uint32_t* guide_s, float* invd_s,
+                                                 bool wait_ready, SampleShared& sh) {
+  if (threadIdx.x == 0) {
+    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u)) raise_status(a.status, LOITS_ERR_TIMEOUT);
+    sh.nonmono = (ld_acquire_u32(&a.dflags[b]) & kNonMonotone) ? 1 : 0;
+    sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
+  }
+  __syncthreads();
+  const int m = __ldg(&a.gbits[b]);
+  for (int64_t i = threadIdx.x; i < G; i += blockDim.x) {
+    rec_s[i] = __ldcg(&a.rec[k0 + i]);
+    if (invd_s) invd_s[i] = __ldcg(&a.invd[k0 + i]);
+  }
+  if (!sh.nonmono) {
+    const uint4* src = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.goff[b]));
+    uint4* dst = reinterpret_cast<uint4*>(guide_s);
+    for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&src[i]);
+  }
+  __syncthreads();
+  DensView v;
+  v.rec = rec_s;
+  v.guide = guide_s;
+  v.shift = 32 - m;
+  v.G = static_cast<int>(G);
+  v.count_all = sh.nonmono != 0;
+  v.cut = sh.cut;
+  return v;
+}
+
+// One slot: uniform from its Philox word, interval, value, acceptance.
+struct Slot {
+  float x, t, m;
+  int j;
+  bool ok;
+};
+
+__device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
+  const float u = uniform_from_bits(bits);
+  int j;
+  if (!d.count_all) {
+    const uint32_t pk = d.guide[bits >> d.shift];
+    j = interval_in_range(d.rec, static_cast<int>(pk & 0xffffu), static_cast<int>(pk >> 16), u, d.G);
+  } else {
+    j = interval_count_all(d.rec, u, d.G);
+  }
+  const float4 r = d.rec[j];
+  Slot o;
+  o.x = interval_value(r, u, o.t);
+  o.m = r.w;
+  o.j = j;
+  o.ok = accept_event(o.x, d.cut);
+  return o;
+}
+
+// Warp-granular work layout of a sampling tile: warp w of the CTA owns
+// Philox blocks blk0 + (w*R + r)*32 + lane for rounds r = 0..R-1, i.e. the
+// 128 consecutive slots of each round, rounds in order.  A warp therefore
+// ranks its kept events with one warp scan per round, and the kept events of
+// a tile are the concatenation of its warps' kept events in warp order.
+
+// Bit mask of the 4 slots of Philox block blk inside the density's slot
+// range [P0, P0 + n) (0 when the block lies past the range).
+__device__ __forceinline__ uint32_t block_range_mask(const TileGeom& tg, int64_t blk) {
+  const int64_t s0 = (blk << 2) - tg.P0;  // density slot of word 0
+  if (s0 >= 0 && s0 + 4 <= tg.n) return 0xfu;
+  const int64_t lo = s0 < 0 ? -s0 : 0;
+  const int64_t hi = tg.n - s0 < 4 ? tg.n - s0 : 4;
+  if (hi <= lo) return 0u;
+  return ((1u << static_cast<int>(hi)) - 1u) & ~((1u << static_cast<int>(lo)) - 1u);
+}
+
+// Exclusive warp prefix of per-lane counts (ints: exact); *total = warp sum.
+__device__ __forceinline__ int warp_exclusive_count(int c, int& total) {
+  const int inc = warp_inclusive_sum(c);
+  total = __shfl_sync(0xffffffffu, inc, 31);
+  return inc - c;
+}
+
+// Copy n floats src[0..n) (shared) to dst[0..n) (global), 16-byte stores where
+// dst is aligned.  One warp.
+__device__ __forceinline__ void warp_store(const float* __restrict__ src, float* __restrict__ dst,
+                                           int n) {
+  const int lane = threadIdx.x & 31;
+  const int head = static_cast<int>((4 - ((reinterpret_cast<uintptr_t>(dst) >> 2) & 3)) & 3);
+  const int h = head < n ? head : n;
+  if (lane < h) dst[lane] = src[lane];
+  const int nv = (n - h) >> 2;
+  float4* dv = reinterpret_cast<float4*>(dst + h);
+  for (int v = lane; v < nv; v += 32) {
+    const int s0 = h + 4 * v;
+    __stcs(&dv[v], make_float4(src[s0], src[s0 + 1], src[s0 + 2], src[s0 + 3]));
+  }
+  const int tail0 = h + 4 * nv;
+  if (tail0 + lane < n) dst[tail0 + lane] = src[tail0 + lane];
+}
+
+// Optional per-row interval output (diagnostics): recomputed for kept rows.
+template <int TPB, int R>
+__device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGeom& tg,
+                                                const DensView& d, int64_t row0) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t row = row0;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    const uint32_t range = block_range_mask(tg, blk);
+    int js[4] = {0, 0, 0, 0};
+    uint32_t keep = 0;
+    if (range) {
+      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+      const Slot e0 = sample_slot(d, w.x), e1 = sample_slot(d, w.y);
+      const Slot e2 = sample_slot(d, w.z), e3 = sample_slot(d, w.w);
+      keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+      js[0] = e0.j; js[1] = e1.j; js[2] = e2.j; js[3] = e3.j;
+    }
+    int total;
+    const int excl = warp_exclusive_count(__popc(keep), total);
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+      if (keep & (1u << i)) a.intervals[row + excl + k++] = js[i];
+    row += total;
+  }
+}
+
+template <int TPB, int R>
+__device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
+                                            uint32_t* guide_s, float* stage, SampleShared& sh) {
+  constexpr int W = TPB / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const TileGeom tg = tile_geom<TPB, R>(a, t);
+  const DensView d = load_density(a, tg.b, tg.k0, tg.G, rec_s, guide_s, nullptr, true, sh);
+  float* sw = stage + warp * (R * 128);
+  int acc = 0;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    const uint32_t range = block_range_mask(tg, blk);
+    float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
+    uint32_t keep = 0;
+    if (range) {
+      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+      const Slot e0 = sample_slot(d, w.x), e1 = sample_slot(d, w.y);
+      const Slot e2 = sample_slot(d, w.z), e3 = sample_slot(d, w.w);
+      keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+      x0 = e0.x; x1 = e1.x; x2 = e2.x; x3 = e3.x;
+    }
+    int total;
+    int pos = acc + warp_exclusive_count(__popc(keep), total);
+    if (keep & 1u) sw[pos++] = x0;
+    if (keep & 2u) sw[pos++] = x1;
+    if (keep & 4u) sw[pos++] = x2;
+    if (keep & 8u) sw[pos] = x3;
+    acc += total;
+  }
+  if (lane == 0) sh.warp_cnt[warp] = acc;
+  __syncthreads();
+  int tile_cnt = 0, warp_excl = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const int c = sh.warp_cnt[w];
+    warp_excl += w < warp ? c : 0;
+    tile_cnt += c;
+  }
+  if (lane == 0) a.warp_off[static_cast<int64_t>(t) * W + warp] = warp_excl;
+  if (warp == 0) {
+    const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(tile_cnt), a.status);
+    if (lane == 0) {
+      sh.base = base;
+      a.tile_prefix[t] = base;
+      if (t == __ldg(&a.tile_first[tg.b])) {
+        for (int dd = __ldg(&a.rowfill_lo[tg.b]); dd <= tg.b; ++dd) a.row_offsets[dd] = base;
+      }
+      if (t == a.tiles_total - 1) {
+        for (int dd = a.last_nonempty + 1; dd <= a.nd; ++dd) a.row_offsets[dd] = base + tile_cnt;
+      }
+    }
+  }
+  __syncthreads();
+  const int64_t row0 = sh.base + warp_excl;
+  warp_store(sw, a.events + row0, acc);
+  if (a.intervals) write_intervals<TPB, R>(a, tg, d, row0);
+}
+
+// --------------------------------------------------------- backward phase
+
+// Scatter of one kept slot's cotangent into the chunk's grad-CDF:
+// d x / d c_j = m (w - 1), d x / d c_{j+1} = -m w, w = (u - c_j) / d_j
+// (cpp/loits_core.cpp:293-300).
+__device__ __forceinline__ void scatter_slot(const Slot& e, float g, const float* invd_s,
+                                             float* gacc_s) {
+  const float w = e.t * invd_s[e.j];
+  const float mg = e.m * g;
+  atomicAdd(&gacc_s[e.j], mg * (w - 1.0f));
+  atomicAdd(&gacc_s[e.j + 1], -(mg * w));
+}
+
+// Chunk (density, run of sampling tiles).  Every warp replays its own slots
+// of each tile; the forward recorded where its kept rows start
+// (tile_prefix + warp_off), so no scan across warps and no barrier is needed
+// until the chunk's grad-CDF is flushed.
+template <int TPB, int R>
+__device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
+                                               uint32_t* guide_s, float* invd_s, float* gacc_s,
+                                               SampleShared& sh) {
+  constexpr int W = TPB / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int b = find_owner(a.chunk_first, a.d_lo, a.d_hi, k);
+  const int32_t ki = k - __ldg(&a.chunk_first[b]);
+  const int32_t tb = __ldg(&a.tile_first[b]);
+  const int32_t t_first = tb + ki * a.tiles_per_chunk;
+  const int32_t t_end0 = t_first + a.tiles_per_chunk;
+  const int32_t t_end = t_end0 < __ldg(&a.tile_first[b + 1]) ? t_end0 : __ldg(&a.tile_first[b + 1]);
+  TileGeom tg = tile_geom<TPB, R>(a, t_first);
+  const int G = static_cast<int>(tg.G);
+  for (int i = threadIdx.x; i < G; i += TPB) gacc_s[i] = 0.0f;
+  const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
+#pragma unroll 1
+  for (int32_t t = t_first; t < t_end; ++t) {
+    tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
+    int64_t row = __ldcg(&a.tile_prefix[t]) + __ldcg(&a.warp_off[static_cast<int64_t>(t) * W + warp]);
+#pragma unroll 1
+    for (int r = 0; r < R; ++r) {
+      const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+      const uint32_t range = block_range_mask(tg, blk);
+      Slot e0, e1, e2, e3;
+      uint32_t keep = 0;
+      if (range) {
+        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+        e0 = sample_slot(d, w.x);
+        e1 = sample_slot(d, w.y);
+        e2 = sample_slot(d, w.z);
+        e3 = sample_slot(d, w.w);
+        keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+      }
+      int total;
+      int64_t my = row + warp_exclusive_count(__popc(keep), total);
+      if (keep & 1u) scatter_slot(e0, __ldcs(&a.grad[my++]), invd_s, gacc_s);
+      if (keep & 2u) scatter_slot(e1, __ldcs(&a.grad[my++]), invd_s, gacc_s);
+      if (keep & 4u) scatter_slot(e2, __ldcs(&a.grad[my++]), invd_s, gacc_s);
+      if (keep & 8u) scatter_slot(e3, __ldcs(&a.grad[my]), invd_s, gacc_s);
+      row += total;
+    }
+  }
+  __syncthreads();
+  float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;
+  for (int i = threadIdx.x; i < G; i += TPB) __stcg(&part[i], gacc_s[i]);
+  __threadfence();
+  __syncthreads();
+  if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
+}
+
+struct FinShared {
+  double dscan[33];
+  double sfirst[512];
+  double red[33];
+  double carry;
+};
+
+// Reverse-mode chain of density b: grad_cdf (sum of chunk partials) ->
+// suffix scan -> grad_rho -> normaliser VJP -> grad_values.
+template <int TPB>
+__device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, double* grho, FinShared& sh) {
+  const int32_t nch = __ldg(&a.chunk_first[b + 1]) - __ldg(&a.chunk_first[b]);
+  const int64_t k0 = __ldg(&a.knot_off[b]);
+  const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
+  if (threadIdx.x == 0) {
+    if (!wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch)))
+      raise_status(a.status, LOITS_ERR_TIMEOUT);
+    sh.carry = 0.0;
+  }
+  __syncthreads();
+  const float* g = a.grid + k0;
+  const float* f = a.values + k0;
+  const double norm = __ldcg(&a.norm[b]);
+  const float* part = a.partials + __ldg(&a.part_off[b]);
+  constexpr int E = 4;
+  const int64_t SEG = static_cast<int64_t>(TPB) * E;
+  double gn_local = 0.0;  // sum grho_t * f_t
+  const int64_t nseg = (G + SEG - 1) / SEG;
+  for (int64_t sgi = nseg - 1; sgi >= 0; --sgi) {
+    const int64_t s0 = sgi * SEG;
+    const int64_t s1 = s0 + SEG < G ? s0 + SEG : G;
+    const int64_t my_lo = s0 + static_cast<int64_t>(threadIdx.x) * E;
+    const int64_t my_hi = my_lo + E < s1 ? my_lo + E : s1;
+    double gc[E];
+    double tot = 0.0;
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int64_t t = my_lo + e;
+      double v = 0.0;
+      if (t < my_hi)
+        for (int32_t c = 0; c < nch; ++c) v += static_cast<double>(__ldcg(&part[static_cast<int64_t>(c) * G + t]));
+      gc[e] = v;
+    }
+    // inclusive suffix within the thread: S_t = sum_{s >= t} gc_s
+#pragma unroll
+    for (int e = E - 1; e >= 0; --e) {
+      tot += gc[e];
+      gc[e] = tot;
+    }
+    double seg_tot;
+    const double later = block_exclusive_suffix_sum<double, TPB>(tot, seg_tot, sh.dscan);
+    const double carry = sh.carry;
+    // S_t for my knots, and S of the knot after my last one
+#pragma unroll
+    for (int e = 0; e < E; ++e) gc[e] = gc[e] + (later + carry);
+    sh.sfirst[threadIdx.x] = my_lo < my_hi ? gc[0] : 0.0;
+    __syncthreads();
+#pragma unroll
+    for (int e = 0; e < E; ++e) {
+      const int64_t t = my_lo + e;
+      if (t >= my_hi) break;
+      // S_{t+1}: next knot in this thread, the next thread, or the next segment
+      double s_next;
+      if (e + 1 < E && t + 1 < my_hi) s_next = gc[e + 1];
+      else if (t + 1 >= G) s_next = 0.0;
+      else if (t + 1 >= s1) s_next = carry;
+      else s_next = sh.sfirst[threadIdx.x + 1];
+      const double h_t = t >= 1 ? 0.5 * (static_cast<double>(__ldg(&g[t])) - static_cast<double>(__ldg(&g[t - 1]))) : 0.0;
+      const double h_n = t + 1 < G ? 0.5 * (static_cast<double>(__ldg(&g[t + 1])) - static_cast<double>(__ldg(&g[t]))) : 0.0;
+      const double gr = h_n * s_next + h_t * gc[e];
+      grho[k0 + t] = gr;
+      gn_local += gr * static_cast<double>(__ldg(&f[t]));
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) sh.carry = carry + seg_tot;
+    __syncthreads();
+  }
+  double gn_total;
+  block_exclusive_sum<double, TPB>(gn_local, gn_total, sh.red);
+  const double inv_n = 1.0 / norm;
+  const double gnorm = -gn_total * inv_n * inv_n;
+  __threadfence_block();
+  for (int64_t t = threadIdx.x; t < G; t += TPB) {
+    const double h_t = t >= 1 ? 0.5 * (static_cast<double>(__ldg(&g[t])) - static_cast<double>(__ldg(&g[t - 1]))) : 0.0;
+    const double h_n = t + 1 < G ? 0.5 * (static_cast<double>(__ldg(&g[t + 1])) - static_cast<double>(__ldg(&g[t]))) : 0.0;
+    const double v = grho[k0 + t] * inv_n + (h_t + h_n) * gnorm;
+    a.grad_values[k0 + t] = __double2float_rn(v);
+  }
+  __syncthreads();
+}
+
+// ---------------------------------------------------------------- kernels
+
+// Register cap: 64 per thread (65536 / (64 * TPB) CTAs) keeps four 256-thread CTAs
+// (or two 512-thread CTAs) resident per SM.
+template <int TPB, int R>
+__global__ void __launch_bounds__(TPB, 1024 / TPB) batch_forward_kernel(BatchArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* rec_s = reinterpret_cast<float4*>(smem_raw);
+  uint32_t* guide_s = reinterpret_cast<uint32_t*>(rec_s + a.gcap);
+  float* stage = reinterpret_cast<float*>(guide_s + ((a.mcap + 7) & ~7));
+  __shared__ union {
+    CdfShared cdf;
+    SampleShared smp;
+  } sh;
+  __shared__ uint32_t s_item;
+  const int32_t nC = a.c_hi - a.c_lo, nF = a.f_hi - a.f_lo, nT = a.t_hi - a.t_lo;
+  const uint32_t n_items = static_cast<uint32_t>(nC + nF + nT);
+  while (true) {
+    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();
+    if (item >= n_items) break;
+    if (item < static_cast<uint32_t>(nC)) {
+      cdf_scan_item<TPB>(a, a.c_lo + static_cast<int32_t>(item), sh.cdf);
+    } else if (item < static_cast<uint32_t>(nC + nF)) {
+      cdf_finalize_item<TPB>(a, a.f_lo + static_cast<int32_t>(item) - nC, sh.cdf);
+    } else {
+      sample_item<TPB, R>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s, guide_s, stage,
+                          sh.smp);
+    }
+  }
+}
+
+template <int TPB, int R>
+__global__ void __launch_bounds__(TPB, 1024 / TPB) batch_backward_kernel(BatchArgs a, double* grho) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  float4* rec_s = reinterpret_cast<float4*>(smem_raw);
+  float* invd_s = reinterpret_cast<float*>(rec_s + a.gcap);
+  float* gacc_s = invd_s + a.gcap;
+  uint32_t* guide_s = reinterpret_cast<uint32_t*>(gacc_s + a.gcap);
+  __shared__ union {
+    FinShared fin;
+    SampleShared smp;
+  } sh;
+  __shared__ uint32_t s_item;
+  const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo;
+  const uint32_t n_items = static_cast<uint32_t>(nK + nD);
+  while (true) {
+    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1u);
+    __syncthreads();
+    const uint32_t item = s_item;
+    __syncthreads();
+    if (item >= n_items) break;
+    if (item < static_cast<uint32_t>(nK)) {
+      vjp_chunk_item<TPB, R>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s, invd_s, gacc_s,
+                             sh.smp);
+    } else {
+      vjp_finalize_item<TPB>(a, a.d_lo + static_cast<int32_t>(item) - nK, grho, sh.fin);
+    }
+  }
+}
+
+// CDF export (hi + lo as fp64) and quantiles -----------------------------
+
+__global__ void batch_cdf_export_kernel(const float4* __restrict__ rec, int64_t n,
+                                        double* __restrict__ cdf) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    const float4 r = rec[i];
+    cdf[i] = static_cast<double>(r.x) + static_cast<double>(r.y);
+  }
+}
+
+__global__ void batch_quantile_kernel(const float4* __restrict__ rec,
+                                      const uint16_t* __restrict__ guide, int m, int G,
+                                      bool count_all, const float* __restrict__ u, int64_t n,
+                                      float* __restrict__ x, int32_t* __restrict__ intervals) {
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    // the guide bucket of u needs its 24-bit word: u = k * 2^-24 exactly
+    const float uc = fminf(fmaxf(u[i], 0.0f), 0x1.fffffep-1f);
+    const uint32_t bits = static_cast<uint32_t>(uc * 16777216.0f) << 8;
+    const uint32_t k = bits >> (32 - m);
+    const int j = count_all ? interval_count_all(rec, u[i], G)
+                            : interval_in_range(rec, guide[k], guide[k + 1], u[i], G);
+    float tv;
+    x[i] = interval_value(rec[j], u[i], tv);
+    if (intervals) intervals[i] = j;
+  }
+}
+
+}  // namespace loits_dev

@@ -1,0 +1,85 @@
+// batch_kernels.cuh -- shared definitions of the batched (ragged 1-D) sampler.
+#pragma once
+
+#include <cstdint>
+
+#include "common.cuh"
+
+namespace loits_dev {
+
+// Per-knot state written by the forward's CDF phase and read by sampling,
+// the backward and the quantile entry:
+//   rec[k]  = {c_hi, c_lo, grid_k, m_k}: the normalised CDF at knot k as a
+//             double-float (c = c_hi + c_lo), the knot position, and the
+//             inverse-CDF slope of interval k, m_k = (g_{k+1} - g_k) /
+//             (c_{k+1} - c_k + 1e-5) (0 on the last knot);
+//   invd[k] = 1 / (c_{k+1} - c_k + 1e-5), the backward's weight of interval k;
+//   guide   = per density with a non-decreasing CDF, M = 2^m >= G buckets of
+//             u: L[k] = number of knots with c_t <= k / M, so the interval of
+//             u in [k/M, (k+1)/M) is found among knots [L[k], L[k+1]].
+struct BatchArgs {
+  // plan tables (device)
+  const int64_t* knot_off;     // [B+1]
+  const int64_t* n_events;     // [B]
+  const int32_t* tile_first;   // [B+1] sampling tiles
+  const int32_t* cdf_first;    // [B+1] CDF scan tiles
+  const int32_t* fin_first;    // [B+1] CDF finalize items (multi-tile densities only)
+  const int32_t* chunk_first;  // [B+1] backward chunks
+  const int64_t* part_off;     // [B] offset of a density's chunk partials
+  const int32_t* rowfill_lo;   // [B] first density whose row offset tile 0 of b writes
+  const int64_t* goff;         // [B] offset of a density's guide table (entries)
+  const int32_t* gbits;        // [B] log2 of a density's guide buckets M
+  int32_t nd;
+  int32_t last_nonempty;       // last density with events (-1 if none)
+  // item ranges of this launch (global indices)
+  int32_t c_lo, c_hi;          // CDF scan tiles
+  int32_t f_lo, f_hi;          // CDF finalize items
+  int32_t t_lo, t_hi;          // sampling tiles
+  int32_t k_lo, k_hi;          // backward chunks
+  int32_t d_lo, d_hi;          // densities (backward finalize items)
+  int32_t tiles_total;         // sampling tiles of the whole plan
+  int32_t scan_knots;          // knots per thread per CDF tile
+  int32_t gcap;                // knots a sampling CTA holds in shared memory
+  int32_t mcap;                // guide entries (M + 1) a sampling CTA holds
+  int32_t tiles_per_chunk;
+  int64_t nmax;                // Philox slots per density (slot stride)
+  int64_t dbase;               // global index of plan density 0
+  uint64_t seed, stream_id;
+  PhiloxKey rk;                // round keys of `seed`
+  // inputs
+  const float* grid;
+  const float* values;
+  const float* x_cut;
+  // state (workspace)
+  float4* rec;
+  float* invd;
+  uint16_t* gl;                // per density: L[k] = #{t : c_t <= k / M}, k = 0..M
+  uint32_t* gpk;               // per density: L[k] | L[k+1] << 16, k = 0..M-1
+  double* norm;
+  uint32_t* dflags;            // bit 0: CDF not non-decreasing (count semantics)
+  uint32_t* cdf_ready;         // 1 once a density's records and packed guide are final
+  uint32_t* cdf_scanned;       // scanned CDF tiles per density
+  uint32_t* fin_done;          // finalized CDF tiles per density (multi-tile densities)
+  uint32_t* cflag;             // per CDF tile: 1 aggregate, 2 inclusive
+  double* cagg;
+  double* cinc;
+  double* cmax;                // per CDF tile: max unnormalised prefix seen
+  unsigned long long* tile_state;
+  int64_t* tile_prefix;        // first kept row of each sampling tile
+  int32_t* warp_off;           // kept rows of earlier warps in the tile, per (tile, warp)
+  uint32_t* ticket;            // this launch's ticket counter
+  int32_t* status;
+  uint32_t* chunks_done;       // per density
+  float* partials;
+  // forward outputs
+  float* events;
+  int64_t* row_offsets;
+  int32_t* intervals;
+  // backward
+  const float* grad;
+  float* grad_values;
+};
+
+constexpr uint32_t kNonMonotone = 1u;
+
+}  // namespace loits_dev

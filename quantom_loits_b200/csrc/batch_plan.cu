@@ -1,0 +1,544 @@
+// batch_plan.cu -- host side of the batched sampler: plans, workspace layout,
+// launches (persistent and one-launch-per-density), CDF export, quantiles.
+#include <algorithm>
+#include <cstdint>
+#include <cstring>
+#include <new>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "batch_kernels.cuh"
+
+namespace loits_dev {
+template <int TPB, int R>
+__global__ void batch_forward_kernel(BatchArgs a);
+template <int TPB, int R>
+__global__ void batch_backward_kernel(BatchArgs a, double* grho);
+__global__ void batch_cdf_export_kernel(const float4* rec, int64_t n, double* cdf);
+__global__ void batch_quantile_kernel(const float4* rec, const uint16_t* guide, int m, int G,
+                                      bool count_all, const float* u, int64_t n, float* x,
+                                      int32_t* intervals);
+}  // namespace loits_dev
+
+#include "batch_kernels.cu"  // template definitions (single translation unit)
+
+using namespace loits_dev;
+
+namespace {
+
+constexpr size_t kAlign = 256;
+size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
+
+struct Layout {
+  size_t status, tickets_fwd, dflags, cdf_ready, cdf_scanned, fin_done, cflag, tile_state;  // zeroed by forward
+  size_t tickets_bwd, chunks_done;                                                // zeroed by backward
+  size_t rec, invd, gl, gpk, norm, cagg, cinc, cmax, tile_prefix, warp_off, partials, grho;
+  size_t fwd_zero_lo, fwd_zero_hi, bwd_zero_lo, bwd_zero_hi, total;
+};
+
+}  // namespace
+
+struct loits_batch_plan {
+  int64_t nd = 0;
+  std::vector<int64_t> koff, nev;
+  int64_t nmax = 0, capacity = 0, total_knots = 0, max_g = 0, dbase = 0;
+  loits_batch_config cfg{};
+  int tpb = 256, r = 4, scan_knots = 8;
+  int32_t n_tiles = 0, n_cdf = 0, n_fin = 0, n_chunks = 0, last_nonempty = -1;
+  int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1;
+  int64_t total_partials = 0, total_guide = 0;
+  std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
+  std::vector<int64_t> part_off, goff;
+  void* dtab = nullptr;
+  const int64_t *d_koff = nullptr, *d_nev = nullptr, *d_part_off = nullptr, *d_goff = nullptr;
+  const int32_t *d_tile_first = nullptr, *d_cdf_first = nullptr, *d_fin_first = nullptr,
+                *d_chunk_first = nullptr, *d_rowfill_lo = nullptr, *d_gbits = nullptr;
+  Layout lay{};
+  size_t fwd_smem = 0, bwd_smem = 0;
+  int fwd_grid = 1, bwd_grid = 1, num_sms = 148;
+};
+
+namespace {
+
+using FwdKernel = void (*)(BatchArgs);
+using BwdKernel = void (*)(BatchArgs, double*);
+
+template <int TPB, int R>
+void pick(FwdKernel& f, BwdKernel& b) {
+  f = batch_forward_kernel<TPB, R>;
+  b = batch_backward_kernel<TPB, R>;
+}
+
+bool kernels_for(int tpb, int r, FwdKernel& f, BwdKernel& b) {
+  if (tpb == 256) {
+    switch (r) {
+      case 2: pick<256, 2>(f, b); return true;
+      case 4: pick<256, 4>(f, b); return true;
+      case 8: pick<256, 8>(f, b); return true;
+      case 16: pick<256, 16>(f, b); return true;
+    }
+  } else if (tpb == 512) {
+    switch (r) {
+      case 2: pick<512, 2>(f, b); return true;
+      case 4: pick<512, 4>(f, b); return true;
+      case 8: pick<512, 8>(f, b); return true;
+      case 16: pick<512, 16>(f, b); return true;
+    }
+  }
+  return false;
+}
+
+// Largest number of knots a sampling CTA may hold in shared memory.
+constexpr int64_t kMaxSmemKnots = 8192;
+constexpr size_t kSmemLimit = 227 * 1024;
+
+int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
+  out = in ? *in : loits_batch_config{};
+  if (out.threads == 0) out.threads = 256;
+  if (out.blocks_per_item == 0) out.blocks_per_item = 8;
+  if (out.scan_knots == 0) out.scan_knots = 8;
+  if (out.threads != 256 && out.threads != 512) return LOITS_ERR_INVALID;
+  if (out.blocks_per_item != 2 && out.blocks_per_item != 4 && out.blocks_per_item != 8 &&
+      out.blocks_per_item != 16)
+    return LOITS_ERR_INVALID;
+  if (out.scan_knots < 1 || out.scan_knots > 64) return LOITS_ERR_INVALID;
+  if (out.ctas_per_sm < 0 || out.ctas_per_sm > 32) return LOITS_ERR_INVALID;
+  if (out.plain != 0 && out.plain != 1) return LOITS_ERR_INVALID;
+  if (out.density_base < 0 || out.slot_stride < 0) return LOITS_ERR_INVALID;
+  return LOITS_OK;
+}
+
+template <typename T>
+T* carve(void* ws, size_t off) {
+  return reinterpret_cast<T*>(static_cast<char*>(ws) + off);
+}
+
+BatchArgs base_args(const loits_batch_plan* p, void* ws) {
+  BatchArgs a{};
+  a.knot_off = p->d_koff;
+  a.n_events = p->d_nev;
+  a.tile_first = p->d_tile_first;
+  a.cdf_first = p->d_cdf_first;
+  a.fin_first = p->d_fin_first;
+  a.chunk_first = p->d_chunk_first;
+  a.part_off = p->d_part_off;
+  a.rowfill_lo = p->d_rowfill_lo;
+  a.goff = p->d_goff;
+  a.gbits = p->d_gbits;
+  a.mcap = p->mcap;
+  a.nd = static_cast<int32_t>(p->nd);
+  a.last_nonempty = p->last_nonempty;
+  a.tiles_total = p->n_tiles;
+  a.scan_knots = p->scan_knots;
+  a.gcap = p->gcap;
+  a.tiles_per_chunk = p->tiles_per_chunk;
+  a.nmax = p->nmax;
+  a.dbase = p->dbase;
+  const Layout& L = p->lay;
+  a.rec = carve<float4>(ws, L.rec);
+  a.invd = carve<float>(ws, L.invd);
+  a.gl = carve<uint16_t>(ws, L.gl);
+  a.gpk = carve<uint32_t>(ws, L.gpk);
+  a.fin_done = carve<uint32_t>(ws, L.fin_done);
+  a.norm = carve<double>(ws, L.norm);
+  a.dflags = carve<uint32_t>(ws, L.dflags);
+  a.cdf_ready = carve<uint32_t>(ws, L.cdf_ready);
+  a.cdf_scanned = carve<uint32_t>(ws, L.cdf_scanned);
+  a.cflag = carve<uint32_t>(ws, L.cflag);
+  a.cagg = carve<double>(ws, L.cagg);
+  a.cinc = carve<double>(ws, L.cinc);
+  a.cmax = carve<double>(ws, L.cmax);
+  a.tile_state = carve<unsigned long long>(ws, L.tile_state);
+  a.tile_prefix = carve<int64_t>(ws, L.tile_prefix);
+  a.warp_off = carve<int32_t>(ws, L.warp_off);
+  a.status = carve<int32_t>(ws, L.status);
+  a.chunks_done = carve<uint32_t>(ws, L.chunks_done);
+  a.partials = carve<float>(ws, L.partials);
+  return a;
+}
+
+bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+}  // namespace
+
+extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_offsets,
+                                       const int64_t* event_counts,
+                                       const loits_batch_config* cfg, loits_batch_plan** out) {
+  if (!out) return LOITS_ERR_INVALID;
+  *out = nullptr;
+  if (n_densities < 1 || n_densities > (1 << 24) || !knot_offsets || !event_counts)
+    return LOITS_ERR_INVALID;
+  loits_batch_config c;
+  int rc = resolve_config(cfg, c);
+  if (rc != LOITS_OK) return rc;
+  auto* p = new (std::nothrow) loits_batch_plan();
+  if (!p) return LOITS_ERR_INVALID;
+  p->nd = n_densities;
+  p->cfg = c;
+  p->tpb = c.threads;
+  p->r = c.blocks_per_item;
+  p->scan_knots = c.scan_knots;
+  p->koff.assign(knot_offsets, knot_offsets + n_densities + 1);
+  p->nev.assign(event_counts, event_counts + n_densities);
+  if (p->koff[0] != 0) { delete p; return LOITS_ERR_INVALID; }
+  for (int64_t b = 0; b < n_densities; ++b) {
+    const int64_t g = p->koff[b + 1] - p->koff[b];
+    if (g < 2 || p->nev[b] < 0) { delete p; return LOITS_ERR_INVALID; }
+    p->max_g = std::max(p->max_g, g);
+    p->nmax = std::max(p->nmax, p->nev[b]);
+    p->capacity += p->nev[b];
+    if (p->nev[b] > 0) p->last_nonempty = static_cast<int32_t>(b);
+  }
+  p->total_knots = p->koff[n_densities];
+  if (p->max_g > kMaxSmemKnots) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  if (c.slot_stride > 0) {
+    if (c.slot_stride < p->nmax) { delete p; return LOITS_ERR_INVALID; }
+    p->nmax = c.slot_stride;
+  }
+  p->dbase = c.density_base;
+  if (p->nmax > 0 && static_cast<double>(p->nmax) * static_cast<double>(n_densities + p->dbase) > 4.0e18) {
+    delete p;
+    return LOITS_ERR_UNSUPPORTED;
+  }
+  // ---- work items
+  const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;
+  const int64_t kt = static_cast<int64_t>(p->tpb) * p->scan_knots;
+  p->tile_first.resize(n_densities + 1);
+  p->cdf_first.resize(n_densities + 1);
+  p->fin_first.resize(n_densities + 1);
+  p->rowfill_lo.resize(n_densities);
+  int64_t nt = 0, nc = 0, nf = 0;
+  int32_t next_fill = 0;
+  for (int64_t b = 0; b < n_densities; ++b) {
+    p->tile_first[b] = static_cast<int32_t>(nt);
+    p->cdf_first[b] = static_cast<int32_t>(nc);
+    p->fin_first[b] = static_cast<int32_t>(nf);
+    const int64_t g = p->koff[b + 1] - p->koff[b];
+    const int64_t tiles_c = (g + kt - 1) / kt;
+    nc += tiles_c;
+    if (tiles_c > 1) nf += tiles_c;
+    const int64_t n = p->nev[b];
+    if (n > 0) {
+      const int64_t P0 = (p->dbase + b) * p->nmax;
+      const int64_t nblk = ((P0 + n - 1) >> 2) - (P0 >> 2) + 1;
+      nt += (nblk + blocks_per_tile - 1) / blocks_per_tile;
+      p->rowfill_lo[b] = next_fill;
+      next_fill = static_cast<int32_t>(b + 1);
+    } else {
+      p->rowfill_lo[b] = next_fill;
+    }
+  }
+  if (nt > 0x7fffffff || nc > 0x7fffffff) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  p->tile_first[n_densities] = static_cast<int32_t>(nt);
+  p->cdf_first[n_densities] = static_cast<int32_t>(nc);
+  p->fin_first[n_densities] = static_cast<int32_t>(nf);
+  p->n_tiles = static_cast<int32_t>(nt);
+  p->n_cdf = static_cast<int32_t>(nc);
+  p->n_fin = static_cast<int32_t>(nf);
+  // multiple of 4 so that every shared-memory array after the records stays
+  // 16-byte aligned (float4 staging)
+  p->gcap = static_cast<int32_t>((p->max_g + 3) & ~int64_t(3));
+  // guide tables: M = 2^m buckets per density, 2G <= M < 4G (4 <= M <=
+  // 2^14), kept as M + 1 uint16 counts and as M packed uint32 pairs; both
+  // arrays use the same entry offsets
+  p->gbits.resize(n_densities);
+  p->goff.resize(n_densities);
+  int64_t go = 0;
+  for (int64_t b = 0; b < n_densities; ++b) {
+    const int64_t g = p->koff[b + 1] - p->koff[b];
+    int m = 2;
+    while ((int64_t(1) << m) < 2 * g && m < 14) ++m;
+    p->gbits[b] = m;
+    p->goff[b] = go;
+    go += ((int64_t(1) << m) + 1 + 7) & ~int64_t(7);
+    p->mcap = std::max<int32_t>(p->mcap, static_cast<int32_t>(int64_t(1) << m));
+  }
+  p->total_guide = go;
+
+  // ---- launch geometry
+  FwdKernel fk;
+  BwdKernel bk;
+  kernels_for(p->tpb, p->r, fk, bk);
+  const int64_t tile_events = blocks_per_tile * 4;
+  // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32
+  const size_t guide_bytes = static_cast<size_t>((p->mcap + 7) & ~7) * sizeof(uint32_t);
+  p->fwd_smem = static_cast<size_t>(p->gcap) * sizeof(float4) + guide_bytes +
+                (tile_events + 4) * sizeof(float);
+  p->bwd_smem = static_cast<size_t>(p->gcap) * (sizeof(float4) + 2 * sizeof(float)) + guide_bytes;
+  if (p->fwd_smem > kSmemLimit || p->bwd_smem > kSmemLimit) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
+  cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
+  if (cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(std::max<size_t>(p->fwd_smem, 1))) != cudaSuccess ||
+      cudaFuncSetAttribute(bk, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(std::max<size_t>(p->bwd_smem, 1))) != cudaSuccess) {
+    delete p;
+    return LOITS_ERR_CUDA;
+  }
+  int occ_f = 0, occ_b = 0;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fk, p->tpb, p->fwd_smem);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, bk, p->tpb, p->bwd_smem);
+  if (occ_f < 1 || occ_b < 1) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  if (c.ctas_per_sm > 0) {
+    occ_f = std::min(occ_f, static_cast<int>(c.ctas_per_sm));
+    occ_b = std::min(occ_b, static_cast<int>(c.ctas_per_sm));
+  }
+  const int64_t items_f = nc + nf + nt;
+  p->fwd_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items_f, int64_t(occ_f) * p->num_sms)));
+  const int64_t resident_b = int64_t(occ_b) * p->num_sms;
+  // backward chunks: ~2 per resident CTA
+  const int64_t target_chunks = std::max<int64_t>(1, 2 * resident_b);
+  p->tiles_per_chunk = static_cast<int32_t>(std::max<int64_t>(1, nt / target_chunks));
+  p->chunk_first.resize(n_densities + 1);
+  p->part_off.resize(n_densities);
+  int64_t nk = 0, po = 0;
+  for (int64_t b = 0; b < n_densities; ++b) {
+    p->chunk_first[b] = static_cast<int32_t>(nk);
+    p->part_off[b] = po;
+    const int64_t tiles_b = p->tile_first[b + 1] - p->tile_first[b];
+    const int64_t ch = (tiles_b + p->tiles_per_chunk - 1) / p->tiles_per_chunk;
+    nk += ch;
+    po += ch * (p->koff[b + 1] - p->koff[b]);
+  }
+  p->chunk_first[n_densities] = static_cast<int32_t>(nk);
+  p->n_chunks = static_cast<int32_t>(nk);
+  p->total_partials = po;
+  const int64_t items_b = nk + n_densities;
+  p->bwd_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items_b, resident_b)));
+
+  // ---- workspace layout
+  Layout& L = p->lay;
+  size_t o = 0;
+  const size_t nd = static_cast<size_t>(n_densities);
+  L.fwd_zero_lo = o;
+  L.status = o; o += 16;
+  L.tickets_fwd = o; o = align_up(o + (nd + 1) * 4, 16);
+  L.dflags = o; o = align_up(o + nd * 4, 16);
+  L.cdf_ready = o; o = align_up(o + nd * 4, 16);
+  L.cdf_scanned = o; o = align_up(o + nd * 4, 16);
+  L.fin_done = o; o = align_up(o + nd * 4, 16);
+  L.cflag = o; o = align_up(o + static_cast<size_t>(nc) * 4, 16);
+  L.tile_state = o; o = align_up(o + static_cast<size_t>(nt) * 8, 16);
+  L.fwd_zero_hi = o;
+  o = align_up(o);
+  L.bwd_zero_lo = o;
+  L.tickets_bwd = o; o = align_up(o + (nd + 1) * 4, 16);
+  L.chunks_done = o; o = align_up(o + nd * 4, 16);
+  L.bwd_zero_hi = o;
+  o = align_up(o);
+  L.rec = o; o = align_up(o + static_cast<size_t>(p->total_knots) * 16);
+  L.invd = o; o = align_up(o + static_cast<size_t>(p->total_knots) * 4);
+  L.gl = o; o = align_up(o + static_cast<size_t>(p->total_guide) * 2);
+  L.gpk = o; o = align_up(o + static_cast<size_t>(p->total_guide) * 4);
+  L.norm = o; o = align_up(o + nd * 8);
+  L.cagg = o; o = align_up(o + static_cast<size_t>(nc) * 8);
+  L.cinc = o; o = align_up(o + static_cast<size_t>(nc) * 8);
+  L.cmax = o; o = align_up(o + static_cast<size_t>(nc) * 8);
+  L.tile_prefix = o; o = align_up(o + static_cast<size_t>(nt) * 8);
+  L.warp_off = o; o = align_up(o + static_cast<size_t>(nt) * (p->tpb / 32) * 4);
+  L.partials = o; o = align_up(o + static_cast<size_t>(po) * 4);
+  L.grho = o; o = align_up(o + static_cast<size_t>(p->total_knots) * 8);
+  L.total = o;
+
+  // ---- device tables (one allocation owned by the plan)
+  std::vector<char> host;
+  auto push = [&host](const void* src, size_t bytes) {
+    const size_t off = align_up(host.size(), 16);
+    host.resize(off + bytes);
+    if (bytes) std::memcpy(host.data() + off, src, bytes);
+    return off;
+  };
+  const size_t o_koff = push(p->koff.data(), p->koff.size() * 8);
+  const size_t o_nev = push(p->nev.data(), p->nev.size() * 8);
+  const size_t o_part = push(p->part_off.data(), p->part_off.size() * 8);
+  const size_t o_tf = push(p->tile_first.data(), p->tile_first.size() * 4);
+  const size_t o_cf = push(p->cdf_first.data(), p->cdf_first.size() * 4);
+  const size_t o_ff = push(p->fin_first.data(), p->fin_first.size() * 4);
+  const size_t o_kf = push(p->chunk_first.data(), p->chunk_first.size() * 4);
+  const size_t o_rf = push(p->rowfill_lo.data(), p->rowfill_lo.size() * 4);
+  const size_t o_go = push(p->goff.data(), p->goff.size() * 8);
+  const size_t o_gb = push(p->gbits.data(), p->gbits.size() * 4);
+  if (cudaMalloc(&p->dtab, host.size()) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
+  if (cudaMemcpy(p->dtab, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(p->dtab);
+    delete p;
+    return LOITS_ERR_CUDA;
+  }
+  char* d = static_cast<char*>(p->dtab);
+  p->d_koff = reinterpret_cast<const int64_t*>(d + o_koff);
+  p->d_nev = reinterpret_cast<const int64_t*>(d + o_nev);
+  p->d_part_off = reinterpret_cast<const int64_t*>(d + o_part);
+  p->d_tile_first = reinterpret_cast<const int32_t*>(d + o_tf);
+  p->d_cdf_first = reinterpret_cast<const int32_t*>(d + o_cf);
+  p->d_fin_first = reinterpret_cast<const int32_t*>(d + o_ff);
+  p->d_chunk_first = reinterpret_cast<const int32_t*>(d + o_kf);
+  p->d_rowfill_lo = reinterpret_cast<const int32_t*>(d + o_rf);
+  p->d_goff = reinterpret_cast<const int64_t*>(d + o_go);
+  p->d_gbits = reinterpret_cast<const int32_t*>(d + o_gb);
+  *out = p;
+  return LOITS_OK;
+}
+
+extern "C" void loits_batch_plan_destroy(loits_batch_plan* plan) {
+  if (!plan) return;
+  if (plan->dtab) cudaFree(plan->dtab);
+  delete plan;
+}
+
+extern "C" int64_t loits_batch_capacity(const loits_batch_plan* p) { return p ? p->capacity : -1; }
+extern "C" int64_t loits_batch_total_knots(const loits_batch_plan* p) {
+  return p ? p->total_knots : -1;
+}
+extern "C" size_t loits_batch_workspace_bytes(const loits_batch_plan* p) {
+  return p ? p->lay.total : 0;
+}
+extern "C" size_t loits_batch_status_offset(const loits_batch_plan* p) {
+  return p ? p->lay.status : 0;
+}
+extern "C" int loits_batch_plan_config(const loits_batch_plan* p, loits_batch_config* cfg) {
+  if (!p || !cfg) return LOITS_ERR_INVALID;
+  *cfg = p->cfg;
+  return LOITS_OK;
+}
+
+extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
+                                   const float* values, const float* x_cut, uint64_t seed,
+                                   uint64_t sequence, float* events, int64_t* row_offsets,
+                                   int32_t* intervals, void* workspace, void* stream) {
+  if (!p || !grid || !values || !row_offsets || !workspace) return LOITS_ERR_INVALID;
+  if (p->capacity > 0 && (!events || !aligned16(events))) return LOITS_ERR_INVALID;
+  if (!aligned16(workspace)) return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const Layout& L = p->lay;
+  if (cudaMemsetAsync(static_cast<char*>(workspace) + L.fwd_zero_lo, 0,
+                      L.fwd_zero_hi - L.fwd_zero_lo, st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  if (p->n_tiles == 0 &&
+      cudaMemsetAsync(row_offsets, 0, (p->nd + 1) * sizeof(int64_t), st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  BatchArgs a = base_args(p, workspace);
+  a.seed = seed;
+  a.rk = philox_key(seed);
+  a.stream_id = 2 * sequence;
+  a.grid = grid;
+  a.values = values;
+  a.x_cut = x_cut;
+  a.events = events;
+  a.row_offsets = row_offsets;
+  a.intervals = intervals;
+  FwdKernel fk;
+  BwdKernel bk;
+  kernels_for(p->tpb, p->r, fk, bk);
+  uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_fwd);
+  if (!p->cfg.plain) {
+    a.c_lo = 0; a.c_hi = p->n_cdf;
+    a.f_lo = 0; a.f_hi = p->n_fin;
+    a.t_lo = 0; a.t_hi = p->n_tiles;
+    a.d_lo = 0; a.d_hi = static_cast<int32_t>(p->nd);
+    a.ticket = tickets + p->nd;
+    fk<<<p->fwd_grid, p->tpb, p->fwd_smem, st>>>(a);
+    return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
+  }
+  for (int64_t b = 0; b < p->nd; ++b) {
+    a.c_lo = p->cdf_first[b]; a.c_hi = p->cdf_first[b + 1];
+    a.f_lo = p->fin_first[b]; a.f_hi = p->fin_first[b + 1];
+    a.t_lo = p->tile_first[b]; a.t_hi = p->tile_first[b + 1];
+    a.d_lo = static_cast<int32_t>(b); a.d_hi = static_cast<int32_t>(b + 1);
+    a.ticket = tickets + b;
+    const int64_t items = (a.c_hi - a.c_lo) + (a.f_hi - a.f_lo) + (a.t_hi - a.t_lo);
+    const int grid_b = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, p->fwd_grid)));
+    fk<<<grid_b, p->tpb, p->fwd_smem, st>>>(a);
+    if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
+  }
+  return LOITS_OK;
+}
+
+extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid,
+                                    const float* values, const float* x_cut, uint64_t seed,
+                                    uint64_t sequence, const float* grad_events,
+                                    float* grad_values, void* workspace, void* stream) {
+  if (!p || !grid || !values || !grad_values || !workspace) return LOITS_ERR_INVALID;
+  if (p->capacity > 0 && (!grad_events || !aligned16(grad_events))) return LOITS_ERR_INVALID;
+  if (!aligned16(workspace)) return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const Layout& L = p->lay;
+  if (cudaMemsetAsync(static_cast<char*>(workspace) + L.bwd_zero_lo, 0,
+                      L.bwd_zero_hi - L.bwd_zero_lo, st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  BatchArgs a = base_args(p, workspace);
+  a.seed = seed;
+  a.rk = philox_key(seed);
+  a.stream_id = 2 * sequence;
+  a.grid = grid;
+  a.values = values;
+  a.x_cut = x_cut;
+  a.grad = grad_events;
+  a.grad_values = grad_values;
+  double* grho = carve<double>(workspace, L.grho);
+  FwdKernel fk;
+  BwdKernel bk;
+  kernels_for(p->tpb, p->r, fk, bk);
+  uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_bwd);
+  if (!p->cfg.plain) {
+    a.k_lo = 0; a.k_hi = p->n_chunks;
+    a.d_lo = 0; a.d_hi = static_cast<int32_t>(p->nd);
+    a.ticket = tickets + p->nd;
+    bk<<<p->bwd_grid, p->tpb, p->bwd_smem, st>>>(a, grho);
+    return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
+  }
+  for (int64_t b = 0; b < p->nd; ++b) {
+    a.k_lo = p->chunk_first[b]; a.k_hi = p->chunk_first[b + 1];
+    a.d_lo = static_cast<int32_t>(b); a.d_hi = static_cast<int32_t>(b + 1);
+    a.ticket = tickets + b;
+    const int64_t items = (a.k_hi - a.k_lo) + 1;
+    const int grid_b = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, p->bwd_grid)));
+    bk<<<grid_b, p->tpb, p->bwd_smem, st>>>(a, grho);
+    if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
+  }
+  return LOITS_OK;
+}
+
+extern "C" int loits_batch_cdf(const loits_batch_plan* p, const void* workspace, double* cdf,
+                               double* norm, void* stream) {
+  if (!p || !workspace || !cdf) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const float4* rec = reinterpret_cast<const float4*>(static_cast<const char*>(workspace) + p->lay.rec);
+  const int64_t n = p->total_knots;
+  const int threads = 256;
+  const int64_t grid = std::min<int64_t>((n + threads - 1) / threads, 148 * 32);
+  batch_cdf_export_kernel<<<static_cast<int>(std::max<int64_t>(grid, 1)), threads, 0, st>>>(rec, n, cdf);
+  if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
+  if (norm &&
+      cudaMemcpyAsync(norm, static_cast<const char*>(workspace) + p->lay.norm,
+                      p->nd * sizeof(double), cudaMemcpyDeviceToDevice, st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  return LOITS_OK;
+}
+
+extern "C" int loits_batch_quantile(const loits_batch_plan* p, const void* workspace,
+                                    int64_t density, const float* u, int64_t n, float* x,
+                                    int32_t* intervals, void* stream) {
+  if (!p || !workspace || density < 0 || density >= p->nd || n < 0 || (n > 0 && (!u || !x)))
+    return LOITS_ERR_INVALID;
+  if (n == 0) return LOITS_OK;
+  // the non-decreasing flag lives on the device; read it (a 4-byte sync copy)
+  uint32_t flags = 0;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const char* ws = static_cast<const char*>(workspace);
+  if (cudaMemcpyAsync(&flags, ws + p->lay.dflags + density * 4, 4, cudaMemcpyDeviceToHost, st) !=
+          cudaSuccess ||
+      cudaStreamSynchronize(st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  const float4* rec = reinterpret_cast<const float4*>(ws + p->lay.rec) + p->koff[density];
+  const uint16_t* guide = reinterpret_cast<const uint16_t*>(ws + p->lay.gl) + p->goff[density];
+  const int G = static_cast<int>(p->koff[density + 1] - p->koff[density]);
+  const int threads = 256;
+  const int64_t grid = std::min<int64_t>((n + threads - 1) / threads, 148 * 32);
+  batch_quantile_kernel<<<static_cast<int>(grid), threads, 0, st>>>(
+      rec, guide, p->gbits[density], G, (flags & kNonMonotone) != 0, u, n, x, intervals);
+  return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
+}

@@ -1,0 +1,556 @@
+// tuple_kernels.cu -- the reference's 2-D theory tuple on sm_100a (fp64).
+//
+// Drop-in for the reference's native module (cpp/bindings.cpp:24-208): same
+// Philox counters (padded slot p = (b*cells + cell)*nmax + slot, x stream
+// 2*sequence, q stream 2*sequence+1, cpp/bindings.cpp:79-92), same int16
+// count-semantics intervals, same epsilon, same compaction predicate and
+// (b, cell, slot) order.  This file is compiled with -fmad=false so that every
+// fp64 product and sum is rounded on its own, in the order the reference
+// writes it (cpp/loits_core.cpp), which makes the forward bit-identical to
+// the reference built without contraction.
+//
+// Kernels:
+//   fill_uniform_kernel    cpp/loits_core.cpp:39-53
+//   tuple_prepare_kernel   allocate_counts :22-37 + density :55-109 + cdf :111-165,
+//                          one thread per cell (each cell owns one x and one q curve)
+//   cell_scan_kernel       exclusive prefix of counts, nmax, active (one CTA)
+//   tuple_sample_kernel    fill_uniform + interpolate :167-237 + compact :239-266
+//                          fused; uniforms live in registers only; stable
+//                          compaction by decoupled look-back over ordered tiles
+//   tuple_backward_kernel  interpolation_vjp :268-338 + cdf_vjp :340-398 +
+//                          density_vjp :400-472, one warp per cell,
+//                          deterministic (fixed-order warp reductions)
+#include <cmath>
+#include <cstdint>
+
+#include "common.cuh"
+#include "lookback.cuh"
+
+namespace loits_dev {
+
+constexpr double kEpsilon = 1e-5;
+
+// ------------------------------------------------------------ fill_uniform
+
+__global__ void fill_uniform_kernel(float* __restrict__ out, int64_t count, uint64_t seed,
+                                    uint64_t stream_id) {
+  const int64_t nblocks = (count + 3) >> 2;
+  for (int64_t blk = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; blk < nblocks;
+       blk += (int64_t)gridDim.x * blockDim.x) {
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_id, seed);
+    const int64_t p = blk << 2;
+    if (p + 3 < count && (reinterpret_cast<uintptr_t>(out + p) & 15) == 0) {
+      *reinterpret_cast<float4*>(out + p) =
+          make_float4(uniform_from_bits(w.x), uniform_from_bits(w.y), uniform_from_bits(w.z),
+                      uniform_from_bits(w.w));
+    } else {
+      for (int i = 0; i < 4 && p + i < count; ++i) out[p + i] = uniform_from_bits(word_of(w, i));
+    }
+  }
+}
+
+// --------------------------------------------------------------- prepare
+
+struct TupleGeom {
+  int64_t batch, nx, ny, kx, kq, cells;
+};
+
+// Trapezoid norm + CDF of one curve, in the reference's operation order.
+__device__ double curve_cdf(const double* __restrict__ bins, const double* __restrict__ xs,
+                            int64_t k, double acc, double* __restrict__ cdf) {
+  double n = 0.0;
+  for (int64_t t = 1; t < k; ++t) {
+    const double hw = 0.5 * (bins[t] - bins[t - 1]);
+    n += hw * (xs[t - 1] + xs[t]);
+  }
+  const double inv_n = 1.0 / n;
+  double cum = 0.0;
+  double r_prev = xs[0] * inv_n;
+  cdf[0] = 0.0;
+  for (int64_t t = 1; t < k; ++t) {
+    const double r_t = xs[t] * inv_n;
+    const double hw = 0.5 * (bins[t] - bins[t - 1]);
+    cum += hw * (r_prev + r_t);
+    cdf[t] = cum * acc;
+    r_prev = r_t;
+  }
+  return n;
+}
+
+__global__ void tuple_prepare_kernel(TupleGeom g, const double* __restrict__ x_bins,
+                                     const double* __restrict__ xsec_x,
+                                     const double* __restrict__ q_bins,
+                                     const double* __restrict__ xsec_q,
+                                     const double* __restrict__ weights,
+                                     const uint8_t* __restrict__ acceptance, int64_t n_events,
+                                     int64_t* __restrict__ counts, double* __restrict__ norm_x,
+                                     double* __restrict__ norm_q, double* __restrict__ cdf_x,
+                                     double* __restrict__ cdf_q) {
+  const int64_t ncell = g.batch * g.cells;
+  const double scale = static_cast<double>(n_events);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < ncell;
+       i += (int64_t)gridDim.x * blockDim.x) {
+    counts[i] = static_cast<int64_t>(fabs(weights[i] * scale));
+    const int64_t b = i / g.cells, cell = i - b * g.cells;
+    const int64_t ix = cell / g.ny, iy = cell - ix * g.ny;
+    const double acc = acceptance[i] ? 1.0 : 0.0;
+    const int64_t xi = (b * g.ny + iy) * g.nx + ix;  // x curve, y-major storage
+    norm_x[xi] = curve_cdf(x_bins + (b * g.nx + ix) * g.kx, xsec_x + xi * g.kx, g.kx, acc,
+                           cdf_x + xi * g.kx);
+    norm_q[i] = curve_cdf(q_bins + (b * g.ny + iy) * g.kq, xsec_q + i * g.kq, g.kq, acc,
+                          cdf_q + i * g.kq);
+  }
+}
+
+// One CTA: cell_offsets = exclusive prefix of counts; alloc = {nmax, active}.
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads)
+    cell_scan_kernel(const int64_t* __restrict__ counts, int64_t ncell,
+                     int64_t* __restrict__ cell_offsets, int64_t* __restrict__ alloc) {
+  __shared__ long long s_sum[kScanThreads / 32 + 1];
+  __shared__ long long s_max[kScanThreads / 32 + 1];
+  const int64_t per = (ncell + kScanThreads - 1) / kScanThreads;
+  const int64_t lo = threadIdx.x * per;
+  const int64_t hi = lo + per < ncell ? lo + per : ncell;
+  long long local = 0, mx = 0;
+  for (int64_t i = lo; i < hi; ++i) {
+    local += counts[i];
+    mx = counts[i] > mx ? counts[i] : mx;
+  }
+  long long total;
+  long long run = block_exclusive_sum<long long, kScanThreads>(local, total, s_sum);
+  long long gmax;
+  block_exclusive_max<long long, kScanThreads>(mx, 0ll, gmax, s_max);
+  for (int64_t i = lo; i < hi; ++i) {
+    cell_offsets[i] = run;
+    run += counts[i];
+  }
+  if (threadIdx.x == 0) {
+    cell_offsets[ncell] = total;
+    alloc[0] = gmax;
+    alloc[1] = total;
+  }
+}
+
+// ----------------------------------------------------------------- sample
+
+// Count-semantics interval of cpp/loits_core.cpp:12-18 (all k knots, then
+// clamp to [0, k-2], int16).
+__device__ __forceinline__ int interval_count(const double* __restrict__ c, int64_t k, double u) {
+  int64_t sel = -1;
+  for (int64_t t = 0; t < k; ++t) sel += (u >= c[t]) ? 1 : 0;
+  if (sel < 0) sel = 0;
+  if (sel > k - 2) sel = k - 2;
+  return static_cast<int16_t>(sel);
+}
+
+__device__ __forceinline__ double curve_value(const double* __restrict__ bins,
+                                              const double* __restrict__ c, int j, double u) {
+  const double c0 = c[j];
+  const double inv_d = 1.0 / (c[j + 1] - c0 + kEpsilon);
+  const double m = (bins[j + 1] - bins[j]) * inv_d;
+  return bins[j] + m * (u - c0);
+}
+
+constexpr int kSampleThreads = 256;
+constexpr int kSampleEPT = 4;  // consecutive active events per thread
+constexpr int kSampleTile = kSampleThreads * kSampleEPT;
+
+struct TupleSampleArgs {
+  TupleGeom g;
+  const double* x_bins;
+  const double* q_bins;
+  const double* cdf_x;
+  const double* cdf_q;
+  const int64_t* cell_offsets;
+  int64_t nmax, active;
+  uint64_t seed, stream_x, stream_q;
+  double* events;
+  int64_t* packed;
+  int16_t* interval_x;
+  int16_t* interval_q;
+  int64_t* valid;
+  int32_t* status;
+  uint32_t* ticket;
+  unsigned long long* tile_state;
+  int64_t n_tiles;
+};
+
+__global__ void __launch_bounds__(kSampleThreads) tuple_sample_kernel(TupleSampleArgs a) {
+  __shared__ long long s_scan[kSampleThreads / 32 + 1];
+  __shared__ long long s_base;
+  __shared__ uint32_t s_tile;
+  if (threadIdx.x == 0) s_tile = atomicAdd(a.ticket, 1u);
+  __syncthreads();
+  const int64_t tile = s_tile;
+  const int64_t ncell = a.g.batch * a.g.cells;
+  const int64_t e0 = tile * kSampleTile + threadIdx.x * kSampleEPT;
+
+  double xs[kSampleEPT], qs[kSampleEPT];
+  int64_t ps[kSampleEPT];
+  int16_t jxs[kSampleEPT], jqs[kSampleEPT];
+  int keep = 0;
+  if (e0 < a.active) {
+    // cell holding active event e0: last c with cell_offsets[c] <= e0
+    int64_t lo = 0, hi = ncell;  // answer in [lo, hi)
+    while (hi - lo > 1) {
+      const int64_t mid = (lo + hi) >> 1;
+      if (a.cell_offsets[mid] <= e0) lo = mid; else hi = mid;
+    }
+    int64_t c = lo;
+    uint64_t cached_blk = ~0ull;
+    uint4 wx = make_uint4(0, 0, 0, 0), wq = wx;
+#pragma unroll
+    for (int i = 0; i < kSampleEPT; ++i) {
+      const int64_t e = e0 + i;
+      if (e >= a.active) break;
+      while (a.cell_offsets[c + 1] <= e) ++c;
+      const int64_t p = c * a.nmax + (e - a.cell_offsets[c]);
+      const uint64_t blk = static_cast<uint64_t>(p) >> 2;
+      if (blk != cached_blk) {
+        wx = philox4x32_10(blk, a.stream_x, a.seed);
+        wq = philox4x32_10(blk, a.stream_q, a.seed);
+        cached_blk = blk;
+      }
+      const double ux = static_cast<double>(uniform_from_bits(word_of(wx, p & 3)));
+      const double uq = static_cast<double>(uniform_from_bits(word_of(wq, p & 3)));
+      const int64_t b = c / a.g.cells, cell = c - b * a.g.cells;
+      const int64_t ix = cell / a.g.ny, iy = cell - ix * a.g.ny;
+      const double* xc = a.cdf_x + ((b * a.g.ny + iy) * a.g.nx + ix) * a.g.kx;
+      const double* xb = a.x_bins + (b * a.g.nx + ix) * a.g.kx;
+      const double* qc = a.cdf_q + c * a.g.kq;
+      const double* qb = a.q_bins + (b * a.g.ny + iy) * a.g.kq;
+      const int jx = interval_count(xc, a.g.kx, ux);
+      const int jq = interval_count(qc, a.g.kq, uq);
+      const double x = curve_value(xb, xc, jx, ux);
+      const double q = curve_value(qb, qc, jq, uq);
+      const bool ok = isfinite(x) && isfinite(q) && x * q != 0.0;
+      xs[i] = x;
+      qs[i] = q;
+      ps[i] = p;
+      jxs[i] = static_cast<int16_t>(jx);
+      jqs[i] = static_cast<int16_t>(jq);
+      keep |= ok ? (1 << i) : 0;
+    }
+  }
+  long long tile_count;
+  const long long rank0 =
+      block_exclusive_sum<long long, kSampleThreads>(__popc(keep), tile_count, s_scan);
+  if (threadIdx.x < 32) {
+    const int64_t base = lookback_exclusive(a.tile_state, tile, tile_count, a.status);
+    if (threadIdx.x == 0) s_base = base;
+  }
+  __syncthreads();
+  int64_t row = s_base + rank0;
+#pragma unroll
+  for (int i = 0; i < kSampleEPT; ++i) {
+    if (!(keep & (1 << i))) continue;
+    a.events[2 * row] = xs[i];
+    a.events[2 * row + 1] = qs[i];
+    a.packed[row] = ps[i];
+    if (a.interval_x) a.interval_x[row] = jxs[i];
+    if (a.interval_q) a.interval_q[row] = jqs[i];
+    ++row;
+  }
+  if (tile == a.n_tiles - 1 && threadIdx.x == 0) *a.valid = s_base + tile_count;
+}
+
+// --------------------------------------------------------------- backward
+
+struct TupleBackwardArgs {
+  TupleGeom g;
+  const double* grad;
+  const int64_t* packed;
+  int64_t nvalid, nmax;
+  uint64_t seed, stream_x, stream_q;
+  const double* x_bins;
+  const double* xsec_x;
+  const double* q_bins;
+  const double* xsec_q;
+  const uint8_t* acceptance;
+  const double* norm_x;
+  const double* norm_q;
+  const double* cdf_x;
+  const double* cdf_q;
+  double* grad_x;
+  double* grad_q;
+};
+
+// First row whose packed index is >= key (packed is strictly increasing).
+__device__ __forceinline__ int64_t lower_bound_i64(const int64_t* __restrict__ v, int64_t n,
+                                                   int64_t key) {
+  int64_t lo = 0, hi = n;
+  while (lo < hi) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (v[mid] < key) lo = mid + 1; else hi = mid;
+  }
+  return lo;
+}
+
+// Contribution of one row to grad_cdf[j] and grad_cdf[j+1]
+// (cpp/loits_core.cpp:293-300).
+__device__ __forceinline__ void value_vjp(const double* __restrict__ bins,
+                                          const double* __restrict__ c, int j, double u, double g,
+                                          double& to_j, double& to_j1) {
+  const double c0 = c[j];
+  const double d = c[j + 1] - c0 + kEpsilon;
+  const double inv_d = 1.0 / d;
+  const double t = u - c0;
+  const double db = bins[j + 1] - bins[j];
+  const double up = g * db;
+  to_j = up * (-inv_d + t * inv_d * inv_d);
+  to_j1 = -(up * t * inv_d * inv_d);
+}
+
+// Reverse suffix scan + normaliser VJP of one curve (cpp/loits_core.cpp:
+// 340-472), sequential; gx doubles as grad_rho scratch.
+__device__ void curve_chain(const double* __restrict__ bins, const double* __restrict__ xs,
+                            double n, double acc, const double* __restrict__ gcdf, int64_t k,
+                            double* __restrict__ gx) {
+  for (int64_t t = 0; t < k; ++t) gx[t] = 0.0;
+  double suffix = 0.0;
+  for (int64_t t = k - 1; t > 0; --t) {
+    suffix += gcdf[t];
+    const double g = 0.5 * (bins[t] - bins[t - 1]) * acc * suffix;
+    gx[t - 1] += g;
+    gx[t] += g;
+  }
+  const double inv_n = 1.0 / n;
+  const double inv_n2 = inv_n * inv_n;
+  double gnorm = 0.0;
+  for (int64_t t = 0; t < k; ++t) {
+    const double gr = gx[t];
+    gx[t] = gr * inv_n;
+    gnorm -= gr * xs[t] * inv_n2;
+  }
+  for (int64_t t = 1; t < k; ++t) {
+    const double g = 0.5 * (bins[t] - bins[t - 1]) * gnorm;
+    gx[t - 1] += g;
+    gx[t] += g;
+  }
+}
+
+// dynamic smem: warps_per_block * (kx + kq) doubles
+__global__ void tuple_backward_kernel(TupleBackwardArgs a) {
+  extern __shared__ double s_acc[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const int64_t gc = static_cast<int64_t>(blockIdx.x) * wpb + warp;
+  const int64_t ncell = a.g.batch * a.g.cells;
+  if (gc >= ncell) return;  // whole warp leaves together
+  const int64_t kx = a.g.kx, kq = a.g.kq;
+  double* acc_x = s_acc + warp * (kx + kq);
+  double* acc_q = acc_x + kx;
+  for (int64_t t = lane; t < kx + kq; t += 32) acc_x[t] = 0.0;
+
+  const int64_t b = gc / a.g.cells, cell = gc - b * a.g.cells;
+  const int64_t ix = cell / a.g.ny, iy = cell - ix * a.g.ny;
+  const int64_t xi = (b * a.g.ny + iy) * a.g.nx + ix;
+  const double* xc = a.cdf_x + xi * kx;
+  const double* xb = a.x_bins + (b * a.g.nx + ix) * kx;
+  const double* qc = a.cdf_q + gc * kq;
+  const double* qb = a.q_bins + (b * a.g.ny + iy) * kq;
+  const int64_t r0 = lower_bound_i64(a.packed, a.nvalid, gc * a.nmax);
+  const int64_t r1 = lower_bound_i64(a.packed, a.nvalid, (gc + 1) * a.nmax);
+  __syncwarp();
+  for (int64_t base = r0; base < r1; base += 32) {
+    const int64_t r = base + lane;
+    int jx = -2, jq = -2;
+    double ax = 0.0, bx = 0.0, aq = 0.0, bq = 0.0;
+    if (r < r1) {
+      const int64_t p = a.packed[r];
+      const uint64_t blk = static_cast<uint64_t>(p) >> 2;
+      const double ux =
+          static_cast<double>(uniform_from_bits(word_of(philox4x32_10(blk, a.stream_x, a.seed), p & 3)));
+      const double uq =
+          static_cast<double>(uniform_from_bits(word_of(philox4x32_10(blk, a.stream_q, a.seed), p & 3)));
+      jx = interval_count(xc, kx, ux);
+      jq = interval_count(qc, kq, uq);
+      value_vjp(xb, xc, jx, ux, a.grad[2 * r], ax, bx);
+      value_vjp(qb, qc, jq, uq, a.grad[2 * r + 1], aq, bq);
+    }
+    // fixed-order warp reductions per knot: deterministic accumulation
+    for (int64_t t = 0; t < kx; ++t) {
+      double v = (jx == t ? ax : 0.0) + (jx + 1 == t ? bx : 0.0);
+      v = warp_sum(v);
+      if (lane == 0) acc_x[t] += v;
+    }
+    for (int64_t t = 0; t < kq; ++t) {
+      double v = (jq == t ? aq : 0.0) + (jq + 1 == t ? bq : 0.0);
+      v = warp_sum(v);
+      if (lane == 0) acc_q[t] += v;
+    }
+  }
+  __syncwarp();
+  const double acc = a.acceptance[gc] ? 1.0 : 0.0;
+  if (lane == 0) {
+    curve_chain(xb, a.xsec_x + xi * kx, a.norm_x[xi], acc, acc_x, kx, a.grad_x + xi * kx);
+  } else if (lane == 1) {
+    curve_chain(qb, a.xsec_q + gc * kq, a.norm_q[gc], acc, acc_q, kq, a.grad_q + gc * kq);
+  }
+}
+
+}  // namespace loits_dev
+
+// ===================================================================== C ABI
+
+using namespace loits_dev;
+
+namespace {
+
+int launch_status(cudaError_t e) { return e == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA; }
+
+bool valid_shape(const loits_shape* s) {
+  return s && s->batch >= 0 && s->nx >= 1 && s->ny >= 1 && s->kx >= 2 && s->kq >= 2;
+}
+
+TupleGeom geom_of(const loits_shape* s) {
+  return TupleGeom{s->batch, s->nx, s->ny, s->kx, s->kq, s->nx * s->ny};
+}
+
+int grid_for(int64_t n, int threads) {
+  int64_t g = (n + threads - 1) / threads;
+  if (g < 1) g = 1;
+  if (g > 148 * 64) g = 148 * 64;
+  return static_cast<int>(g);
+}
+
+}  // namespace
+
+extern "C" int loits_fill_uniform(float* values, int64_t count, uint64_t seed, uint64_t stream_id,
+                                  void* stream) {
+  if (count < 0 || (count > 0 && !values)) return LOITS_ERR_INVALID;
+  if (count == 0) return LOITS_OK;
+  const int threads = 256;
+  fill_uniform_kernel<<<grid_for((count + 3) / 4, threads), threads, 0,
+                        static_cast<cudaStream_t>(stream)>>>(values, count, seed, stream_id);
+  return launch_status(cudaGetLastError());
+}
+
+extern "C" int loits_tuple_prepare(const loits_shape* shape, const double* x_bins,
+                                   const double* xsec_x, const double* q_bins,
+                                   const double* xsec_q, const double* weights,
+                                   const uint8_t* acceptance, int64_t n_events, int64_t* counts,
+                                   int64_t* cell_offsets, double* norm_x, double* norm_q,
+                                   double* cdf_x, double* cdf_q, int64_t* alloc, void* stream) {
+  if (!valid_shape(shape) || n_events < 0) return LOITS_ERR_INVALID;
+  if (shape->kx > 32767 || shape->kq > 32767) return LOITS_ERR_UNSUPPORTED;  // int16 intervals
+  const TupleGeom g = geom_of(shape);
+  const int64_t ncell = g.batch * g.cells;
+  if (!alloc || !cell_offsets) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (ncell > 0) {
+    if (!x_bins || !xsec_x || !q_bins || !xsec_q || !weights || !acceptance || !counts ||
+        !norm_x || !norm_q || !cdf_x || !cdf_q)
+      return LOITS_ERR_INVALID;
+    tuple_prepare_kernel<<<grid_for(ncell, 128), 128, 0, st>>>(
+        g, x_bins, xsec_x, q_bins, xsec_q, weights, acceptance, n_events, counts, norm_x, norm_q,
+        cdf_x, cdf_q);
+    if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
+  }
+  cell_scan_kernel<<<1, kScanThreads, 0, st>>>(counts, ncell, cell_offsets, alloc);
+  return launch_status(cudaGetLastError());
+}
+
+extern "C" size_t loits_tuple_sample_workspace(int64_t active) {
+  const int64_t tiles = (active + kSampleTile - 1) / kSampleTile;
+  return 16 + static_cast<size_t>(tiles) * sizeof(unsigned long long);
+}
+
+extern "C" int loits_tuple_sample(const loits_shape* shape, const double* x_bins,
+                                  const double* q_bins, const double* cdf_x, const double* cdf_q,
+                                  const int64_t* cell_offsets, int64_t nmax, int64_t active,
+                                  uint64_t seed, uint64_t sequence, double* events,
+                                  int64_t* packed, int16_t* interval_x, int16_t* interval_q,
+                                  int64_t* valid, int32_t* status, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  if (!valid_shape(shape) || nmax < 0 || active < 0 || !valid || !status) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(status, 0, sizeof(int32_t), st) != cudaSuccess) return LOITS_ERR_CUDA;
+  if (active == 0) return launch_status(cudaMemsetAsync(valid, 0, sizeof(int64_t), st));
+  if (!x_bins || !q_bins || !cdf_x || !cdf_q || !cell_offsets || !events || !packed || !workspace)
+    return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  const size_t need = loits_tuple_sample_workspace(active);
+  if (workspace_bytes < need) return LOITS_ERR_CAPACITY;
+  if (cudaMemsetAsync(workspace, 0, need, st) != cudaSuccess) return LOITS_ERR_CUDA;
+  TupleSampleArgs a;
+  a.g = geom_of(shape);
+  a.x_bins = x_bins;
+  a.q_bins = q_bins;
+  a.cdf_x = cdf_x;
+  a.cdf_q = cdf_q;
+  a.cell_offsets = cell_offsets;
+  a.nmax = nmax;
+  a.active = active;
+  a.seed = seed;
+  a.stream_x = 2 * sequence;
+  a.stream_q = 2 * sequence + 1;
+  a.events = events;
+  a.packed = packed;
+  a.interval_x = interval_x;
+  a.interval_q = interval_q;
+  a.valid = valid;
+  a.status = status;
+  a.ticket = static_cast<uint32_t*>(workspace);
+  a.tile_state = reinterpret_cast<unsigned long long*>(static_cast<char*>(workspace) + 16);
+  a.n_tiles = (active + kSampleTile - 1) / kSampleTile;
+  if (a.n_tiles > 0x7fffffff) return LOITS_ERR_UNSUPPORTED;
+  tuple_sample_kernel<<<static_cast<unsigned>(a.n_tiles), kSampleThreads, 0, st>>>(a);
+  return launch_status(cudaGetLastError());
+}
+
+extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
+                                    const int64_t* packed, int64_t nvalid, int64_t nmax,
+                                    uint64_t seed, uint64_t sequence, const double* x_bins,
+                                    const double* xsec_x, const double* q_bins,
+                                    const double* xsec_q, const uint8_t* acceptance,
+                                    const double* norm_x, const double* norm_q,
+                                    const double* cdf_x, const double* cdf_q,
+                                    double* grad_xsec_x, double* grad_xsec_q, void* stream) {
+  if (!valid_shape(shape) || nvalid < 0 || nmax < 0) return LOITS_ERR_INVALID;
+  if (shape->kx > 32767 || shape->kq > 32767) return LOITS_ERR_UNSUPPORTED;
+  const TupleGeom g = geom_of(shape);
+  const int64_t ncell = g.batch * g.cells;
+  if (ncell == 0) return LOITS_OK;
+  if (!x_bins || !xsec_x || !q_bins || !xsec_q || !acceptance || !norm_x || !norm_q || !cdf_x ||
+      !cdf_q || !grad_xsec_x || !grad_xsec_q || (nvalid > 0 && (!grad_events || !packed)))
+    return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  TupleBackwardArgs a;
+  a.g = g;
+  a.grad = grad_events;
+  a.packed = packed;
+  a.nvalid = nvalid;
+  a.nmax = nmax;
+  a.seed = seed;
+  a.stream_x = 2 * sequence;
+  a.stream_q = 2 * sequence + 1;
+  a.x_bins = x_bins;
+  a.xsec_x = xsec_x;
+  a.q_bins = q_bins;
+  a.xsec_q = xsec_q;
+  a.acceptance = acceptance;
+  a.norm_x = norm_x;
+  a.norm_q = norm_q;
+  a.cdf_x = cdf_x;
+  a.cdf_q = cdf_q;
+  a.grad_x = grad_xsec_x;
+  a.grad_q = grad_xsec_q;
+  const size_t per_warp = static_cast<size_t>(g.kx + g.kq) * sizeof(double);
+  int wpb = 8;
+  while (wpb > 1 && per_warp * wpb > 48 * 1024) wpb >>= 1;
+  const size_t smem = per_warp * wpb;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (smem > 48 * 1024) {
+    if (smem > 200 * 1024) return LOITS_ERR_UNSUPPORTED;
+    if (cudaFuncSetAttribute(tuple_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             static_cast<int>(smem)) != cudaSuccess)
+      return LOITS_ERR_CUDA;
+  }
+  const int64_t blocks = (ncell + wpb - 1) / wpb;
+  if (blocks > 0x7fffffff) return LOITS_ERR_UNSUPPORTED;
+  tuple_backward_kernel<<<static_cast<unsigned>(blocks), wpb * 32, smem, st>>>(a);
+  return launch_status(cudaGetLastError());
+}

@@ -1,0 +1,68 @@
+"""Data-parallel sharding of a density batch across ranks (one GPU each).
+
+Densities are independent and Philox is counter based, so a batch splits into
+contiguous density ranges with no exchange on the data path: rank r plans its
+range with ``density_base`` = the global index of its first density and
+``slot_stride`` = the whole batch's max n_b, and then draws exactly the
+counters the unsplit batch would (slot s of global density g uses counter
+g * slot_stride + s).  Concatenating the ranks' kept rows in rank order gives
+the unsplit batch's rows.
+
+Ranges are balanced by cumulative event count (the work measure).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+
+def shard_range(event_counts, world_size: int, rank: int) -> tuple[int, int]:
+    """[lo, hi) densities of `rank`: the densities whose first event falls in
+    the rank's equal share of the total event count."""
+    counts = np.asarray(event_counts, dtype=np.int64)
+    if world_size < 1 or not 0 <= rank < world_size:
+        raise ValueError("bad world_size / rank")
+    nd = len(counts)
+    starts = np.concatenate([[0], np.cumsum(counts)[:-1]])
+    total = int(counts.sum())
+    if total == 0:
+        per = -(-nd // world_size)
+        return min(rank * per, nd), min((rank + 1) * per, nd)
+    # density d belongs to the rank whose share contains its first event
+    owner = np.minimum((starts * world_size) // max(total, 1), world_size - 1)
+    idx = np.flatnonzero(owner == rank)
+    if idx.size == 0:
+        # empty share: an empty range positioned after the previous rank's
+        before = np.flatnonzero(owner < rank)
+        lo = int(before[-1]) + 1 if before.size else 0
+        return lo, lo
+    return int(idx[0]), int(idx[-1]) + 1
+
+
+def sub_case(case: dict, lo: int, hi: int) -> dict:
+    """Densities [lo, hi) of a batch given as a dict of host arrays
+    (knot_offsets, event_counts, grid, values, optional x_cut, scalars)."""
+    koff = np.asarray(case["knot_offsets"], dtype=np.int64)
+    k0, k1 = int(koff[lo]), int(koff[hi])
+    out = dict(case)
+    out["knot_offsets"] = koff[lo:hi + 1] - k0
+    out["event_counts"] = np.asarray(case["event_counts"])[lo:hi]
+    out["grid"] = np.asarray(case["grid"])[k0:k1]
+    out["values"] = np.asarray(case["values"])[k0:k1]
+    if case.get("x_cut") is not None:
+        out["x_cut"] = np.asarray(case["x_cut"])[lo:hi]
+    for k in ("cotangent", "events", "intervals", "row_offsets", "grad_values", "slots"):
+        out.pop(k, None)
+    return out
+
+
+def shard_spec(spec, world_size: int, rank: int):
+    """(sub-spec, density_base, slot_stride) of a workloads.DensityBatchSpec."""
+    from dataclasses import replace
+
+    lo, hi = shard_range(spec.event_counts, world_size, rank)
+    koff = spec.knot_offsets
+    k0, k1 = int(koff[lo]), int(koff[hi])
+    sub = replace(spec, knot_offsets=koff[lo:hi + 1] - k0, grid=spec.grid[k0:k1],
+                  values=spec.values[k0:k1], event_counts=spec.event_counts[lo:hi],
+                  x_cut=None if spec.x_cut is None else spec.x_cut[lo:hi])
+    return sub, lo, int(np.max(spec.event_counts)) if len(spec.event_counts) else 0

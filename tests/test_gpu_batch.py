@@ -1,0 +1,307 @@
+"""GPU parity of the batched ragged-density sampler (fp32 storage) through the C ABI.
+
+References:
+* golden vectors of the reference's own compiled core on the exact embedding
+  of a batch into the reference tuple (tests/golden/make_golden.py);
+* the CPU oracle (fp64) for larger shapes, the CDF, quantiles and the
+  branch-frozen central finite differences;
+* a plain PyTorch fp64 restatement of the reference's torch stages
+  (pytorch/loits.py:16-63) differentiated by autograd with the same uniforms.
+
+Tolerances (stated by the sampler's contract): events within 1e-5 relative of
+the reference; intervals bit-exact except where u lies within 2 ulp of a CDF
+knot (counted); row offsets / compaction order exact; gradients within 1e-4
+of the gradient scale; CDF within 1e-6 of the fp64 oracle.
+"""
+import numpy as np
+import pytest
+import torch
+
+from conftest import DENSITY_CASES, golden_case
+
+pytestmark = pytest.mark.gpu
+
+DEV = torch.device("cuda:0")
+EVENT_RTOL = 1e-5
+GRAD_TOL = 1e-4
+CDF_TOL = 1e-6
+
+
+@pytest.fixture(scope="module")
+def B():
+    from quantom_loits_b200 import batched
+
+    return batched
+
+
+def run_batch(B, case, config=None, with_intervals=True, seed=None, sequence=None):
+    """Forward (+ backward when a cotangent is given) on static buffers."""
+    koff, counts = case["knot_offsets"], case["event_counts"]
+    plan = B.BatchPlan(koff, counts, config, DEV)
+    grid = torch.from_numpy(np.ascontiguousarray(case["grid"], dtype=np.float32)).to(DEV)
+    values = torch.from_numpy(np.ascontiguousarray(case["values"], dtype=np.float32)).to(DEV)
+    x_cut = case.get("x_cut")
+    x_cut = None if x_cut is None else torch.from_numpy(np.asarray(x_cut, np.float32)).to(DEV)
+    seed = int(case["scalars"][0]) if seed is None else seed
+    seq = int(case["scalars"][1]) if sequence is None else sequence
+    events, rows, ws = plan.new_events(), plan.new_row_offsets(), plan.new_workspace()
+    ints = torch.full((max(plan.capacity, 1),), -1, dtype=torch.int32, device=DEV) if with_intervals else None
+    plan.forward(grid, values, x_cut, seed, seq, events, rows, ws, ints)
+    plan.check_status(ws)
+    valid = int(rows[-1].item())
+    out = dict(plan=plan, events=events[:valid].cpu().numpy(), rows=rows.cpu().numpy(), ws=ws,
+               valid=valid, grid=grid, values=values, x_cut=x_cut, seed=seed, seq=seq)
+    if with_intervals:
+        out["intervals"] = ints[:valid].cpu().numpy()
+    if "cotangent" in case:
+        g = torch.zeros(max(plan.capacity, 4), dtype=torch.float32, device=DEV)
+        g[:valid] = torch.from_numpy(np.asarray(case["cotangent"], dtype=np.float32)).to(DEV)
+        gv = torch.empty_like(values)
+        plan.backward(grid, values, x_cut, seed, seq, g, gv, ws)
+        plan.check_status(ws)
+        out["grad_values"] = gv.cpu().numpy()
+    return out
+
+
+def near_knot(u, cdf_row, ulps=2):
+    """True where fp32 u lies within `ulps` fp32 ulps of some CDF knot."""
+    u = np.asarray(u, np.float32)
+    spacing = np.spacing(u.astype(np.float32)).astype(np.float64) * ulps
+    idx = np.searchsorted(cdf_row, u.astype(np.float64))
+    lo = np.abs(u - cdf_row[np.clip(idx - 1, 0, len(cdf_row) - 1)])
+    hi = np.abs(u - cdf_row[np.clip(idx, 0, len(cdf_row) - 1)])
+    return np.minimum(lo, hi) <= np.maximum(spacing, 2.0**-24 * ulps)
+
+
+def check_against_oracle(out, case, ora, x_cut=None, density_base=0, slot_stride=0):
+    eoff = np.concatenate([[0], np.cumsum(case["event_counts"])])
+    ref = ora.d_forward(case["knot_offsets"], eoff, case["grid"], case["values"], x_cut,
+                        out["seed"], out["seq"], density_base, slot_stride)
+    return ref
+
+
+@pytest.mark.parametrize("name", DENSITY_CASES)
+def test_forward_backward_match_reference(B, golden, oracle_lib, name):
+    c = golden_case(golden, name)
+    out = run_batch(B, c)
+    # compaction order and per-density row offsets: exact
+    assert np.array_equal(out["rows"], c["row_offsets"])
+    np.testing.assert_allclose(out["events"], c["events"], rtol=EVENT_RTOL, atol=0)
+    # intervals: exact except u within 2 ulp of a knot
+    diff = out["intervals"] != c["intervals"]
+    if diff.any():
+        eoff = np.concatenate([[0], np.cumsum(c["event_counts"])])
+        ref = oracle_lib.d_forward(c["knot_offsets"], eoff, c["grid"], c["values"], c.get("x_cut"),
+                                   out["seed"], out["seq"])
+        for r in np.flatnonzero(diff):
+            b = np.searchsorted(c["row_offsets"], r, side="right") - 1
+            o, e = c["knot_offsets"][b], c["knot_offsets"][b + 1]
+            assert near_knot(ref["u"][r:r + 1], ref["cdf"][o:e])[0], f"row {r} flipped far from a knot"
+    scale = np.abs(c["grad_values"]).max()
+    assert np.abs(out["grad_values"] - c["grad_values"]).max() <= GRAD_TOL * scale
+
+
+def test_single_density_workload_matches_reference_digest(B, golden):
+    """The 256-knot, 1e5-event workload: every kept event within 1e-5 of the
+    reference (strided sample) and the same number of rows."""
+    c = golden_case(golden, "single")
+    c = dict(c)
+    out = run_batch(B, c)
+    assert out["valid"] == 100_000
+    np.testing.assert_allclose(out["events"][c["sample_index"]], c["events_sample"],
+                               rtol=EVENT_RTOL, atol=0)
+
+
+def test_cdf_matches_fp64_oracle(B, golden, oracle_lib):
+    for name in DENSITY_CASES:
+        c = golden_case(golden, name)
+        out = run_batch(B, c, with_intervals=False)
+        cdf, norm = out["plan"].cdf(out["ws"])
+        onorm, ocdf, _ = oracle_lib.d_cdf(c["knot_offsets"], c["grid"], c["values"])
+        err = np.abs(cdf.cpu().numpy() - ocdf).max()
+        assert err <= CDF_TOL, (name, err)
+        np.testing.assert_allclose(norm.cpu().numpy(), onorm, rtol=1e-12)
+
+
+# The backward accumulates each chunk's grad-CDF with fp32 shared-memory
+# atomics, whose order varies from run to run: gradients are reproducible to
+# fp32 accumulation rounding, events and row offsets bit for bit.
+GRAD_REPRO = 1e-6
+
+
+def test_plain_and_persistent_forms_agree(B, golden):
+    c = golden_case(golden, "ragged_workload_small")
+    a = run_batch(B, c)
+    b = run_batch(B, c, B.make_config(plain=1))
+    assert np.array_equal(a["rows"], b["rows"])
+    assert np.array_equal(a["events"], b["events"])
+    scale = np.abs(a["grad_values"]).max()
+    assert np.abs(a["grad_values"] - b["grad_values"]).max() <= GRAD_REPRO * scale
+
+
+@pytest.mark.parametrize("threads,blocks,scan", [(256, 2, 1), (256, 2, 3), (512, 4, 8),
+                                                 (512, 8, 16), (256, 16, 64)])
+def test_launch_geometries_agree(B, golden, threads, blocks, scan):
+    c = golden_case(golden, "ragged_small")
+    a = run_batch(B, c)
+    b = run_batch(B, c, B.make_config(threads=threads, blocks_per_item=blocks, scan_knots=scan))
+    assert np.array_equal(a["rows"], b["rows"])
+    assert np.array_equal(a["events"], b["events"])
+    assert np.array_equal(a["intervals"], b["intervals"])
+    scale = np.abs(a["grad_values"]).max()
+    assert np.abs(a["grad_values"] - b["grad_values"]).max() <= GRAD_REPRO * scale
+
+
+def test_graph_replay_matches_eager(B):
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.uniform(scale=5e-3, n_densities=8)
+    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, None, DEV)
+    step = B.BatchStep(plan, seed=spec.seed)
+    step.grid.copy_(torch.from_numpy(spec.grid))
+    step.values.copy_(torch.from_numpy(spec.values))
+    step.grad_events.normal_()
+    step.step()
+    step.check_status()
+    ev0, gv0 = step.events.clone(), step.grad_values.clone()
+    step.capture()
+    step.events.zero_()
+    step.grad_values.zero_()
+    for _ in range(3):
+        step.step()
+    torch.cuda.synchronize()
+    step.check_status()
+    assert torch.equal(step.events, ev0)
+    scale = gv0.abs().max()
+    assert (step.grad_values - gv0).abs().max() <= GRAD_REPRO * scale
+
+
+def test_shards_reproduce_the_whole_batch(B, golden):
+    """Densities split across plans with (density_base, slot_stride) sample the
+    same events as the unsplit batch (the multi-GPU sharding contract)."""
+    c = golden_case(golden, "ragged_workload_small")
+    full = run_batch(B, c)
+    from quantom_loits_b200 import sharding
+
+    nmax = int(np.max(c["event_counts"]))
+    parts = []
+    for rank in range(3):
+        lo, hi = sharding.shard_range(c["event_counts"], 3, rank)
+        if lo == hi:
+            continue
+        sub = sharding.sub_case(c, lo, hi)
+        cfg = B.make_config(density_base=lo, slot_stride=nmax)
+        parts.append(run_batch(B, sub, cfg, seed=full["seed"], sequence=full["seq"]))
+    assert np.array_equal(np.concatenate([p["events"] for p in parts]), full["events"])
+
+
+def test_quantiles_match_oracle(B, oracle_lib):
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.uniform(scale=1e-3, n_densities=4)
+    case = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, scalars=np.array([1234, 0]))
+    out = run_batch(B, case, with_intervals=False)
+    _, ocdf, _ = oracle_lib.d_cdf(spec.knot_offsets, spec.grid, spec.values)
+    p = np.array([1e-6, 0.5, 1 - 1e-6], dtype=np.float32)
+    for b in range(4):
+        x, j = out["plan"].quantile(out["ws"], b, torch.from_numpy(p))
+        xo, jo = oracle_lib.d_quantile(b, spec.knot_offsets, spec.grid, ocdf, p.astype(np.float64))
+        np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=EVENT_RTOL)
+        assert np.array_equal(j.cpu().numpy(), jo)
+
+
+def torch_reference_events(grid, values, koff, u_rows, rows_density, x_cut):
+    """fp64 restatement of the reference torch stages (pytorch/loits.py:16-63)
+    on 1-D densities with given uniforms; differentiable w.r.t. values."""
+    xs = []
+    for b in range(len(koff) - 1):
+        o, e = int(koff[b]), int(koff[b + 1])
+        g, f = grid[o:e], values[o:e]
+        norm = torch.trapezoid(f, g)
+        rho = f / norm
+        cdf = torch.nn.functional.pad(torch.cumulative_trapezoid(rho, g), (1, 0))
+        m = (g[1:] - g[:-1]) / (cdf[1:] - cdf[:-1] + 1e-5)
+        c0 = g[:-1] - m * cdf[:-1]
+        u = u_rows[rows_density == b]
+        j = ((u[:, None] >= cdf[None, :]).sum(-1) - 1).clamp(0, len(m) - 1)
+        xs.append(torch.gather(m, 0, j) * u + torch.gather(c0, 0, j))
+    return torch.cat(xs)
+
+
+def test_gradient_matches_torch_autograd(B, golden, oracle_lib):
+    c = golden_case(golden, "ragged_small")
+    out = run_batch(B, c)
+    eoff = np.concatenate([[0], np.cumsum(c["event_counts"])])
+    ref = oracle_lib.d_forward(c["knot_offsets"], eoff, c["grid"], c["values"], c["x_cut"],
+                               out["seed"], out["seq"])
+    rows_d = np.repeat(np.arange(len(c["event_counts"])), np.diff(ref["row_offsets"]))
+    values = torch.tensor(c["values"], dtype=torch.float64, requires_grad=True)
+    x = torch_reference_events(torch.tensor(c["grid"], dtype=torch.float64), values,
+                               c["knot_offsets"], torch.tensor(ref["u"], dtype=torch.float64),
+                               torch.tensor(rows_d), c["x_cut"])
+    np.testing.assert_allclose(x.detach().numpy(), out["events"], rtol=EVENT_RTOL)
+    (x * torch.tensor(c["cotangent"], dtype=torch.float64)).sum().backward()
+    tg = values.grad.numpy()
+    scale = np.abs(tg).max()
+    assert np.abs(out["grad_values"] - tg).max() <= GRAD_TOL * scale
+
+
+def test_finite_difference_gradient_uniform_workload(B, oracle_lib):
+    """The 64 x 1024-knot workload (event count scaled to 2e4 per density):
+    analytic VJP vs branch-frozen FP64 central differences, step 1e-6
+    relative, at 32 random grid entries."""
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.uniform(scale=0.02)
+    rng = np.random.default_rng(0)
+    case = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, scalars=np.array([spec.seed, 0]))
+    case["cotangent"] = rng.standard_normal(spec.total_events).astype(np.float32)
+    out = run_batch(B, case, with_intervals=False)
+    assert out["valid"] == spec.total_events
+    eoff = spec.event_offsets
+    rows = out["rows"]
+    flips_total = 0
+    for _ in range(32):
+        b = int(rng.integers(0, spec.n_densities))
+        o, k = int(spec.knot_offsets[b]), int(spec.knot_offsets[b + 1] - spec.knot_offsets[b])
+        t = int(rng.integers(0, k))
+        fmean = float(np.abs(spec.values[o:o + k]).mean())
+        h = 1e-6 * max(abs(float(spec.values[o + t])), fmean)
+        d, flips = oracle_lib.d_fd(b, t, h, spec.knot_offsets, eoff, spec.grid, spec.values, None,
+                                   spec.seed, 0, case["cotangent"][rows[b]:rows[b + 1]])
+        flips_total += flips
+        scale = max(np.abs(out["grad_values"][o:o + k]).max(), 1e-12)
+        assert abs(out["grad_values"][o + t] - d) <= GRAD_TOL * scale, (b, t, d)
+
+
+def test_non_monotone_density_uses_count_semantics(B, oracle_lib):
+    """Negative density values make the CDF non-monotone; the reference then
+    counts every knot (cpp/loits_core.cpp:12-18) and so must the sampler."""
+    grid = np.linspace(0.0, 1.0, 9, dtype=np.float32)
+    values = np.array([1.0, 2.0, -1.5, -0.5, 1.0, 3.0, 0.5, -0.2, 1.0], dtype=np.float32)
+    case = dict(knot_offsets=np.array([0, 9]), event_counts=np.array([5000]), grid=grid,
+                values=values, scalars=np.array([7, 3]))
+    out = run_batch(B, case)
+    ref = oracle_lib.d_forward(case["knot_offsets"], np.array([0, 5000]), grid, values, None, 7, 3)
+    assert ref["monotone"][0] == 0
+    assert out["valid"] == len(ref["events"])
+    np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL, atol=1e-6)
+    assert np.mean(out["intervals"] == ref["intervals"]) > 0.999
+
+
+def test_empty_and_tiny_densities(B, oracle_lib):
+    grid = np.concatenate([np.array([0.2, 0.4], np.float32), np.linspace(0.1, 1, 5, dtype=np.float32),
+                           np.array([0.5, 0.6], np.float32)])
+    values = np.concatenate([np.array([1.0, 1.0], np.float32), np.ones(5, np.float32),
+                             np.array([0.0, 2.0], np.float32)])
+    koff = np.array([0, 2, 7, 9])
+    for counts in ([0, 0, 0], [0, 13, 0], [3, 0, 1], [1, 1, 1]):
+        case = dict(knot_offsets=koff, event_counts=np.array(counts), grid=grid, values=values,
+                    scalars=np.array([3, 1]))
+        out = run_batch(B, case)
+        ref = oracle_lib.d_forward(koff, np.concatenate([[0], np.cumsum(counts)]), grid, values,
+                                   None, 3, 1)
+        assert np.array_equal(out["rows"], ref["row_offsets"]), counts
+        np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
