@@ -123,12 +123,17 @@ __device__ __forceinline__ bool add_area(const float* __restrict__ g, const floa
 }
 
 // Pass 1 over this thread's knots [my_lo, my_hi): local total and max prefix.
+// bad_grid: a knot position is not finite or below its predecessor.
 __device__ __forceinline__ void cdf_pass1(const float* g, const float* f, int64_t my_lo,
-                                          int64_t my_hi, double& total, double& maxp, bool& neg) {
+                                          int64_t my_hi, double& total, double& maxp, bool& neg,
+                                          bool& bad_grid) {
   float ph = 0.0f, pl = 0.0f;
   maxp = kNegInf;
   neg = false;
+  bad_grid = false;
   for (int64_t t = my_lo; t < my_hi; ++t) {
+    const float gt = __ldg(&g[t]);
+    bad_grid |= !isfinite(gt) || (t >= 1 && !(gt >= __ldg(&g[t - 1])));
     neg |= !add_area(g, f, t, ph, pl);
     const double p = static_cast<double>(ph) + static_cast<double>(pl);
     maxp = p > maxp ? p : maxp;
@@ -173,6 +178,23 @@ __device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, int6
     if (t == 0)
       for (int32_t k = 0; k < k_lo; ++k) gd[k] = 0;
   }
+}
+
+// kAcceptAll when every event of density b is provably kept: with a
+// non-decreasing CDF the search gives u >= c_j, so t = u - c_j >= 0 (exactly
+// evaluated), and with an ascending finite grid the slope is finite and >= 0,
+// hence x = g_j + m t >= g_0.  If g_0 > 0 and the cut (if any) is below g_0,
+// x is finite, non-zero and above the cut for every uniform: the stable
+// compaction is the identity.
+__device__ __forceinline__ uint32_t accept_all_flag(const BatchArgs& a, int b, int64_t k0,
+                                                    int64_t G, double norm, uint32_t flags) {
+  if (flags & (kNonMonotone | kBadGrid)) return 0u;
+  if (!(norm > 0.0) || !isfinite(norm)) return 0u;
+  const float g0 = __ldg(&a.grid[k0]);
+  // g_last bounds every slope (g_last - g_0) / 1e-5 well inside fp32 range
+  if (!(g0 > 0.0f) || !(__ldg(&a.grid[k0 + G - 1]) < 1e30f)) return 0u;
+  if (a.x_cut && !(__ldg(&a.x_cut[b]) < g0)) return 0u;
+  return kAcceptAll;
 }
 
 // Pack density b's guide for sampling: gpk[k] = L[k] | L[k+1] << 16.  Every
@@ -284,13 +306,15 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
   double tot, maxp;
   bool neg;
-  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg);
+  bool bad_grid;
+  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg, bad_grid);
   double tile_tot;
   const double excl = block_exclusive_sum<double, TPB>(tot, tile_tot, sh.dscan);
   const double thr_max = my_lo < my_hi ? excl + maxp : kNegInf;
   double tile_max;
   const double run0 = block_exclusive_max<double, TPB>(thr_max, kNegInf, tile_max, sh.dmax);
   const bool any_neg = __syncthreads_or(neg ? 1 : 0) != 0;
+  const bool any_bad = __syncthreads_or(bad_grid ? 1 : 0) != 0;
   if (nci == 1) {
     // whole density in one tile: finalise now
     uint16_t* gd = any_neg ? nullptr : a.gl + __ldg(&a.goff[b]);
@@ -300,7 +324,8 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
     __syncthreads();
     if (threadIdx.x == 0) {
       a.norm[b] = tile_tot;
-      a.dflags[b] = any_neg ? kNonMonotone : 0u;
+      const uint32_t fl = (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u);
+      a.dflags[b] = fl | accept_all_flag(a, b, k0, G, tile_tot, fl);
       __threadfence();
       atomicAdd(&a.cdf_ready[b], 1u);
     }
@@ -309,7 +334,8 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   (void)tile_max;
   (void)run0;
   if (threadIdx.x == 0) {
-    if (any_neg) atomicOr(&a.dflags[b], kNonMonotone);
+    if (any_neg || any_bad)
+      atomicOr(&a.dflags[b], (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u));
     sh.tile_excl = cdf_lookback(a, first, ct, tile_tot);
   }
   __syncthreads();
@@ -372,8 +398,8 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   const int64_t my_lo = my_lo_raw < hi ? my_lo_raw : hi;
   const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
   double tot, maxp;
-  bool neg;
-  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg);
+  bool neg, bad_grid;
+  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg, bad_grid);
   double tile_tot;
   const double excl = block_exclusive_sum<double, TPB>(tot, tile_tot, sh.dscan);
   const double thr_max = my_lo < my_hi ? (tile_excl + excl) + maxp : kNegInf;
@@ -392,7 +418,8 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
     if (!nonmono) pack_guide<TPB>(a, b);
     __syncthreads();
     if (threadIdx.x == 0) {
-      a.dflags[b] = nonmono ? kNonMonotone : 0u;
+      const uint32_t fl = ld_acquire_u32(&a.dflags[b]) & (kNonMonotone | kBadGrid);
+      a.dflags[b] = fl | accept_all_flag(a, b, k0, G, norm, fl);
       __threadfence();
       atomicAdd(&a.cdf_ready[b], 1u);
     }
@@ -429,13 +456,14 @@ struct DensView {
   int shift;              // 32 - m: bucket of a Philox word = word >> shift
   int G;
   bool count_all;
+  bool accept_all;
   float cut;
 };
 
 struct SampleShared {
   int warp_cnt[16];
   int64_t base;
-  int nonmono;
+  uint32_t flags;
   float cut;
 };
 
@@ -446,16 +474,17 @@ __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int6
                                                  bool wait_ready, SampleShared& sh) {
   if (threadIdx.x == 0) {
     if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u)) raise_status(a.status, LOITS_ERR_TIMEOUT);
-    sh.nonmono = (ld_acquire_u32(&a.dflags[b]) & kNonMonotone) ? 1 : 0;
+    sh.flags = ld_acquire_u32(&a.dflags[b]);
     sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
   }
   __syncthreads();
+  const bool nonmono = (sh.flags & kNonMonotone) != 0;
   const int m = __ldg(&a.gbits[b]);
   for (int64_t i = threadIdx.x; i < G; i += blockDim.x) {
     rec_s[i] = __ldcg(&a.rec[k0 + i]);
     if (invd_s) invd_s[i] = __ldcg(&a.invd[k0 + i]);
   }
-  if (!sh.nonmono) {
+  if (!nonmono) {
     const uint4* src = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.goff[b]));
     uint4* dst = reinterpret_cast<uint4*>(guide_s);
     for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&src[i]);
@@ -466,7 +495,8 @@ __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int6
   v.guide = guide_s;
   v.shift = 32 - m;
   v.G = static_cast<int>(G);
-  v.count_all = sh.nonmono != 0;
+  v.count_all = nonmono;
+  v.accept_all = (sh.flags & kAcceptAll) != 0;
   v.cut = sh.cut;
   return v;
 }
@@ -481,13 +511,37 @@ struct Slot {
 __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
   const float u = uniform_from_bits(bits);
   int j;
+  float4 r;
   if (!d.count_all) {
+    // count = #{t : u >= c_t} lies in [lo, hi] (guide bucket of u); c_0 = 0,
+    // so lo >= 1.  Both candidate records are loaded at once: interval lo-1
+    // (count == lo) and knot/interval lo (count > lo); one exact compare
+    // selects.  Only a bucket holding several knots needs more compares.
     const uint32_t pk = d.guide[bits >> d.shift];
-    j = interval_in_range(d.rec, static_cast<int>(pk & 0xffffu), static_cast<int>(pk >> 16), u, d.G);
+    const int lo = static_cast<int>(pk & 0xffffu), hi = static_cast<int>(pk >> 16);
+    const int ja = max(min(lo - 1, d.G - 2), 0);
+    const float4 ra = d.rec[ja];
+    const float4 rb = d.rec[ja + 1];
+    const bool step = (lo < hi) & ge_knot(u, make_float2(rb.x, rb.y));
+    j = ja;
+    r = ra;
+    if (step) {
+      int c = lo + 1;
+      if (hi - lo >= 2) {
+        int l = c, h = hi;
+        while (l < h) {
+          const int mid = (l + h) >> 1;
+          if (ge_knot(u, hilo(d.rec, mid))) l = mid + 1; else h = mid;
+        }
+        c = l;
+      }
+      j = min(c - 1, d.G - 2);
+      r = j == ja + 1 ? rb : d.rec[j];
+    }
   } else {
     j = interval_count_all(d.rec, u, d.G);
+    r = d.rec[j];
   }
-  const float4 r = d.rec[j];
   Slot o;
   o.x = interval_value(r, u, o.t);
   o.m = r.w;
@@ -567,6 +621,66 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
   }
 }
 
+// First and one-past-last absolute slot of tile tg inside its density.
+template <int TPB, int R>
+__device__ __forceinline__ void tile_slot_range(const TileGeom& tg, int64_t& s_lo, int64_t& s_hi) {
+  const int64_t pb = tg.blk0 << 2, pe = (tg.blk0 + static_cast<int64_t>(TPB) * R) << 2;
+  const int64_t dend = tg.P0 + tg.n;
+  s_lo = pb > tg.P0 ? pb : tg.P0;
+  s_hi = pe < dend ? pe : dend;
+}
+
+// Tile of a density whose every event is kept (kAcceptAll): the tile's count
+// is its number of slots, published before any event is computed, and slot p
+// lands in row p + (base - s_lo) -- the identity compaction, no staging.
+template <int TPB, int R>
+__device__ __forceinline__ void sample_tile_all(const BatchArgs& a, int32_t t, const TileGeom& tg,
+                                                const DensView& d, SampleShared& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int64_t s_lo, s_hi;
+  tile_slot_range<TPB, R>(tg, s_lo, s_hi);
+  const int cnt = static_cast<int>(s_hi - s_lo);
+  if (warp == 0) {
+    const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(cnt), a.status);
+    if (lane == 0) {
+      sh.base = base;
+      a.tile_prefix[t] = base;
+      if (t == __ldg(&a.tile_first[tg.b])) {
+        for (int dd = __ldg(&a.rowfill_lo[tg.b]); dd <= tg.b; ++dd) a.row_offsets[dd] = base;
+      }
+      if (t == a.tiles_total - 1) {
+        for (int dd = a.last_nonempty + 1; dd <= a.nd; ++dd) a.row_offsets[dd] = base + cnt;
+      }
+    }
+  }
+  __syncthreads();
+  const int64_t shiftrow = sh.base - s_lo;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    const uint32_t range = block_range_mask(tg, blk);
+    if (!range) continue;
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+    const Slot e0 = sample_slot(d, w.x), e1 = sample_slot(d, w.y);
+    const Slot e2 = sample_slot(d, w.z), e3 = sample_slot(d, w.w);
+    const int64_t row0 = (blk << 2) + shiftrow;
+    if (range == 0xfu && (row0 & 3) == 0) {
+      __stcs(reinterpret_cast<float4*>(a.events + row0), make_float4(e0.x, e1.x, e2.x, e3.x));
+    } else {
+      if (range & 1u) a.events[row0] = e0.x;
+      if (range & 2u) a.events[row0 + 1] = e1.x;
+      if (range & 4u) a.events[row0 + 2] = e2.x;
+      if (range & 8u) a.events[row0 + 3] = e3.x;
+    }
+    if (a.intervals) {
+      if (range & 1u) a.intervals[row0] = e0.j;
+      if (range & 2u) a.intervals[row0 + 1] = e1.j;
+      if (range & 4u) a.intervals[row0 + 2] = e2.j;
+      if (range & 8u) a.intervals[row0 + 3] = e3.j;
+    }
+  }
+}
+
 template <int TPB, int R>
 __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
                                             uint32_t* guide_s, float* stage, SampleShared& sh) {
@@ -574,6 +688,10 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const TileGeom tg = tile_geom<TPB, R>(a, t);
   const DensView d = load_density(a, tg.b, tg.k0, tg.G, rec_s, guide_s, nullptr, true, sh);
+  if (d.accept_all) {
+    sample_tile_all<TPB, R>(a, t, tg, d, sh);
+    return;
+  }
   float* sw = stage + warp * (R * 128);
   int acc = 0;
 #pragma unroll 1
@@ -659,6 +777,37 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   const int G = static_cast<int>(tg.G);
   for (int i = threadIdx.x; i < G; i += TPB) gacc_s[i] = 0.0f;
   const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
+  if (d.accept_all) {
+    // identity compaction: slot p of tile t is row p + (tile_prefix[t] - s_lo)
+#pragma unroll 1
+    for (int32_t t = t_first; t < t_end; ++t) {
+      tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
+      int64_t s_lo, s_hi;
+      tile_slot_range<TPB, R>(tg, s_lo, s_hi);
+      const int64_t shiftrow = __ldcg(&a.tile_prefix[t]) - s_lo;
+#pragma unroll 1
+      for (int r = 0; r < R; ++r) {
+        const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+        const uint32_t range = block_range_mask(tg, blk);
+        if (!range) continue;
+        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+        const int64_t row0 = (blk << 2) + shiftrow;
+        float4 g4;
+        if (range == 0xfu && (row0 & 3) == 0) {
+          g4 = __ldcs(reinterpret_cast<const float4*>(a.grad + row0));
+        } else {
+          g4.x = (range & 1u) ? __ldcs(a.grad + row0) : 0.0f;
+          g4.y = (range & 2u) ? __ldcs(a.grad + row0 + 1) : 0.0f;
+          g4.z = (range & 4u) ? __ldcs(a.grad + row0 + 2) : 0.0f;
+          g4.w = (range & 8u) ? __ldcs(a.grad + row0 + 3) : 0.0f;
+        }
+        if (range & 1u) scatter_slot(sample_slot(d, w.x), g4.x, invd_s, gacc_s);
+        if (range & 2u) scatter_slot(sample_slot(d, w.y), g4.y, invd_s, gacc_s);
+        if (range & 4u) scatter_slot(sample_slot(d, w.z), g4.z, invd_s, gacc_s);
+        if (range & 8u) scatter_slot(sample_slot(d, w.w), g4.w, invd_s, gacc_s);
+      }
+    }
+  } else {
 #pragma unroll 1
   for (int32_t t = t_first; t < t_end; ++t) {
     tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
@@ -685,6 +834,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       if (keep & 8u) scatter_slot(e3, __ldcs(&a.grad[my]), invd_s, gacc_s);
       row += total;
     }
+  }
   }
   __syncthreads();
   float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;

@@ -80,6 +80,9 @@ struct BatchArgs {
   float* grad_values;
 };
 
-constexpr uint32_t kNonMonotone = 1u;
+// Per-density flags (dflags):
+constexpr uint32_t kNonMonotone = 1u;  // an area is negative/NaN: count semantics
+constexpr uint32_t kBadGrid = 2u;      // grid not ascending or not finite
+constexpr uint32_t kAcceptAll = 4u;    // every event provably kept (see accept_all_flag)
 
 }  // namespace loits_dev

@@ -1,5 +1,5 @@
 // capi.cu -- library-wide C entry points (status strings, version).
-#include "../../include/loits_b200.h"
+#include "loits_b200.h"
 
 extern "C" const char* loits_status_string(int status) {
   switch (status) {

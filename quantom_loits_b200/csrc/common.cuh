@@ -12,7 +12,7 @@
 #include <cstdint>
 #include <cuda_runtime.h>
 
-#include "../../include/loits_b200.h"
+#include "loits_b200.h"
 
 namespace loits_dev {
 

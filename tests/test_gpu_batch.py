@@ -305,3 +305,29 @@ def test_empty_and_tiny_densities(B, oracle_lib):
                                    None, 3, 1)
         assert np.array_equal(out["rows"], ref["row_offsets"]), counts
         np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+
+
+def test_identity_compaction_path_matches_general_path(B):
+    """Densities whose every event is kept (grid > 0, no effective cut) take
+    the identity-compaction path; putting the cut exactly at the first knot
+    forces the general compaction path, which may only additionally drop
+    events with x == g_0.  Both must give the same surviving rows, and the
+    same gradient for the same cotangent."""
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.uniform(scale=4e-3, n_densities=5)
+    base = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, scalars=np.array([spec.seed, 3]))
+    fast = run_batch(B, base)
+    g0 = spec.grid[spec.knot_offsets[:-1]]
+    slow = run_batch(B, dict(base, x_cut=g0.astype(np.float32)))
+    keep = np.concatenate([fast["events"][fast["rows"][b]:fast["rows"][b + 1]] > g0[b]
+                           for b in range(spec.n_densities)])
+    assert np.array_equal(fast["events"][keep], slow["events"])
+    assert np.array_equal(fast["intervals"][keep], slow["intervals"])
+    rng = np.random.default_rng(3)
+    cot = rng.standard_normal(fast["valid"]).astype(np.float32)
+    gf = run_batch(B, dict(base, cotangent=cot))["grad_values"]
+    gs = run_batch(B, dict(base, x_cut=g0.astype(np.float32), cotangent=cot[keep]))["grad_values"]
+    scale = np.abs(gf).max()
+    assert np.abs(gf - gs).max() <= GRAD_REPRO * scale
