@@ -101,6 +101,25 @@ int loits_tuple_sample(const loits_shape* shape, const double* x_bins, const dou
                        int64_t* valid, int32_t* status, void* workspace, size_t workspace_bytes,
                        void* stream);
 
+/* Allocation-free form of loits_tuple_sample.  No counterpart in the
+ * reference.  For callers that cannot allocate device memory where they
+ * sample (a framework that owns the whole GPU through its own memory pool,
+ * or a loop that must not allocate after start-up): the look-back scratch is
+ * a fixed 512 KiB array inside the library (16 B + 8 B per 1024-slot tile),
+ * so `active` may be at most LOITS_TUPLE_NOALLOC_MAX_ACTIVE (67,108,864);
+ * more returns LOITS_ERR_CAPACITY without launching.  The first call on a
+ * device looks up that array's device address (cudaGetSymbolAddress), so make
+ * it before any stream capture.  Every call on a device shares the one array
+ * and leaves its contents behind: calls that may overlap on the GPU
+ * (different streams without ordering between them) race. */
+#define LOITS_TUPLE_NOALLOC_MAX_ACTIVE 67108864
+int loits_tuple_sample_noalloc(const loits_shape* shape, const double* x_bins,
+                               const double* q_bins, const double* cdf_x, const double* cdf_q,
+                               const int64_t* cell_offsets, int64_t nmax, int64_t active,
+                               uint64_t seed, uint64_t sequence, double* events,
+                               int64_t* packed, int16_t* interval_x, int16_t* interval_q,
+                               int64_t* valid, int32_t* status, void* stream);
+
 /* Replaces the pybind backward of cpp/bindings.cpp:132-208
  * (interpolation_vjp_x/q cpp/loits_core.cpp:268-338, cdf_vjp_x/q :340-398,
  * density_vjp_x/q :400-472).  grad_events: nvalid rows of 2; packed: the

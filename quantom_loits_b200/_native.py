@@ -28,6 +28,7 @@ LOITS_ERR_CUDA = 3
 LOITS_ERR_TIMEOUT = 4
 LOITS_ERR_CAPACITY = 5
 LOITS_ERR_EPSILON = 6
+LOITS_TUPLE_NOALLOC_MAX_ACTIVE = 67108864
 
 
 class LoitsError(RuntimeError):
@@ -61,6 +62,8 @@ SIGNATURES = {
     "loits_tuple_sample_workspace": (_sz, [_i64]),
     "loits_tuple_sample": (C.c_int, [C.POINTER(Shape), _vp, _vp, _vp, _vp, _vp, _i64, _i64, _u64,
                                      _u64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
+    "loits_tuple_sample_noalloc": (C.c_int, [C.POINTER(Shape), _vp, _vp, _vp, _vp, _vp, _i64, _i64,
+                                             _u64, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "loits_tuple_backward": (C.c_int, [C.POINTER(Shape), _vp, _vp, _i64, _i64, _u64, _u64, _vp,
                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "loits_batch_plan_create": (C.c_int, [_i64, _vp, _vp, C.POINTER(BatchConfig),

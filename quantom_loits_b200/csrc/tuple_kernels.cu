@@ -22,6 +22,7 @@
 //                          deterministic (fixed-order warp reductions)
 #include <cmath>
 #include <cstdint>
+#include <mutex>
 
 #include "common.cuh"
 #include "lookback.cuh"
@@ -553,4 +554,72 @@ extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad
   if (blocks > 0x7fffffff) return LOITS_ERR_UNSUPPORTED;
   tuple_backward_kernel<<<static_cast<unsigned>(blocks), wpb * 32, smem, st>>>(a);
   return launch_status(cudaGetLastError());
+}
+
+// ============================================== allocation-free sampling call
+//
+// Some callers cannot allocate device memory at the point where they sample:
+// code running inside a framework that owns every byte of the GPU through
+// its own pool (the pool would have to hand out a buffer, and cudaMalloc
+// beside it can fail or fragment it), or real-time loops that forbid any
+// allocation after start-up.  loits_tuple_sample_noalloc serves them: the
+// only scratch loits_tuple_sample needs (a ticket counter and the look-back
+// words of its tiles) lives in the fixed array below, which is part of the
+// library image and exists on every GPU that loads the library until the
+// process exits.  The caller still passes all inputs and outputs.
+
+namespace {
+
+// 16 bytes of ticket + 8 bytes of look-back state per 1024-slot tile.
+constexpr int64_t kNoAllocMaxTiles = LOITS_TUPLE_NOALLOC_MAX_ACTIVE / kSampleTile;
+static_assert(kNoAllocMaxTiles * kSampleTile == LOITS_TUPLE_NOALLOC_MAX_ACTIVE,
+              "the limit is a whole number of tiles");
+constexpr size_t kNoAllocScratchBytes = 16 + static_cast<size_t>(kNoAllocMaxTiles) * 8;
+
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_tuple_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+// Device address of the scratch array on the current device.  In host code
+// the array's name is a host-side stand-in, not a device address, so the
+// address is looked up once per device (with that device current) and kept.
+int noalloc_scratch(void** out) {
+  int dev = -1;
+  if (cudaGetDevice(&dev) != cudaSuccess) return LOITS_ERR_CUDA;
+  if (dev < 0 || dev >= kNoAllocMaxDevices) return LOITS_ERR_UNSUPPORTED;
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_tuple_noalloc_scratch) != cudaSuccess || !p)
+      return LOITS_ERR_CUDA;
+    g_noalloc_ptr[dev] = p;
+  }
+  *out = g_noalloc_ptr[dev];
+  return LOITS_OK;
+}
+
+}  // namespace
+
+extern "C" int loits_tuple_sample_noalloc(const loits_shape* shape, const double* x_bins,
+                                          const double* q_bins, const double* cdf_x,
+                                          const double* cdf_q, const int64_t* cell_offsets,
+                                          int64_t nmax, int64_t active, uint64_t seed,
+                                          uint64_t sequence, double* events, int64_t* packed,
+                                          int16_t* interval_x, int16_t* interval_q,
+                                          int64_t* valid, int32_t* status, void* stream) {
+  if (active < 0) return LOITS_ERR_INVALID;
+  if (loits_tuple_sample_workspace(active) > kNoAllocScratchBytes) return LOITS_ERR_CAPACITY;
+  void* scratch = nullptr;
+  const int rc = noalloc_scratch(&scratch);
+  if (rc != LOITS_OK) return rc;
+  // the sampling call clears the part of the scratch that must start at zero
+  return loits_tuple_sample(shape, x_bins, q_bins, cdf_x, cdf_q, cell_offsets, nmax, active, seed,
+                            sequence, events, packed, interval_x, interval_q, valid, status,
+                            scratch, kNoAllocScratchBytes, stream);
 }
