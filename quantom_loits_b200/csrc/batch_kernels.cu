@@ -19,9 +19,9 @@
 //   3. Sampling tiles (density, run of Philox blocks): in-register Philox
 //      (rng/philox.hpp), exact search of u against the double-float CDF with
 //      fp32 compares, linear interpolation (cpp/loits_core.cpp:193-196),
-//      acceptance (finite, non-zero, x > x_cut), block scan + decoupled
+//      acceptance (finite, non-zero, x > x_cut), warp scans + decoupled
 //      look-back for a stable (density, slot) compaction, coalesced 16-byte
-//      stores through shared memory.
+//      stores from a per-CTA staging run that stays in L2.
 // Backward items:
 //   1. Chunks (density, run of sampling tiles): recompute uniforms, intervals
 //      and the compaction ranks of the forward, read the cotangents of the
@@ -103,10 +103,11 @@ __device__ __forceinline__ bool accept_event(float x, float cut) {
 
 // ------------------------------------------------------------- CDF phase
 
+template <int TPB>
 struct CdfShared {
   double dscan[33];
   double dmax[33];
-  double cfirst[512];
+  double cfirst[TPB];
   double tile_excl, norm, mprev, cnext;
   int nonmono, has_next;
 };
@@ -218,7 +219,7 @@ __device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
 template <int TPB>
 __device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_t G, int64_t hi, int64_t my_lo,
                           int64_t my_hi, double base, double run0, double norm, bool nonmono,
-                          double tile_next_c, uint16_t* gd, int m, CdfShared& sh) {
+                          double tile_next_c, uint16_t* gd, int m, CdfShared<TPB>& sh) {
   const float* g = a.grid + k0;
   const float* f = a.values + k0;
   // first knot of each thread goes to shared memory for its left neighbour
@@ -293,7 +294,7 @@ __device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first
 }
 
 template <int TPB>
-__device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared& sh) {
+__device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared<TPB>& sh) {
   const int b = find_owner(a.cdf_first, a.d_lo, a.d_hi, ct);
   const int32_t first = __ldg(&a.cdf_first[b]);
   const int32_t ci = ct - first, nci = __ldg(&a.cdf_first[b + 1]) - first;
@@ -355,7 +356,7 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
 }
 
 template <int TPB>
-__device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi, CdfShared& sh) {
+__device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi, CdfShared<TPB>& sh) {
   const int b = find_owner(a.fin_first, a.d_lo, a.d_hi, fi);
   const int32_t ci = fi - __ldg(&a.fin_first[b]);
   const int32_t first = __ldg(&a.cdf_first[b]);
@@ -461,7 +462,7 @@ struct DensView {
 };
 
 struct SampleShared {
-  int warp_cnt[16];
+  int warp_cnt[32];
   int64_t base;
   uint32_t flags;
   float cut;
@@ -574,22 +575,23 @@ __device__ __forceinline__ int warp_exclusive_count(int c, int& total) {
   return inc - c;
 }
 
-// Copy n floats src[0..n) (shared) to dst[0..n) (global), 16-byte stores where
-// dst is aligned.  One warp.
+// Copy n floats src[0..n) (the warp's staging run, L2-resident) to dst[0..n)
+// (final rows), 16-byte stores where dst is aligned.  One warp.
 __device__ __forceinline__ void warp_store(const float* __restrict__ src, float* __restrict__ dst,
                                            int n) {
   const int lane = threadIdx.x & 31;
   const int head = static_cast<int>((4 - ((reinterpret_cast<uintptr_t>(dst) >> 2) & 3)) & 3);
   const int h = head < n ? head : n;
-  if (lane < h) dst[lane] = src[lane];
+  if (lane < h) dst[lane] = __ldcg(&src[lane]);
   const int nv = (n - h) >> 2;
   float4* dv = reinterpret_cast<float4*>(dst + h);
   for (int v = lane; v < nv; v += 32) {
     const int s0 = h + 4 * v;
-    __stcs(&dv[v], make_float4(src[s0], src[s0 + 1], src[s0 + 2], src[s0 + 3]));
+    __stcs(&dv[v], make_float4(__ldcg(&src[s0]), __ldcg(&src[s0 + 1]), __ldcg(&src[s0 + 2]),
+                               __ldcg(&src[s0 + 3])));
   }
   const int tail0 = h + 4 * nv;
-  if (tail0 + lane < n) dst[tail0 + lane] = src[tail0 + lane];
+  if (tail0 + lane < n) dst[tail0 + lane] = __ldcg(&src[tail0 + lane]);
 }
 
 // Optional per-row interval output (diagnostics): recomputed for kept rows.
@@ -709,10 +711,10 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
     }
     int total;
     int pos = acc + warp_exclusive_count(__popc(keep), total);
-    if (keep & 1u) sw[pos++] = x0;
-    if (keep & 2u) sw[pos++] = x1;
-    if (keep & 4u) sw[pos++] = x2;
-    if (keep & 8u) sw[pos] = x3;
+    if (keep & 1u) __stcg(&sw[pos++], x0);
+    if (keep & 2u) __stcg(&sw[pos++], x1);
+    if (keep & 4u) __stcg(&sw[pos++], x2);
+    if (keep & 8u) __stcg(&sw[pos], x3);
     acc += total;
   }
   if (lane == 0) sh.warp_cnt[warp] = acc;
@@ -844,9 +846,10 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
 }
 
+template <int TPB>
 struct FinShared {
   double dscan[33];
-  double sfirst[512];
+  double sfirst[TPB];
   double red[33];
   double carry;
 };
@@ -854,7 +857,7 @@ struct FinShared {
 // Reverse-mode chain of density b: grad_cdf (sum of chunk partials) ->
 // suffix scan -> grad_rho -> normaliser VJP -> grad_values.
 template <int TPB>
-__device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, double* grho, FinShared& sh) {
+__device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, double* grho, FinShared<TPB>& sh) {
   const int32_t nch = __ldg(&a.chunk_first[b + 1]) - __ldg(&a.chunk_first[b]);
   const int64_t k0 = __ldg(&a.knot_off[b]);
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
@@ -937,16 +940,18 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
 
 // ---------------------------------------------------------------- kernels
 
-// Register cap: 64 per thread (65536 / (64 * TPB) CTAs) keeps four 256-thread CTAs
-// (or two 512-thread CTAs) resident per SM.
+// Register cap: 1280 threads per SM, i.e. 48 registers for five resident
+// 256-thread CTAs, 64 for two 512-thread CTAs or one 1024-thread CTA.
 template <int TPB, int R>
-__global__ void __launch_bounds__(TPB, 1024 / TPB) batch_forward_kernel(BatchArgs a) {
+__global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
   uint32_t* guide_s = reinterpret_cast<uint32_t*>(rec_s + a.gcap);
-  float* stage = reinterpret_cast<float*>(guide_s + ((a.mcap + 7) & ~7));
+  // this CTA's staging run in global memory (TPB * R * 4 floats): kept
+  // events wait there for their tile's row base; they stay in L2
+  float* stage = a.stage_g + static_cast<int64_t>(blockIdx.x) * (TPB * R * 4);
   __shared__ union {
-    CdfShared cdf;
+    CdfShared<TPB> cdf;
     SampleShared smp;
   } sh;
   __shared__ uint32_t s_item;
@@ -970,14 +975,14 @@ __global__ void __launch_bounds__(TPB, 1024 / TPB) batch_forward_kernel(BatchArg
 }
 
 template <int TPB, int R>
-__global__ void __launch_bounds__(TPB, 1024 / TPB) batch_backward_kernel(BatchArgs a, double* grho) {
+__global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchArgs a, double* grho) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
   float* invd_s = reinterpret_cast<float*>(rec_s + a.gcap);
   float* gacc_s = invd_s + a.gcap;
   uint32_t* guide_s = reinterpret_cast<uint32_t*>(gacc_s + a.gcap);
   __shared__ union {
-    FinShared fin;
+    FinShared<TPB> fin;
     SampleShared smp;
   } sh;
   __shared__ uint32_t s_item;

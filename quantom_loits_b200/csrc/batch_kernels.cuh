@@ -67,6 +67,7 @@ struct BatchArgs {
   unsigned long long* tile_state;
   int64_t* tile_prefix;        // first kept row of each sampling tile
   int32_t* warp_off;           // kept rows of earlier warps in the tile, per (tile, warp)
+  float* stage_g;              // per forward CTA: TPB * R * 4 floats of staged kept events
   uint32_t* ticket;            // this launch's ticket counter
   int32_t* status;
   uint32_t* chunks_done;       // per density

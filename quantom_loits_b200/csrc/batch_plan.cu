@@ -33,7 +33,7 @@ size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
 struct Layout {
   size_t status, tickets_fwd, dflags, cdf_ready, cdf_scanned, fin_done, cflag, tile_state;  // zeroed by forward
   size_t tickets_bwd, chunks_done;                                                // zeroed by backward
-  size_t rec, invd, gl, gpk, norm, cagg, cinc, cmax, tile_prefix, warp_off, partials, grho;
+  size_t rec, invd, gl, gpk, norm, cagg, cinc, cmax, tile_prefix, warp_off, stage, partials, grho;
   size_t fwd_zero_lo, fwd_zero_hi, bwd_zero_lo, bwd_zero_hi, total;
 };
 
@@ -85,6 +85,12 @@ bool kernels_for(int tpb, int r, FwdKernel& f, BwdKernel& b) {
       case 8: pick<512, 8>(f, b); return true;
       case 16: pick<512, 16>(f, b); return true;
     }
+  } else if (tpb == 1024) {
+    switch (r) {
+      case 2: pick<1024, 2>(f, b); return true;
+      case 4: pick<1024, 4>(f, b); return true;
+      case 8: pick<1024, 8>(f, b); return true;
+    }
   }
   return false;
 }
@@ -96,12 +102,13 @@ constexpr size_t kSmemLimit = 227 * 1024;
 int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
   out = in ? *in : loits_batch_config{};
   if (out.threads == 0) out.threads = 256;
-  if (out.blocks_per_item == 0) out.blocks_per_item = 8;
+  if (out.blocks_per_item == 0) out.blocks_per_item = out.threads == 1024 ? 8 : 16;
   if (out.scan_knots == 0) out.scan_knots = 8;
-  if (out.threads != 256 && out.threads != 512) return LOITS_ERR_INVALID;
+  if (out.threads != 256 && out.threads != 512 && out.threads != 1024) return LOITS_ERR_INVALID;
   if (out.blocks_per_item != 2 && out.blocks_per_item != 4 && out.blocks_per_item != 8 &&
       out.blocks_per_item != 16)
     return LOITS_ERR_INVALID;
+  if (out.threads == 1024 && out.blocks_per_item == 16) return LOITS_ERR_INVALID;
   if (out.scan_knots < 1 || out.scan_knots > 64) return LOITS_ERR_INVALID;
   if (out.ctas_per_sm < 0 || out.ctas_per_sm > 32) return LOITS_ERR_INVALID;
   if (out.plain != 0 && out.plain != 1) return LOITS_ERR_INVALID;
@@ -152,6 +159,7 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.tile_state = carve<unsigned long long>(ws, L.tile_state);
   a.tile_prefix = carve<int64_t>(ws, L.tile_prefix);
   a.warp_off = carve<int32_t>(ws, L.warp_off);
+  a.stage_g = carve<float>(ws, L.stage);
   a.status = carve<int32_t>(ws, L.status);
   a.chunks_done = carve<uint32_t>(ws, L.chunks_done);
   a.partials = carve<float>(ws, L.partials);
@@ -239,36 +247,53 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   // multiple of 4 so that every shared-memory array after the records stays
   // 16-byte aligned (float4 staging)
   p->gcap = static_cast<int32_t>((p->max_g + 3) & ~int64_t(3));
-  // guide tables: M = 2^m buckets per density, 2G <= M < 4G (4 <= M <=
-  // 2^14), kept as M + 1 uint16 counts and as M packed uint32 pairs; both
-  // arrays use the same entry offsets
+  // ---- launch geometry
+  FwdKernel fk;
+  BwdKernel bk;
+  kernels_for(p->tpb, p->r, fk, bk);
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
+  cudaFuncAttributes fattr{}, battr{};
+  if (cudaFuncGetAttributes(&fattr, fk) != cudaSuccess ||
+      cudaFuncGetAttributes(&battr, bk) != cudaSuccess) {
+    delete p;
+    return LOITS_ERR_CUDA;
+  }
+  const size_t static_smem = std::max(fattr.sharedSizeBytes, battr.sharedSizeBytes);
+  // a backward CTA holds per knot a record, a weight and a gradient slot (24
+  // bytes) plus the density's guide
+  const size_t knot_bytes = static_cast<size_t>(p->gcap) * (sizeof(float4) + 2 * sizeof(float));
+  if (knot_bytes + static_smem + 64 * sizeof(uint32_t) > kSmemLimit) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  // guide tables: M = 2^m buckets per density, 2G <= M < 4G, at most 2^14 and
+  // at most what shared memory leaves beside the records (a smaller guide
+  // only widens buckets: the search finishes them exactly); kept as M + 1
+  // uint16 counts and as M packed uint32 pairs at the same entry offsets
+  int m_cap = 14;
+  while (m_cap > 2 &&
+         knot_bytes + static_smem + (size_t(1) << m_cap) * sizeof(uint32_t) > kSmemLimit)
+    --m_cap;
   p->gbits.resize(n_densities);
   p->goff.resize(n_densities);
   int64_t go = 0;
   for (int64_t b = 0; b < n_densities; ++b) {
     const int64_t g = p->koff[b + 1] - p->koff[b];
     int m = 2;
-    while ((int64_t(1) << m) < 2 * g && m < 14) ++m;
+    while ((int64_t(1) << m) < 2 * g && m < m_cap) ++m;
     p->gbits[b] = m;
     p->goff[b] = go;
     go += ((int64_t(1) << m) + 1 + 7) & ~int64_t(7);
     p->mcap = std::max<int32_t>(p->mcap, static_cast<int32_t>(int64_t(1) << m));
   }
   p->total_guide = go;
-
-  // ---- launch geometry
-  FwdKernel fk;
-  BwdKernel bk;
-  kernels_for(p->tpb, p->r, fk, bk);
-  const int64_t tile_events = blocks_per_tile * 4;
-  // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32
+  // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
+  // kept events are staged in global memory, not here
   const size_t guide_bytes = static_cast<size_t>((p->mcap + 7) & ~7) * sizeof(uint32_t);
-  p->fwd_smem = static_cast<size_t>(p->gcap) * sizeof(float4) + guide_bytes +
-                (tile_events + 4) * sizeof(float);
-  p->bwd_smem = static_cast<size_t>(p->gcap) * (sizeof(float4) + 2 * sizeof(float)) + guide_bytes;
-  if (p->fwd_smem > kSmemLimit || p->bwd_smem > kSmemLimit) { delete p; return LOITS_ERR_UNSUPPORTED; }
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
+  p->fwd_smem = static_cast<size_t>(p->gcap) * sizeof(float4) + guide_bytes;
+  p->bwd_smem = knot_bytes + guide_bytes;
+  if (p->fwd_smem + static_smem > kSmemLimit || p->bwd_smem + static_smem > kSmemLimit) {
+    delete p;
+    return LOITS_ERR_UNSUPPORTED;
+  }
   cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
   if (cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            static_cast<int>(std::max<size_t>(p->fwd_smem, 1))) != cudaSuccess ||
@@ -285,6 +310,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
     occ_f = std::min(occ_f, static_cast<int>(c.ctas_per_sm));
     occ_b = std::min(occ_b, static_cast<int>(c.ctas_per_sm));
   }
+  const int64_t tile_events = blocks_per_tile * 4;
   const int64_t items_f = nc + nf + nt;
   p->fwd_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items_f, int64_t(occ_f) * p->num_sms)));
   const int64_t resident_b = int64_t(occ_b) * p->num_sms;
@@ -338,6 +364,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   L.cmax = o; o = align_up(o + static_cast<size_t>(nc) * 8);
   L.tile_prefix = o; o = align_up(o + static_cast<size_t>(nt) * 8);
   L.warp_off = o; o = align_up(o + static_cast<size_t>(nt) * (p->tpb / 32) * 4);
+  L.stage = o; o = align_up(o + static_cast<size_t>(p->fwd_grid) * tile_events * 4);
   L.partials = o; o = align_up(o + static_cast<size_t>(po) * 4);
   L.grho = o; o = align_up(o + static_cast<size_t>(p->total_knots) * 8);
   L.total = o;

@@ -140,7 +140,8 @@ def test_plain_and_persistent_forms_agree(B, golden):
 
 
 @pytest.mark.parametrize("threads,blocks,scan", [(256, 2, 1), (256, 2, 3), (512, 4, 8),
-                                                 (512, 8, 16), (256, 16, 64)])
+                                                 (512, 8, 16), (256, 16, 64), (1024, 2, 1),
+                                                 (1024, 8, 4)])
 def test_launch_geometries_agree(B, golden, threads, blocks, scan):
     c = golden_case(golden, "ragged_small")
     a = run_batch(B, c)
@@ -331,3 +332,39 @@ def test_identity_compaction_path_matches_general_path(B):
     gs = run_batch(B, dict(base, x_cut=g0.astype(np.float32), cotangent=cot[keep]))["grad_values"]
     scale = np.abs(gf).max()
     assert np.abs(gf - gs).max() <= GRAD_REPRO * scale
+
+
+@pytest.mark.parametrize("threads", [256, 1024])
+def test_large_knot_densities_match_oracle(B, oracle_lib, threads):
+    """Densities of up to 8192 knots (the most a sampling CTA holds), where
+    shared memory caps the guide table below 2G buckets so buckets hold several
+    knots, with a cut: rows exact, events and gradients against the fp64
+    oracle, intervals exact except next to a knot."""
+    rng = np.random.default_rng(21)
+    sizes = [8192, 5001, 8191, 64]
+    grids, vals = [], []
+    for g in sizes:
+        x = np.linspace(1e-3, 1.0, g, dtype=np.float32)
+        a, b = rng.uniform(-0.5, 1.0), rng.uniform(1.0, 5.0)
+        grids.append(x)
+        vals.append((np.power(x.astype(np.float64), a) * np.power(1.0 - x, b)).astype(np.float32))
+    koff = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    counts = np.array([60_000, 25_000, 40_000, 3_000], dtype=np.int64)
+    x_cut = rng.uniform(0.01, 0.1, len(sizes)).astype(np.float32)
+    grid, values = np.concatenate(grids), np.concatenate(vals)
+    eoff = np.concatenate([[0], np.cumsum(counts)])
+    ref = oracle_lib.d_forward(koff, eoff, grid, values, x_cut, 99, 2)
+    cot = rng.standard_normal(len(ref["events"])).astype(np.float32)
+    case = dict(knot_offsets=koff, event_counts=counts, grid=grid, values=values, x_cut=x_cut,
+                scalars=np.array([99, 2]), cotangent=cot)
+    out = run_batch(B, case, B.make_config(threads=threads))
+    assert np.array_equal(out["rows"], ref["row_offsets"])
+    np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+    for r in np.flatnonzero(out["intervals"] != ref["intervals"]):
+        b = np.searchsorted(ref["row_offsets"], r, side="right") - 1
+        assert near_knot(ref["u"][r:r + 1], ref["cdf"][koff[b]:koff[b + 1]])[0], r
+    gref = oracle_lib.d_backward(koff, eoff, grid, values, x_cut, 99, 2, cot, fwd=ref)
+    for b in range(len(sizes)):
+        o, e = koff[b], koff[b + 1]
+        scale = np.abs(gref[o:e]).max()
+        assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b
