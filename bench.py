@@ -16,6 +16,11 @@ Arms:
                     from the reference sources) on the host cores, on the exact
                     embedding of the same workload, a bounded sample per step.
 
+Before timing, the launch geometry (threads per CTA, Philox blocks per thread,
+CDF scan width) is tuned on the workload itself by timing each candidate
+(quantom_loits_b200.tuning; untimed, reported as config.tuning_ms_per_step);
+--no-tune keeps the plan's default (CTA size by occupancy).
+
 Under torchrun each rank (one GPU) samples its own 64 densities of a global
 batch (density_base = rank * 64, same Philox slot stride): weak scaling, no
 collective on the data path; the step time is the max over ranks.
@@ -40,7 +45,7 @@ METRIC = "fwd+VJP events/s on 1 B200 (batched vs plain), %HBM peak, CDF err vs F
 PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "traffic.json"
 FALLBACK_HBM_GBS = 6650.0
-# algorithmic bytes per event: the forward writes the event (4 B), the VJP
+# algorithmic bytes per kept event: the forward writes the event (4 B), the VJP
 # reads its cotangent (4 B); per knot the forward reads grid + value (8 B), the
 # VJP reads them again and writes the gradient (12 B)
 FWD_B_PER_EVENT, BWD_B_PER_EVENT = 4, 4
@@ -196,8 +201,18 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     nmax = int(spec.event_counts.max())
-    cfg = B.make_config(threads=args.threads, blocks_per_item=args.blocks,
-                        density_base=rank * spec.n_densities, slot_stride=nmax)
+    # launch geometry: tuned on this rank's batch (untimed), unless given
+    geom = dict(threads=args.threads, blocks_per_item=args.blocks, scan_knots=0)
+    tune_ms = None
+    if not args.no_tune and args.threads == 0 and args.blocks == 0:
+        from quantom_loits_b200.tuning import Autotuner
+
+        tbatch = B.DensityBatch.from_spec(spec, dev)
+        best, tune_ms = Autotuner(dev).tune(tbatch, spec.event_counts, spec.seed, 0)
+        geom.update(best)
+        del tbatch
+    args.geom = geom
+    cfg = B.make_config(**geom, density_base=rank * spec.n_densities, slot_stride=nmax)
     plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev)
     step = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None)
     step.grid.copy_(torch.from_numpy(spec.grid))
@@ -255,8 +270,8 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     valid = int(step.row_offsets[-1].item())
 
     # ---- plain form: one launch per density for forward and for backward
-    plain_cfg = B.make_config(threads=args.threads, blocks_per_item=args.blocks, plain=1,
-                              density_base=rank * spec.n_densities, slot_stride=nmax)
+    plain_cfg = B.make_config(**geom, plain=1, density_base=rank * spec.n_densities,
+                              slot_stride=nmax)
     pplan = B.BatchPlan(spec.knot_offsets, spec.event_counts, plain_cfg, dev)
     pstep = B.BatchStep(pplan, seed=spec.seed, with_cut=spec.x_cut is not None)
     pstep.grid.copy_(step.grid); pstep.values.copy_(step.values)
@@ -287,8 +302,8 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     # ---- roofline of the dominant kernel
     f_ms, b_ms = float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
     knots = spec.total_knots
-    fwd_bytes = FWD_B_PER_EVENT * spec.total_events + FWD_B_PER_KNOT * knots
-    bwd_bytes = BWD_B_PER_EVENT * spec.total_events + BWD_B_PER_KNOT * knots
+    fwd_bytes = FWD_B_PER_EVENT * valid + FWD_B_PER_KNOT * knots
+    bwd_bytes = BWD_B_PER_EVENT * valid + BWD_B_PER_KNOT * knots
     kname, k_ms, k_bytes = (("batch_forward_kernel", f_ms, fwd_bytes) if f_ms >= b_ms
                             else ("batch_backward_kernel", b_ms, bwd_bytes))
     peak, peak_kind = hbm_peak()
@@ -298,7 +313,8 @@ def run_b200(args, spec, rank, world, dist) -> dict:
         t = json.loads(TRAFFIC.read_text())
         entry = t.get(spec.name, {}).get(kname)
         if entry:
-            traffic = entry["bytes_per_event"] * spec.total_events
+            # measured on this workload; scaled by kept events if they differ
+            traffic = entry["bytes_per_launch"] * valid / entry["kept_events"]
     except Exception:
         pass
     cdf_err = cdf_error(plan, step, spec) if rank == 0 else None
@@ -310,9 +326,12 @@ def run_b200(args, spec, rank, world, dist) -> dict:
         "dtype": "f32", "data": "synthetic",
         "config": {**describe(spec), "form": "persistent forward + backward, one CUDA graph",
                    "parallelism": f"density-sharded x{world} (no collective on the data path)",
-                   "l2": "per step 256 MB of events written and 256 MB of cotangents read, "
-                         "both larger than the 126 MB L2 (no flush)",
-                   "launch": plan.config, "accepted_events_per_step": valid * world},
+                   "l2": f"per step {4 * valid / 1e6:.0f} MB of events written and "
+                         f"{4 * valid / 1e6:.0f} MB of cotangents read, each larger than the "
+                         "126 MB L2 (no flush)" if 4 * valid > 126e6 else
+                         "inputs smaller than L2: not a valid roofline case",
+                   "launch": plan.config, "accepted_events_per_step": valid * world,
+                   "tuning_ms_per_step": tune_ms},
         "plain": {"value": plain_value, "ms_per_step": plain_ms,
                   "form": "one forward + one backward launch per density, no graph",
                   "batched_over_plain": value / plain_value, "events_identical": bool(same)},
@@ -352,8 +371,7 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
 
     nmax = int(spec.event_counts.max())
     sampler = B.BatchedLOITS(dev, seed=spec.seed,
-                             config=B.make_config(threads=args.threads,
-                                                  blocks_per_item=args.blocks,
+                             config=B.make_config(**args.geom,
                                                   density_base=rank * spec.n_densities,
                                                   slot_stride=nmax))
     h_vals = torch.from_numpy(spec.values).pin_memory()
@@ -429,6 +447,8 @@ def main(argv=None) -> int:
     ap.add_argument("--ref-seconds", type=float, default=3.0,
                     help="CPU seconds per reference step (bounded sample)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-tune", action="store_true",
+                    help="use the plan's default launch geometry instead of tuning it")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -227,7 +227,11 @@ class BatchedLOITS:
 
     events: fp32 (valid,) in (density, slot) order; row_offsets: int64 (B+1),
     kept rows of density b are [row_offsets[b], row_offsets[b+1]).  Gradients
-    flow to ``batch.values``.  Plans are cached per batch shape."""
+    flow to ``batch.values``.  Plans are cached per batch shape.
+
+    ``config``: None (the plan's defaults: CTA size by occupancy), a
+    ``loits_batch_config`` / dict, or ``"auto"``: the launch geometry is timed
+    on the first batch of each shape bucket (:mod:`quantom_loits_b200.tuning`)."""
 
     def __init__(self, device="cuda", seed=None, config=None):
         self.device = torch.device(device)
@@ -237,11 +241,19 @@ class BatchedLOITS:
         self.sequence = 0
         self._plans: dict = {}
 
-    def plan_for(self, knot_offsets, event_counts) -> BatchPlan:
+    def plan_for(self, knot_offsets, event_counts, batch=None) -> BatchPlan:
         key = (knot_offsets.tobytes(), event_counts.tobytes())
         plan = self._plans.get(key)
         if plan is None:
-            plan = BatchPlan(knot_offsets, event_counts, self.config, self.device)
+            config = self.config
+            if isinstance(config, str):
+                if config != "auto" or batch is None:
+                    raise ValueError(f"unknown config {config!r} (expected 'auto')")
+                from .tuning import default_tuner
+
+                config = make_config(**default_tuner(self.device).config_for(
+                    batch, event_counts, self.seed, self.sequence))
+            plan = BatchPlan(knot_offsets, event_counts, config, self.device)
             self._plans[key] = plan
         return plan
 
@@ -255,7 +267,7 @@ class BatchedLOITS:
         if sequence is None:
             sequence = self.sequence
             self.sequence += 1
-        plan = self.plan_for(batch.knot_offsets, counts)
+        plan = self.plan_for(batch.knot_offsets, counts, batch)
         grid = batch.grid.detach().contiguous()
         x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
         return _BatchFunction.apply(batch.values, grid, x_cut, plan, self.seed, sequence)

@@ -3,6 +3,7 @@
 #include <algorithm>
 #include <cstdint>
 #include <cstring>
+#include <mutex>
 #include <new>
 #include <vector>
 
@@ -99,20 +100,118 @@ bool kernels_for(int tpb, int r, FwdKernel& f, BwdKernel& b) {
 constexpr int64_t kMaxSmemKnots = 8192;
 constexpr size_t kSmemLimit = 227 * 1024;
 
+int default_blocks(int threads) { return threads == 1024 ? 8 : 16; }
+
+// Validates a configuration; threads == 0 (choose by occupancy) and
+// blocks_per_item == 0 (default for the thread count) stay unresolved.
 int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
   out = in ? *in : loits_batch_config{};
-  if (out.threads == 0) out.threads = 256;
-  if (out.blocks_per_item == 0) out.blocks_per_item = out.threads == 1024 ? 8 : 16;
   if (out.scan_knots == 0) out.scan_knots = 8;
-  if (out.threads != 256 && out.threads != 512 && out.threads != 1024) return LOITS_ERR_INVALID;
-  if (out.blocks_per_item != 2 && out.blocks_per_item != 4 && out.blocks_per_item != 8 &&
-      out.blocks_per_item != 16)
+  if (out.threads != 0 && out.threads != 256 && out.threads != 512 && out.threads != 1024)
+    return LOITS_ERR_INVALID;
+  if (out.blocks_per_item != 0 && out.blocks_per_item != 2 && out.blocks_per_item != 4 &&
+      out.blocks_per_item != 8 && out.blocks_per_item != 16)
     return LOITS_ERR_INVALID;
   if (out.threads == 1024 && out.blocks_per_item == 16) return LOITS_ERR_INVALID;
   if (out.scan_knots < 1 || out.scan_knots > 64) return LOITS_ERR_INVALID;
   if (out.ctas_per_sm < 0 || out.ctas_per_sm > 32) return LOITS_ERR_INVALID;
   if (out.plain != 0 && out.plain != 1) return LOITS_ERR_INVALID;
   if (out.density_base < 0 || out.slot_stride < 0) return LOITS_ERR_INVALID;
+  return LOITS_OK;
+}
+
+// Raise a kernel's dynamic shared-memory limit to at least `bytes`.  The
+// limit is a property of the function shared by every plan, so it only ever
+// grows: a plan built later with smaller densities must not lower it below
+// what an earlier plan launches with.
+bool allow_dynamic_smem(const void* fn, size_t bytes) {
+  static std::mutex mu;
+  std::lock_guard<std::mutex> lock(mu);
+  cudaFuncAttributes now{};
+  if (cudaFuncGetAttributes(&now, fn) != cudaSuccess) return false;
+  if (static_cast<size_t>(now.maxDynamicSharedSizeBytes) >= bytes) return true;
+  return cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                              static_cast<int>(bytes)) == cudaSuccess;
+}
+
+// Shared memory of the sampling kernels of (tpb, r) for densities of at most
+// max_g knots (gcap rounded to 4): the guide cap m_cap, the largest guide
+// (mcap entries) and the dynamic bytes of the forward and backward CTAs.
+struct SmemGeometry {
+  int m_cap = 2;
+  int32_t mcap = 0;
+  size_t static_smem = 0, fwd = 0, bwd = 0;
+};
+
+int smem_geometry(int tpb, int r, int32_t gcap, int64_t max_g, SmemGeometry& g) {
+  FwdKernel fk;
+  BwdKernel bk;
+  if (!kernels_for(tpb, r, fk, bk)) return LOITS_ERR_INVALID;
+  cudaFuncAttributes fattr{}, battr{};
+  if (cudaFuncGetAttributes(&fattr, fk) != cudaSuccess ||
+      cudaFuncGetAttributes(&battr, bk) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  g.static_smem = std::max(fattr.sharedSizeBytes, battr.sharedSizeBytes);
+  // a backward CTA holds per knot a record, a weight and a gradient slot (24
+  // bytes) plus the density's guide
+  const size_t knot_bytes = static_cast<size_t>(gcap) * (sizeof(float4) + 2 * sizeof(float));
+  if (knot_bytes + g.static_smem + 64 * sizeof(uint32_t) > kSmemLimit) return LOITS_ERR_UNSUPPORTED;
+  // guide tables: M = 2^m buckets per density, 2G <= M < 4G, at most 2^14 and
+  // at most what shared memory leaves beside the records (a smaller guide
+  // only widens buckets: the search finishes them exactly)
+  g.m_cap = 14;
+  while (g.m_cap > 2 &&
+         knot_bytes + g.static_smem + (size_t(1) << g.m_cap) * sizeof(uint32_t) > kSmemLimit)
+    --g.m_cap;
+  int m = 2;
+  while ((int64_t(1) << m) < 2 * max_g && m < g.m_cap) ++m;
+  g.mcap = static_cast<int32_t>(int64_t(1) << m);
+  // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
+  // kept events are staged in global memory, not here
+  const size_t guide_bytes = static_cast<size_t>((g.mcap + 7) & ~7) * sizeof(uint32_t);
+  g.fwd = static_cast<size_t>(gcap) * sizeof(float4) + guide_bytes;
+  g.bwd = knot_bytes + guide_bytes;
+  if (g.fwd + g.static_smem > kSmemLimit || g.bwd + g.static_smem > kSmemLimit)
+    return LOITS_ERR_UNSUPPORTED;
+  if (!allow_dynamic_smem(reinterpret_cast<const void*>(fk), g.fwd) ||
+      !allow_dynamic_smem(reinterpret_cast<const void*>(bk), g.bwd))
+    return LOITS_ERR_CUDA;
+  return LOITS_OK;
+}
+
+// Resident CTAs per SM of the forward and backward kernels of (tpb, r).
+void occupancy(int tpb, int r, const SmemGeometry& g, int& occ_f, int& occ_b) {
+  FwdKernel fk;
+  BwdKernel bk;
+  occ_f = occ_b = 0;
+  if (!kernels_for(tpb, r, fk, bk)) return;
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fk, tpb, g.fwd);
+  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, bk, tpb, g.bwd);
+}
+
+// CTA size with the most resident threads per SM for both kernels (the
+// smaller CTA on a tie: fewer threads wait at each tile barrier).
+int choose_threads(int r_req, int32_t gcap, int64_t max_g, int& tpb_out) {
+  int best = -1, best_tpb = 0, last_rc = LOITS_ERR_UNSUPPORTED;
+  for (int tpb : {256, 512, 1024}) {
+    const int r = r_req ? r_req : default_blocks(tpb);
+    if (tpb == 1024 && r == 16) continue;
+    SmemGeometry g;
+    const int rc = smem_geometry(tpb, r, gcap, max_g, g);
+    if (rc != LOITS_OK) {
+      last_rc = rc;
+      continue;
+    }
+    int of = 0, ob = 0;
+    occupancy(tpb, r, g, of, ob);
+    const int resident = tpb * std::min(of, ob);
+    if (resident > best) {
+      best = resident;
+      best_tpb = tpb;
+    }
+  }
+  if (best <= 0) return last_rc == LOITS_OK ? LOITS_ERR_UNSUPPORTED : last_rc;
+  tpb_out = best_tpb;
   return LOITS_OK;
 }
 
@@ -183,9 +282,6 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   auto* p = new (std::nothrow) loits_batch_plan();
   if (!p) return LOITS_ERR_INVALID;
   p->nd = n_densities;
-  p->cfg = c;
-  p->tpb = c.threads;
-  p->r = c.blocks_per_item;
   p->scan_knots = c.scan_knots;
   p->koff.assign(knot_offsets, knot_offsets + n_densities + 1);
   p->nev.assign(event_counts, event_counts + n_densities);
@@ -209,6 +305,23 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
     delete p;
     return LOITS_ERR_UNSUPPORTED;
   }
+  // multiple of 4 so that every shared-memory array after the records stays
+  // 16-byte aligned
+  p->gcap = static_cast<int32_t>((p->max_g + 3) & ~int64_t(3));
+  // ---- launch geometry: the CTA size (by occupancy unless given)
+  if (c.threads == 0) {
+    int tpb = 0;
+    rc = choose_threads(c.blocks_per_item, p->gcap, p->max_g, tpb);
+    if (rc != LOITS_OK) { delete p; return rc; }
+    c.threads = tpb;
+  }
+  if (c.blocks_per_item == 0) c.blocks_per_item = default_blocks(c.threads);
+  p->cfg = c;
+  p->tpb = c.threads;
+  p->r = c.blocks_per_item;
+  SmemGeometry sg;
+  rc = smem_geometry(p->tpb, p->r, p->gcap, p->max_g, sg);
+  if (rc != LOITS_OK) { delete p; return rc; }
   // ---- work items
   const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;
   const int64_t kt = static_cast<int64_t>(p->tpb) * p->scan_knots;
@@ -244,67 +357,28 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->n_tiles = static_cast<int32_t>(nt);
   p->n_cdf = static_cast<int32_t>(nc);
   p->n_fin = static_cast<int32_t>(nf);
-  // multiple of 4 so that every shared-memory array after the records stays
-  // 16-byte aligned (float4 staging)
-  p->gcap = static_cast<int32_t>((p->max_g + 3) & ~int64_t(3));
-  // ---- launch geometry
-  FwdKernel fk;
-  BwdKernel bk;
-  kernels_for(p->tpb, p->r, fk, bk);
-  int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
-  cudaFuncAttributes fattr{}, battr{};
-  if (cudaFuncGetAttributes(&fattr, fk) != cudaSuccess ||
-      cudaFuncGetAttributes(&battr, bk) != cudaSuccess) {
-    delete p;
-    return LOITS_ERR_CUDA;
-  }
-  const size_t static_smem = std::max(fattr.sharedSizeBytes, battr.sharedSizeBytes);
-  // a backward CTA holds per knot a record, a weight and a gradient slot (24
-  // bytes) plus the density's guide
-  const size_t knot_bytes = static_cast<size_t>(p->gcap) * (sizeof(float4) + 2 * sizeof(float));
-  if (knot_bytes + static_smem + 64 * sizeof(uint32_t) > kSmemLimit) { delete p; return LOITS_ERR_UNSUPPORTED; }
-  // guide tables: M = 2^m buckets per density, 2G <= M < 4G, at most 2^14 and
-  // at most what shared memory leaves beside the records (a smaller guide
-  // only widens buckets: the search finishes them exactly); kept as M + 1
-  // uint16 counts and as M packed uint32 pairs at the same entry offsets
-  int m_cap = 14;
-  while (m_cap > 2 &&
-         knot_bytes + static_smem + (size_t(1) << m_cap) * sizeof(uint32_t) > kSmemLimit)
-    --m_cap;
+  // guide tables, M + 1 uint16 counts and M packed uint32 pairs per density
+  // at the same entry offsets
   p->gbits.resize(n_densities);
   p->goff.resize(n_densities);
   int64_t go = 0;
   for (int64_t b = 0; b < n_densities; ++b) {
     const int64_t g = p->koff[b + 1] - p->koff[b];
     int m = 2;
-    while ((int64_t(1) << m) < 2 * g && m < m_cap) ++m;
+    while ((int64_t(1) << m) < 2 * g && m < sg.m_cap) ++m;
     p->gbits[b] = m;
     p->goff[b] = go;
     go += ((int64_t(1) << m) + 1 + 7) & ~int64_t(7);
     p->mcap = std::max<int32_t>(p->mcap, static_cast<int32_t>(int64_t(1) << m));
   }
   p->total_guide = go;
-  // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
-  // kept events are staged in global memory, not here
-  const size_t guide_bytes = static_cast<size_t>((p->mcap + 7) & ~7) * sizeof(uint32_t);
-  p->fwd_smem = static_cast<size_t>(p->gcap) * sizeof(float4) + guide_bytes;
-  p->bwd_smem = knot_bytes + guide_bytes;
-  if (p->fwd_smem + static_smem > kSmemLimit || p->bwd_smem + static_smem > kSmemLimit) {
-    delete p;
-    return LOITS_ERR_UNSUPPORTED;
-  }
+  p->fwd_smem = sg.fwd;
+  p->bwd_smem = sg.bwd;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
   cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
-  if (cudaFuncSetAttribute(fk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(std::max<size_t>(p->fwd_smem, 1))) != cudaSuccess ||
-      cudaFuncSetAttribute(bk, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           static_cast<int>(std::max<size_t>(p->bwd_smem, 1))) != cudaSuccess) {
-    delete p;
-    return LOITS_ERR_CUDA;
-  }
   int occ_f = 0, occ_b = 0;
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fk, p->tpb, p->fwd_smem);
-  cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, bk, p->tpb, p->bwd_smem);
+  occupancy(p->tpb, p->r, sg, occ_f, occ_b);
   if (occ_f < 1 || occ_b < 1) { delete p; return LOITS_ERR_UNSUPPORTED; }
   if (c.ctas_per_sm > 0) {
     occ_f = std::min(occ_f, static_cast<int>(c.ctas_per_sm));

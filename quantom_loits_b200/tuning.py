@@ -1,0 +1,164 @@
+"""Launch-geometry autotuner for the batched sampler.
+
+The batched kernels take three launch parameters (``loits_batch_config``):
+threads per CTA (256, 512, 1024), Philox blocks per thread per sampling tile
+(2, 4, 8, 16; at most 8 with 1024 threads) and knots per thread in the CDF
+scan.  Which is fastest depends on the batch: the largest density decides
+how much shared memory a CTA holds (hence how many CTAs fit on an SM), the
+event counts decide how many tiles there are to balance, and the cut decides
+whether the identity compaction applies.  Without tuning, the plan picks the
+CTA size with the most resident threads per SM.
+
+:class:`Autotuner` times forward + backward of each candidate on the caller's
+own batch (values, grid, cut; a fixed cotangent) with CUDA events and keeps
+the fastest, per shape bucket: (log2 densities, log2 largest knot count,
+log2 total events, cut or not).  Every candidate samples the same events (the
+configuration changes only the launch geometry), so tuning never changes
+results beyond the backward's fp32 accumulation order.  Results can be kept
+in a JSON file (``cache_path`` or the ``LOITS_TUNE_CACHE`` environment
+variable) so later processes skip the timing.
+"""
+from __future__ import annotations
+
+import json
+import math
+import os
+import threading
+from pathlib import Path
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+# (threads, blocks_per_item, scan_knots)
+CANDIDATES = (
+    (256, 16, 8), (256, 8, 8), (256, 4, 8),
+    (512, 16, 8), (512, 8, 8),
+    (1024, 8, 8), (1024, 4, 8), (1024, 8, 16),
+)
+
+
+def shape_key(knot_offsets, event_counts, has_cut: bool) -> str:
+    """Shape bucket of a batch: densities, largest knot count and total
+    events rounded up to powers of two, and whether a cut is applied."""
+    koff = np.asarray(knot_offsets, dtype=np.int64)
+    counts = np.asarray(event_counts, dtype=np.int64)
+    g = int(np.diff(koff).max())
+    n = int(counts.sum())
+    lg = lambda v: int(math.ceil(math.log2(max(int(v), 1))))  # noqa: E731
+    return f"d{lg(len(counts))}-g{lg(g)}-n{lg(n)}-{'cut' if has_cut else 'all'}"
+
+
+class Autotuner:
+    """Chooses (threads, blocks_per_item, scan_knots) per shape bucket by
+    timing forward + backward on the batch being sampled."""
+
+    def __init__(self, device="cuda", candidates=CANDIDATES, reps: int = 3,
+                 cache_path: str | os.PathLike | None = None):
+        self.device = torch.device(device)
+        self.candidates = tuple(candidates)
+        self.reps = max(1, int(reps))
+        path = cache_path if cache_path is not None else os.environ.get("LOITS_TUNE_CACHE")
+        self.cache_path = Path(path) if path else None
+        self._lock = threading.Lock()
+        self.table: dict[str, dict] = {}
+        self.timings: dict[str, dict] = {}
+        if self.cache_path is not None and self.cache_path.exists():
+            try:
+                self.table.update(json.loads(self.cache_path.read_text()))
+            except (OSError, ValueError):
+                pass
+
+    def config_for(self, batch, event_counts=None, seed: int = 0, sequence: int = 0) -> dict:
+        """The tuned configuration (a dict for ``make_config``) for this
+        batch's shape bucket, timing the candidates on first use."""
+        counts = batch.event_counts if event_counts is None else np.asarray(event_counts, np.int64)
+        key = shape_key(batch.knot_offsets, counts, batch.x_cut is not None)
+        with self._lock:
+            hit = self.table.get(key)
+        if hit is not None:
+            return dict(hit)
+        best, times = self.tune(batch, counts, seed, sequence)
+        with self._lock:
+            self.table[key] = best
+            self.timings[key] = times
+            self._save()
+        return dict(best)
+
+    def tune(self, batch, event_counts, seed: int = 0, sequence: int = 0):
+        """Time every candidate; returns (best config dict, {label: ms})."""
+        from .batched import BatchPlan, make_config
+
+        grid = batch.grid.detach().contiguous()
+        values = batch.values.detach().contiguous()
+        x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
+        counts = np.asarray(event_counts, dtype=np.int64)
+        capacity = int(counts.sum())
+        gen = torch.Generator(device=self.device).manual_seed(0)
+        cot = torch.randn(max(capacity, 4), generator=gen, device=self.device, dtype=torch.float32)
+        grad_values = torch.empty_like(values)
+        stream = torch.cuda.current_stream(self.device)
+        times: dict[str, float] = {}
+        best, best_ms = None, math.inf
+        for threads, blocks, scan in self.candidates:
+            label = f"{threads}x{blocks}/{scan}"
+            try:
+                plan = BatchPlan(batch.knot_offsets, counts,
+                                 make_config(threads=threads, blocks_per_item=blocks,
+                                             scan_knots=scan), self.device)
+            except RuntimeError:
+                continue  # geometry not supported for this shape (shared memory)
+            events, rows, ws = plan.new_events(), plan.new_row_offsets(), plan.new_workspace()
+
+            def step():
+                plan.forward(grid, values, x_cut, seed, sequence, events, rows, ws)
+                plan.backward(grid, values, x_cut, seed, sequence, cot, grad_values, ws)
+
+            step()
+            torch.cuda.synchronize(self.device)
+            plan.check_status(ws)
+            t0 = torch.cuda.Event(enable_timing=True)
+            t1 = torch.cuda.Event(enable_timing=True)
+            samples = []
+            for _ in range(self.reps):
+                t0.record(stream)
+                step()
+                t1.record(stream)
+                t1.synchronize()
+                samples.append(t0.elapsed_time(t1))
+            plan.check_status(ws)
+            ms = float(np.median(samples))
+            times[label] = ms
+            if ms < best_ms:
+                best_ms = ms
+                best = dict(threads=threads, blocks_per_item=blocks, scan_knots=scan)
+            del plan, events, rows, ws
+        if best is None:
+            raise RuntimeError("no launch geometry of the batched sampler fits this batch")
+        return best, times
+
+    def _save(self) -> None:
+        if self.cache_path is None:
+            return
+        try:
+            self.cache_path.parent.mkdir(parents=True, exist_ok=True)
+            tmp = self.cache_path.with_suffix(".tmp")
+            tmp.write_text(json.dumps(self.table, indent=1, sort_keys=True))
+            tmp.replace(self.cache_path)
+        except OSError:
+            pass
+
+
+_DEFAULT: dict[str, Autotuner] = {}
+
+
+def default_tuner(device) -> Autotuner:
+    """Process-wide tuner of a device (shared by every ``BatchedLOITS``
+    created with ``config="auto"``)."""
+    dev = torch.device(device)
+    key = str(dev)
+    if key not in _DEFAULT:
+        N.require_device(dev)
+        _DEFAULT[key] = Autotuner(dev)
+    return _DEFAULT[key]

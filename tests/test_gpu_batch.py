@@ -368,3 +368,53 @@ def test_large_knot_densities_match_oracle(B, oracle_lib, threads):
         o, e = koff[b], koff[b + 1]
         scale = np.abs(gref[o:e]).max()
         assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b
+
+
+def test_default_cta_size_follows_occupancy(B):
+    """Without a configuration the plan takes the CTA size with the most
+    resident threads: 256 for 1024-knot densities (five CTAs per SM), 1024
+    when 8192-knot records leave room for one CTA per SM."""
+    small = B.BatchPlan(np.array([0, 1024, 2048]), np.array([10, 10]), None, DEV)
+    large = B.BatchPlan(np.array([0, 8192, 8256]), np.array([10, 10]), None, DEV)
+    assert small.config["threads"] == 256 and small.config["blocks_per_item"] == 16
+    assert large.config["threads"] == 1024 and large.config["blocks_per_item"] == 8
+
+
+def test_plans_of_different_sizes_coexist(B, oracle_lib):
+    """A plan for small densities built after one for large densities must not
+    lower the shared memory the large plan launches with."""
+    rng = np.random.default_rng(4)
+    big = dict(knot_offsets=np.array([0, 8000]), event_counts=np.array([5000]),
+               grid=np.linspace(0.01, 1.0, 8000, dtype=np.float32),
+               values=rng.uniform(0.5, 1.5, 8000).astype(np.float32), scalars=np.array([5, 1]))
+    cfg = B.make_config(threads=256)
+    keep = B.BatchPlan(big["knot_offsets"], big["event_counts"], cfg, DEV)
+    small = B.BatchPlan(np.array([0, 16]), np.array([100]), cfg, DEV)
+    out = run_batch(B, big, cfg)
+    ref = oracle_lib.d_forward(big["knot_offsets"], np.array([0, 5000]), big["grid"],
+                               big["values"], None, 5, 1)
+    np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+    del keep, small
+
+
+def test_autotuner_picks_a_geometry_that_samples_identically(B, tmp_path):
+    from quantom_loits_b200 import tuning, workloads
+
+    spec = workloads.ragged(scale=0.01, n_densities=24)
+    batch = B.DensityBatch.from_spec(spec, DEV)
+    tuner = tuning.Autotuner(DEV, reps=2, cache_path=tmp_path / "tune.json")
+    cfg = tuner.config_for(batch, seed=spec.seed)
+    key = tuning.shape_key(spec.knot_offsets, spec.event_counts, True)
+    assert tuner.table[key] == cfg and len(tuner.timings[key]) >= 4
+    # the cache file serves a new tuner without timing
+    again = tuning.Autotuner(DEV, cache_path=tmp_path / "tune.json")
+    assert again.config_for(batch) == cfg and not again.timings
+    case = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, x_cut=spec.x_cut, scalars=np.array([spec.seed, 0]))
+    a = run_batch(B, case)
+    b = run_batch(B, case, B.make_config(**cfg))
+    assert np.array_equal(a["rows"], b["rows"]) and np.array_equal(a["events"], b["events"])
+    # BatchedLOITS(config="auto") goes through the same tuner
+    sampler = B.BatchedLOITS(DEV, seed=spec.seed, config="auto")
+    ev, rows = sampler.sample(batch, sequence=0)
+    assert torch.equal(ev.cpu(), torch.from_numpy(a["events"]))
