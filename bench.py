@@ -163,7 +163,18 @@ def reference_sample(spec, n_dens: int):
     return int(counts.sum()), dt
 
 
+# The reference's intervals are int16 (cpp/loits_core.cpp:12-18) and its
+# search counts every knot per event: a 2^20-knot density is out of its range.
+REFERENCE_INFEASIBLE = {
+    "precision": "reference infeasible on this workload: its int16 intervals overflow at 2^20 "
+                 "knots and its search is O(knots) per event (cpp/loits_core.cpp:12-18)",
+}
+
+
 def run_reference(args, spec) -> dict:
+    if spec.name in REFERENCE_INFEASIBLE:
+        return {"impl": "reference", "unavailable": REFERENCE_INFEASIBLE[spec.name],
+                "metric": METRIC, "config": describe(spec)}
     # calibrate on one density, then take a sample of ~args.ref_seconds per step
     n1, t1 = reference_sample(spec, 1)
     per_density = max(t1, 1e-6)
@@ -317,7 +328,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
             traffic = entry["bytes_per_launch"] * valid / entry["kept_events"]
     except Exception:
         pass
-    cdf_err = cdf_error(plan, step, spec) if rank == 0 else None
+    precision = precision_report(plan, step, spec) if rank == 0 else None
 
     out = {
         "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world,
@@ -341,7 +352,8 @@ def run_b200(args, spec, rank, world, dist) -> dict:
                      "traffic": traffic,
                      "algorithmic_bytes": k_bytes},
         "step_hbm_frac": (fwd_bytes + bwd_bytes) / (ms * 1e-3) / 1e9 / peak,
-        "cdf_err_vs_fp64": cdf_err,
+        "cdf_err_vs_fp64": None if precision is None else precision.get("cdf_err"),
+        "precision": precision,
         "e2e": e2e,
         "gpu_launches": 2 * args.steps,
         "clocks": clocks.summary(),
@@ -349,16 +361,56 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     return out
 
 
-def cdf_error(plan, step, spec):
-    """max |CDF - FP64 oracle CDF| over every knot of the workload."""
+def precision_report(plan, step, spec, n_check: int = 2) -> dict:
+    """Accuracy against the fp64 oracle, outside the timed region:
+    max |CDF - oracle CDF| over every knot; max relative event-quantile error
+    at p = 1e-6, 0.5, 1 - 1e-6 over every density; and, over the first
+    n_check densities' events, the intervals that differ from the oracle's
+    (bin flips) and how many of those lie farther than 2 ulp from a knot."""
+    import torch
+
     try:
         from oracle import oracle as O
 
+        ora = O.Oracle()
         cdf, _ = plan.cdf(step.workspace)
-        _, ocdf, _ = O.Oracle().d_cdf(spec.knot_offsets, spec.grid, spec.values)
-        return float(np.abs(cdf.cpu().numpy() - ocdf).max())
+        _, ocdf, _ = ora.d_cdf(spec.knot_offsets, spec.grid, spec.values)
+        rep = {"cdf_err": float(np.abs(cdf.cpu().numpy() - ocdf).max())}
+        p = np.array([1e-6, 0.5, 1 - 1e-6], dtype=np.float32)
+        qerr = np.zeros(3)
+        for b in range(spec.n_densities):
+            x, _ = plan.quantile(step.workspace, b, torch.from_numpy(p))
+            xo, _ = ora.d_quantile(b, spec.knot_offsets, spec.grid, ocdf, p.astype(np.float64))
+            qerr = np.maximum(qerr, np.abs(x.cpu().numpy() - xo) / np.maximum(np.abs(xo), 1e-30))
+        rep["quantile_rel_err"] = {"1e-6": float(qerr[0]), "0.5": float(qerr[1]),
+                                   "1-1e-6": float(qerr[2])}
+        # intervals of the first n_check densities against the oracle's
+        nd = min(n_check, spec.n_densities)
+        ints = torch.full((max(plan.capacity, 1),), -1, dtype=torch.int32, device=step.events.device)
+        plan.forward(step.grid, step.values, step.x_cut, step.seed, step.sequence, step.events,
+                     step.row_offsets, step.workspace, ints)
+        rows = step.row_offsets.cpu().numpy()
+        koff = spec.knot_offsets[:nd + 1]
+        counts = spec.event_counts[:nd]
+        ref = ora.d_forward(koff, np.concatenate([[0], np.cumsum(counts)]),
+                            spec.grid[:koff[-1]], spec.values[:koff[-1]],
+                            None if spec.x_cut is None else spec.x_cut[:nd], step.seed,
+                            step.sequence, 0, int(spec.event_counts.max()))
+        mine = ints[:rows[nd]].cpu().numpy()
+        diff = np.flatnonzero(mine != ref["intervals"])
+        far = 0
+        for r in diff:
+            b = int(np.searchsorted(ref["row_offsets"], r, side="right") - 1)
+            c = ref["cdf"][koff[b]:koff[b + 1]]
+            u = np.float32(ref["u"][r])
+            i = int(np.searchsorted(c, float(u)))
+            gap = min(abs(float(u) - c[max(i - 1, 0)]), abs(float(u) - c[min(i, len(c) - 1)]))
+            far += gap > 2 * max(float(np.spacing(u)), 2.0 ** -24)
+        rep.update({"flips": int(len(diff)), "flips_far_from_knot": int(far),
+                    "checked_events": int(len(mine)), "checked_densities": nd})
+        return rep
     except Exception as exc:  # pragma: no cover
-        return f"unavailable: {exc}"
+        return {"unavailable": str(exc)}
 
 
 def run_e2e(args, spec, dev, rank, world, dist) -> dict:
@@ -422,6 +474,9 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
 
 def cpu_baseline_leg(args, spec) -> dict:
     """The reference openmp core on a bounded sample, rank 0 / N=1 only."""
+    if spec.name in REFERENCE_INFEASIBLE:
+        return {"value": None, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
+                "sample": REFERENCE_INFEASIBLE[spec.name]}
     try:
         n1, t1 = reference_sample(spec, 1)
         n_dens = int(max(1, min(spec.n_densities, args.ref_seconds / max(t1, 1e-6))))

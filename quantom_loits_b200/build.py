@@ -31,8 +31,9 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INCLUDE}
 # The reference-tuple kernels must round every fp64 product and sum on its
 # own, in source order, like the reference's C++ built without contraction.
 PER_FILE = {"tuple_kernels.cu": ["-fmad=false"]}
-# batch_plan.cu includes batch_kernels.cu (one translation unit).
-SOURCES = ["capi.cu", "tuple_kernels.cu", "batch_plan.cu"]
+# The batched kernels are instantiated per CTA size in batch_inst_*.cu.
+SOURCES = ["capi.cu", "tuple_kernels.cu", "batch_plan.cu", "batch_export.cu", "batch_inst_256.cu",
+           "batch_inst_512.cu", "batch_inst_1024.cu"]
 
 
 def nvcc() -> str:

@@ -1,0 +1,23 @@
+// batch_inst_512.cu -- the batched kernels with 512-thread CTAs.
+#include "batch_kernels_impl.cuh"
+
+namespace loits_dev {
+
+template __global__ void batch_forward_kernel<512, 2, false>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 2, false>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 2, true>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 2, true>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 4, false>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 4, false>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 4, true>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 4, true>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 8, false>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 8, false>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 8, true>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 8, true>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 16, false>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 16, false>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<512, 16, true>(BatchArgs);
+template __global__ void batch_backward_kernel<512, 16, true>(BatchArgs, double*);
+
+}  // namespace loits_dev

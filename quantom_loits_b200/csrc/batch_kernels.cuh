@@ -17,6 +17,13 @@ namespace loits_dev {
 //   guide   = per density with a non-decreasing CDF, M = 2^m >= G buckets of
 //             u: L[k] = number of knots with c_t <= k / M, so the interval of
 //             u in [k/M, (k+1)/M) is found among knots [L[k], L[k+1]].
+//
+// Densities of at most `gcap` knots are sampled from shared memory (records
+// and packed guide copied per tile); larger ones ("large densities", more
+// than 8192 knots) are sampled straight from the records and the uint32
+// guide in global memory (L2-resident where the events concentrate), their
+// backward accumulates the grad-CDF with fp64 global atomics and finalizes
+// with a multi-tile reverse scan.
 struct BatchArgs {
   // plan tables (device)
   const int64_t* knot_off;     // [B+1]
@@ -28,7 +35,10 @@ struct BatchArgs {
   const int64_t* part_off;     // [B] offset of a density's chunk partials
   const int32_t* rowfill_lo;   // [B] first density whose row offset tile 0 of b writes
   const int64_t* goff;         // [B] offset of a density's guide table (entries)
+  const int64_t* pkoff;        // [B] offset of a small density's packed guide (-1: large)
   const int32_t* gbits;        // [B] log2 of a density's guide buckets M
+  const int64_t* gc_off;       // [B] offset of a large density's fp64 grad-CDF (-1: small)
+  const int32_t* lfin_first;   // [B+1] reverse-scan tiles of large densities
   int32_t nd;
   int32_t last_nonempty;       // last density with events (-1 if none)
   // item ranges of this launch (global indices)
@@ -37,6 +47,7 @@ struct BatchArgs {
   int32_t t_lo, t_hi;          // sampling tiles
   int32_t k_lo, k_hi;          // backward chunks
   int32_t d_lo, d_hi;          // densities (backward finalize items)
+  int32_t l_lo, l_hi;          // reverse-scan tiles of large densities (each run twice)
   int32_t tiles_total;         // sampling tiles of the whole plan
   int32_t scan_knots;          // knots per thread per CDF tile
   int32_t gcap;                // knots a sampling CTA holds in shared memory
@@ -53,8 +64,8 @@ struct BatchArgs {
   // state (workspace)
   float4* rec;
   float* invd;
-  uint16_t* gl;                // per density: L[k] = #{t : c_t <= k / M}, k = 0..M
-  uint32_t* gpk;               // per density: L[k] | L[k+1] << 16, k = 0..M-1
+  uint32_t* gl;                // per density: L[k] = #{t : c_t <= k / M}, k = 0..M
+  uint32_t* gpk;               // per small density: L[k] | L[k+1] << 16, k = 0..M-1
   double* norm;
   uint32_t* dflags;            // bit 0: CDF not non-decreasing (count semantics)
   uint32_t* cdf_ready;         // 1 once a density's records and packed guide are final
@@ -72,6 +83,12 @@ struct BatchArgs {
   int32_t* status;
   uint32_t* chunks_done;       // per density
   float* partials;
+  double* gcdf;                // large densities: grad-CDF (zeroed per backward)
+  uint32_t* lflag;             // per reverse-scan tile: 1 aggregate, 2 inclusive
+  double* lagg;
+  double* linc;
+  double* lgn;                 // per reverse-scan tile: sum of grad_rho * value
+  uint32_t* lfin_done;         // per density: reverse-scan tiles done
   // forward outputs
   float* events;
   int64_t* row_offsets;

@@ -1,4 +1,7 @@
-// batch_kernels.cu -- batched ragged 1-D LOITS on sm_100a (fp32 storage).
+// batch_kernels_impl.cuh -- batched ragged 1-D LOITS on sm_100a (fp32 storage).
+//
+// Template definitions of the persistent kernels; batch_inst_*.cu instantiate
+// them (one translation unit per CTA size, compiled in parallel).
 //
 // One persistent forward kernel and one persistent backward kernel serve a
 // whole batch of densities.  CTAs take work items from an atomic ticket in a
@@ -30,6 +33,8 @@
 //   2. Density finalize: sum the partials in chunk order (fp64,
 //      deterministic), reverse suffix scan (cdf_vjp, :340-368) and the
 //      normaliser VJP (density_vjp, :400-435), fp32 output.
+#pragma once
+
 #include <cmath>
 #include <cstdint>
 
@@ -155,7 +160,7 @@ __device__ __forceinline__ int32_t bucket_start(float key, int m) {
 // and the guide buckets whose knot count becomes t + 1 at this knot.
 // gd (guide of the density, nullptr when the CDF is not non-decreasing).
 __device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, int64_t t, double c,
-                                            bool has_next, double c_next, uint16_t* gd, int m) {
+                                            bool has_next, double c_next, uint32_t* gd, int m) {
   const float2 h = split_df(c);
   const float gt = __ldg(&a.grid[k0 + t]);
   float m_slope = 0.0f, inv = 0.0f;
@@ -175,7 +180,7 @@ __device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, int6
     const int32_t M = 1 << m;
     const int32_t k_lo = bucket_start(knot_key(h), m);
     const int32_t k_hi = has_next ? bucket_start(knot_key(hn), m) : M + 1;
-    for (int32_t k = k_lo; k < k_hi; ++k) gd[k] = static_cast<uint16_t>(t + 1);
+    for (int32_t k = k_lo; k < k_hi; ++k) gd[k] = static_cast<uint32_t>(t + 1);
     if (t == 0)
       for (int32_t k = 0; k < k_lo; ++k) gd[k] = 0;
   }
@@ -198,16 +203,19 @@ __device__ __forceinline__ uint32_t accept_all_flag(const BatchArgs& a, int b, i
   return kAcceptAll;
 }
 
-// Pack density b's guide for sampling: gpk[k] = L[k] | L[k+1] << 16.  Every
-// L entry was written (and fenced) before this runs.
+// Pack small density b's guide for sampling from shared memory: gpk[k] =
+// L[k] | L[k+1] << 16 (counts of a small density fit 16 bits).  Every L entry
+// was written (and fenced) before this runs.  Large densities are sampled
+// from L itself.
 template <int TPB>
 __device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
+  const int64_t po = __ldg(&a.pkoff[b]);
+  if (po < 0) return;
   const int M = 1 << __ldg(&a.gbits[b]);
-  const int64_t o = __ldg(&a.goff[b]);
-  const uint16_t* L = a.gl + o;
-  uint32_t* P = a.gpk + o;
+  const uint32_t* L = a.gl + __ldg(&a.goff[b]);
+  uint32_t* P = a.gpk + po;
   for (int k = threadIdx.x; k < M; k += TPB)
-    P[k] = static_cast<uint32_t>(__ldcg(&L[k])) | (static_cast<uint32_t>(__ldcg(&L[k + 1])) << 16);
+    P[k] = __ldcg(&L[k]) | (__ldcg(&L[k + 1]) << 16);
   __threadfence();
 }
 
@@ -219,7 +227,7 @@ __device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
 template <int TPB>
 __device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_t G, int64_t hi, int64_t my_lo,
                           int64_t my_hi, double base, double run0, double norm, bool nonmono,
-                          double tile_next_c, uint16_t* gd, int m, CdfShared<TPB>& sh) {
+                          double tile_next_c, uint32_t* gd, int m, CdfShared<TPB>& sh) {
   const float* g = a.grid + k0;
   const float* f = a.values + k0;
   // first knot of each thread goes to shared memory for its left neighbour
@@ -258,39 +266,45 @@ __device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_
   __syncthreads();
 }
 
-// Chained look-back over the CDF tiles of one density (thread 0 only):
-// returns the fp64 sum of all earlier tiles and publishes this tile's
-// inclusive sum.
-__device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first, int32_t ct, double agg) {
+// Chained look-back over tiles [first, ct) of one density (thread 0 only):
+// publishes tile ct's aggregate, returns the fp64 sum of the earlier tiles
+// and publishes tile ct's inclusive sum.  flag: 1 aggregate, 2 inclusive.
+__device__ __forceinline__ double chained_lookback(uint32_t* flag, double* agg_arr, double* inc_arr,
+                                                   int32_t* status, int32_t first, int32_t ct,
+                                                   double agg) {
   double excl = 0.0;
   if (ct > first) {
-    __stcg(&a.cagg[ct], agg);
+    __stcg(&agg_arr[ct], agg);
     __threadfence();
-    atomicExch(&a.cflag[ct], 1u);
+    atomicExch(&flag[ct], 1u);
     int32_t i = ct - 1;
     uint32_t polls = 0;
     while (i >= first) {
-      const uint32_t fl = ld_acquire_u32(&a.cflag[i]);
+      const uint32_t fl = ld_acquire_u32(&flag[i]);
       if (fl == 0) {
-        if (++polls >= kSpinLimit) {
-          raise_status(a.status, LOITS_ERR_TIMEOUT);
+        if (++polls >= kSpinLimit || ((polls & 63u) == 0u && launch_timed_out(status))) {
+          raise_status(status, LOITS_ERR_TIMEOUT);
           break;
         }
         spin_pause(polls);
         continue;
       }
       if (fl == 2) {
-        excl += __ldcg(&a.cinc[i]);
+        excl += __ldcg(&inc_arr[i]);
         break;
       }
-      excl += __ldcg(&a.cagg[i]);
+      excl += __ldcg(&agg_arr[i]);
       --i;
     }
   }
-  __stcg(&a.cinc[ct], excl + agg);
+  __stcg(&inc_arr[ct], excl + agg);
   __threadfence();
-  atomicExch(&a.cflag[ct], 2u);
+  atomicExch(&flag[ct], 2u);
   return excl;
+}
+
+__device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first, int32_t ct, double agg) {
+  return chained_lookback(a.cflag, a.cagg, a.cinc, a.status, first, ct, agg);
 }
 
 template <int TPB>
@@ -318,7 +332,7 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   const bool any_bad = __syncthreads_or(bad_grid ? 1 : 0) != 0;
   if (nci == 1) {
     // whole density in one tile: finalise now
-    uint16_t* gd = any_neg ? nullptr : a.gl + __ldg(&a.goff[b]);
+    uint32_t* gd = any_neg ? nullptr : a.gl + __ldg(&a.goff[b]);
     cdf_pass2<TPB>(a, k0, G, hi, my_lo, my_hi, excl, run0, tile_tot, any_neg, 0.0, gd,
                    __ldg(&a.gbits[b]), sh);
     if (!any_neg) pack_guide<TPB>(a, b);
@@ -366,30 +380,40 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
   const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
-  if (threadIdx.x == 0) {
-    if (!wait_counter(&a.cdf_scanned[b], static_cast<uint32_t>(nci)))
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    if (lane == 0 && !wait_counter(&a.cdf_scanned[b], static_cast<uint32_t>(nci), a.status))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
-    sh.norm = __ldcg(&a.norm[b]);
-    sh.nonmono = (ld_acquire_u32(&a.dflags[b]) & kNonMonotone) ? 1 : 0;
-    sh.tile_excl = ci == 0 ? 0.0 : __ldcg(&a.cinc[ct - 1]);
+    __syncwarp();
+    // largest unnormalised prefix of all earlier tiles (warp-strided max)
     double mp = kNegInf;
-    for (int32_t i = first; i < ct; ++i) {
+    for (int32_t i = first + lane; i < ct; i += 32) {
       const double v = __ldcg(&a.cmax[i]);
       mp = v > mp ? v : mp;
     }
-    sh.mprev = mp;
-    sh.has_next = hi < G ? 1 : 0;
-    if (hi < G) {
-      // first knot of the next tile, exactly as that tile's own pass 2 forms it
-      float ph = 0.0f, pl = 0.0f;
-      add_area(a.grid + k0, a.values + k0, hi, ph, pl);
-      double s = (__ldcg(&a.cinc[ct]) + 0.0) + (static_cast<double>(ph) + static_cast<double>(pl));
-      if (!sh.nonmono) {
-        const double m_own = __ldcg(&a.cmax[ct]);
-        const double m = mp > m_own ? mp : m_own;
-        s = s > m ? s : m;
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double v = __shfl_xor_sync(0xffffffffu, mp, o);
+      mp = v > mp ? v : mp;
+    }
+    if (lane == 0) {
+      sh.norm = __ldcg(&a.norm[b]);
+      sh.nonmono = (ld_acquire_u32(&a.dflags[b]) & kNonMonotone) ? 1 : 0;
+      sh.tile_excl = ci == 0 ? 0.0 : __ldcg(&a.cinc[ct - 1]);
+      sh.mprev = mp;
+      sh.has_next = hi < G ? 1 : 0;
+      if (hi < G) {
+        // first knot of the next tile, exactly as that tile's own pass 2 forms it
+        float ph = 0.0f, pl = 0.0f;
+        add_area(a.grid + k0, a.values + k0, hi, ph, pl);
+        double s = (__ldcg(&a.cinc[ct]) + 0.0) + (static_cast<double>(ph) + static_cast<double>(pl));
+        if (!sh.nonmono) {
+          const double m_own = __ldcg(&a.cmax[ct]);
+          const double m = mp > m_own ? mp : m_own;
+          s = s > m ? s : m;
+        }
+        sh.cnext = s / sh.norm;
       }
-      sh.cnext = s / sh.norm;
     }
   }
   __syncthreads();
@@ -408,7 +432,7 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   double run0 = block_exclusive_max<double, TPB>(thr_max, kNegInf, tile_max, sh.dmax);
   run0 = run0 > mprev ? run0 : mprev;
   (void)has_next;
-  uint16_t* gd = nonmono ? nullptr : a.gl + __ldg(&a.goff[b]);
+  uint32_t* gd = nonmono ? nullptr : a.gl + __ldg(&a.goff[b]);
   cdf_pass2<TPB>(a, k0, G, hi, my_lo, my_hi, tile_excl + excl, run0, norm, nonmono, cnext, gd,
                  __ldg(&a.gbits[b]), sh);
   // the last finalize item of the density packs its guide and publishes it
@@ -450,14 +474,46 @@ __device__ __forceinline__ TileGeom tile_geom(const BatchArgs& a, int32_t t) {
   return tg;
 }
 
-// A density's sampling state as held in shared memory.
+// Where a density's records and guide are read from:
+//   kShared  small density, copied into shared memory for the tile;
+//   kL2      large density in the forward: global memory written earlier in
+//            the same launch, read through L2 (coherent);
+//   kRO      large density in the backward: global memory, read-only for the
+//            launch (read-only data cache).
+enum : int { kShared = 0, kL2 = 1, kRO = 2 };
+
+template <int kMode>
+__device__ __forceinline__ float4 rec_at(const float4* rec, int i) {
+  if constexpr (kMode == kL2) return __ldcg(rec + i);
+  else if constexpr (kMode == kRO) return __ldg(rec + i);
+  else return rec[i];
+}
+
+template <int kMode>
+__device__ __forceinline__ float2 hilo_at(const float4* rec, int i) {
+  const float2* p = reinterpret_cast<const float2*>(rec + i);
+  if constexpr (kMode == kL2) return __ldcg(p);
+  else if constexpr (kMode == kRO) return __ldg(p);
+  else return *p;
+}
+
+template <int kMode>
+__device__ __forceinline__ uint32_t guide_at(const uint32_t* g, uint32_t k) {
+  if constexpr (kMode == kL2) return __ldcg(g + k);
+  else if constexpr (kMode == kRO) return __ldg(g + k);
+  else return g[k];
+}
+
+// A density's sampling state.
 struct DensView {
-  const float4* rec;
-  const uint32_t* guide;  // packed (L[k], L[k+1]) per bucket
+  const float4* rec;      // records (shared or global)
+  const uint32_t* guide;  // shared: packed (L[k], L[k+1]); global: L itself
+  const float* invd;      // backward weights (shared or global)
   int shift;              // 32 - m: bucket of a Philox word = word >> shift
   int G;
   bool count_all;
   bool accept_all;
+  bool skip;              // large density whose CDF is not non-decreasing: not sampled
   float cut;
 };
 
@@ -468,36 +524,49 @@ struct SampleShared {
   float cut;
 };
 
-// Wait until density b's CDF is final, then load its records, packed guide
-// and (backward) weights into shared memory.
+// Wait until density b's CDF is final, then (small densities) copy its
+// records, packed guide and (backward) weights into shared memory.  Large
+// densities stay in global memory; count semantics over all of their knots
+// would cost O(G) per event, so a large density whose CDF is not
+// non-decreasing is not sampled and the launch reports LOITS_ERR_UNSUPPORTED.
 __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
                                                  float4* rec_s, uint32_t* guide_s, float* invd_s,
                                                  bool wait_ready, SampleShared& sh) {
+  const bool large = G > a.gcap;
   if (threadIdx.x == 0) {
-    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u)) raise_status(a.status, LOITS_ERR_TIMEOUT);
+    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status)) raise_status(a.status, LOITS_ERR_TIMEOUT);
     sh.flags = ld_acquire_u32(&a.dflags[b]);
     sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
+    if (large && (sh.flags & kNonMonotone)) raise_status(a.status, LOITS_ERR_UNSUPPORTED);
   }
   __syncthreads();
   const bool nonmono = (sh.flags & kNonMonotone) != 0;
   const int m = __ldg(&a.gbits[b]);
-  for (int64_t i = threadIdx.x; i < G; i += blockDim.x) {
-    rec_s[i] = __ldcg(&a.rec[k0 + i]);
-    if (invd_s) invd_s[i] = __ldcg(&a.invd[k0 + i]);
-  }
-  if (!nonmono) {
-    const uint4* src = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.goff[b]));
-    uint4* dst = reinterpret_cast<uint4*>(guide_s);
-    for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&src[i]);
-  }
-  __syncthreads();
   DensView v;
-  v.rec = rec_s;
-  v.guide = guide_s;
+  if (large) {
+    v.rec = a.rec + k0;
+    v.guide = a.gl + __ldg(&a.goff[b]);
+    v.invd = a.invd + k0;
+  } else {
+    for (int64_t i = threadIdx.x; i < G; i += blockDim.x) {
+      rec_s[i] = __ldcg(&a.rec[k0 + i]);
+      if (invd_s) invd_s[i] = __ldcg(&a.invd[k0 + i]);
+    }
+    if (!nonmono) {
+      const uint4* src = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.pkoff[b]));
+      uint4* dst = reinterpret_cast<uint4*>(guide_s);
+      for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&src[i]);
+    }
+    __syncthreads();
+    v.rec = rec_s;
+    v.guide = guide_s;
+    v.invd = invd_s;
+  }
   v.shift = 32 - m;
   v.G = static_cast<int>(G);
-  v.count_all = nonmono;
+  v.count_all = nonmono && !large;
   v.accept_all = (sh.flags & kAcceptAll) != 0;
+  v.skip = nonmono && large;
   v.cut = sh.cut;
   return v;
 }
@@ -509,20 +578,32 @@ struct Slot {
   bool ok;
 };
 
+template <int kMode>
 __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
   const float u = uniform_from_bits(bits);
   int j;
   float4 r;
-  if (!d.count_all) {
+  if (kMode == kShared && d.count_all) {
+    j = interval_count_all(d.rec, u, d.G);
+    r = d.rec[j];
+  } else {
     // count = #{t : u >= c_t} lies in [lo, hi] (guide bucket of u); c_0 = 0,
     // so lo >= 1.  Both candidate records are loaded at once: interval lo-1
     // (count == lo) and knot/interval lo (count > lo); one exact compare
     // selects.  Only a bucket holding several knots needs more compares.
-    const uint32_t pk = d.guide[bits >> d.shift];
-    const int lo = static_cast<int>(pk & 0xffffu), hi = static_cast<int>(pk >> 16);
+    const uint32_t k = bits >> d.shift;
+    int lo, hi;
+    if constexpr (kMode == kShared) {
+      const uint32_t pk = d.guide[k];
+      lo = static_cast<int>(pk & 0xffffu);
+      hi = static_cast<int>(pk >> 16);
+    } else {
+      lo = static_cast<int>(guide_at<kMode>(d.guide, k));
+      hi = static_cast<int>(guide_at<kMode>(d.guide, k + 1));
+    }
     const int ja = max(min(lo - 1, d.G - 2), 0);
-    const float4 ra = d.rec[ja];
-    const float4 rb = d.rec[ja + 1];
+    const float4 ra = rec_at<kMode>(d.rec, ja);
+    const float4 rb = rec_at<kMode>(d.rec, ja + 1);
     const bool step = (lo < hi) & ge_knot(u, make_float2(rb.x, rb.y));
     j = ja;
     r = ra;
@@ -532,16 +613,13 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
         int l = c, h = hi;
         while (l < h) {
           const int mid = (l + h) >> 1;
-          if (ge_knot(u, hilo(d.rec, mid))) l = mid + 1; else h = mid;
+          if (ge_knot(u, hilo_at<kMode>(d.rec, mid))) l = mid + 1; else h = mid;
         }
         c = l;
       }
       j = min(c - 1, d.G - 2);
-      r = j == ja + 1 ? rb : d.rec[j];
+      r = j == ja + 1 ? rb : rec_at<kMode>(d.rec, j);
     }
-  } else {
-    j = interval_count_all(d.rec, u, d.G);
-    r = d.rec[j];
   }
   Slot o;
   o.x = interval_value(r, u, o.t);
@@ -595,7 +673,7 @@ __device__ __forceinline__ void warp_store(const float* __restrict__ src, float*
 }
 
 // Optional per-row interval output (diagnostics): recomputed for kept rows.
-template <int TPB, int R>
+template <int TPB, int R, int kMode>
 __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGeom& tg,
                                                 const DensView& d, int64_t row0) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -603,13 +681,13 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
-    const uint32_t range = block_range_mask(tg, blk);
+    const uint32_t range = d.skip ? 0u : block_range_mask(tg, blk);
     int js[4] = {0, 0, 0, 0};
     uint32_t keep = 0;
     if (range) {
       const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
-      const Slot e0 = sample_slot(d, w.x), e1 = sample_slot(d, w.y);
-      const Slot e2 = sample_slot(d, w.z), e3 = sample_slot(d, w.w);
+      const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+      const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
       keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
       js[0] = e0.j; js[1] = e1.j; js[2] = e2.j; js[3] = e3.j;
     }
@@ -632,10 +710,28 @@ __device__ __forceinline__ void tile_slot_range(const TileGeom& tg, int64_t& s_l
   s_hi = pe < dend ? pe : dend;
 }
 
+// Publish tile t's kept count, take its first row from the look-back, and
+// fill the row offsets its density (and trailing empty densities) own.
+// Called by warp 0; returns the base on every lane.
+__device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, const TileGeom& tg,
+                                                int cnt) {
+  const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(cnt), a.status);
+  if ((threadIdx.x & 31) == 0) {
+    a.tile_prefix[t] = base;
+    if (t == __ldg(&a.tile_first[tg.b])) {
+      for (int dd = __ldg(&a.rowfill_lo[tg.b]); dd <= tg.b; ++dd) a.row_offsets[dd] = base;
+    }
+    if (t == a.tiles_total - 1) {
+      for (int dd = a.last_nonempty + 1; dd <= a.nd; ++dd) a.row_offsets[dd] = base + cnt;
+    }
+  }
+  return base;
+}
+
 // Tile of a density whose every event is kept (kAcceptAll): the tile's count
 // is its number of slots, published before any event is computed, and slot p
 // lands in row p + (base - s_lo) -- the identity compaction, no staging.
-template <int TPB, int R>
+template <int TPB, int R, int kMode>
 __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, int32_t t, const TileGeom& tg,
                                                 const DensView& d, SampleShared& sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -643,17 +739,8 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, int32_t t, c
   tile_slot_range<TPB, R>(tg, s_lo, s_hi);
   const int cnt = static_cast<int>(s_hi - s_lo);
   if (warp == 0) {
-    const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(cnt), a.status);
-    if (lane == 0) {
-      sh.base = base;
-      a.tile_prefix[t] = base;
-      if (t == __ldg(&a.tile_first[tg.b])) {
-        for (int dd = __ldg(&a.rowfill_lo[tg.b]); dd <= tg.b; ++dd) a.row_offsets[dd] = base;
-      }
-      if (t == a.tiles_total - 1) {
-        for (int dd = a.last_nonempty + 1; dd <= a.nd; ++dd) a.row_offsets[dd] = base + cnt;
-      }
-    }
+    const int64_t base = publish_tile(a, t, tg, cnt);
+    if (lane == 0) sh.base = base;
   }
   __syncthreads();
   const int64_t shiftrow = sh.base - s_lo;
@@ -663,8 +750,8 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, int32_t t, c
     const uint32_t range = block_range_mask(tg, blk);
     if (!range) continue;
     const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
-    const Slot e0 = sample_slot(d, w.x), e1 = sample_slot(d, w.y);
-    const Slot e2 = sample_slot(d, w.z), e3 = sample_slot(d, w.w);
+    const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+    const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
     const int64_t row0 = (blk << 2) + shiftrow;
     if (range == 0xfu && (row0 & 3) == 0) {
       __stcs(reinterpret_cast<float4*>(a.events + row0), make_float4(e0.x, e1.x, e2.x, e3.x));
@@ -683,29 +770,26 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, int32_t t, c
   }
 }
 
-template <int TPB, int R>
-__device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
-                                            uint32_t* guide_s, float* stage, SampleShared& sh) {
+// General tile: kept events are ranked per warp, staged, and stored once the
+// tile's first row is known.
+template <int TPB, int R, int kMode>
+__device__ __forceinline__ void sample_tile_general(const BatchArgs& a, int32_t t,
+                                                    const TileGeom& tg, const DensView& d,
+                                                    float* stage, SampleShared& sh) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const TileGeom tg = tile_geom<TPB, R>(a, t);
-  const DensView d = load_density(a, tg.b, tg.k0, tg.G, rec_s, guide_s, nullptr, true, sh);
-  if (d.accept_all) {
-    sample_tile_all<TPB, R>(a, t, tg, d, sh);
-    return;
-  }
   float* sw = stage + warp * (R * 128);
   int acc = 0;
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
-    const uint32_t range = block_range_mask(tg, blk);
+    const uint32_t range = d.skip ? 0u : block_range_mask(tg, blk);
     float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
     uint32_t keep = 0;
     if (range) {
       const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
-      const Slot e0 = sample_slot(d, w.x), e1 = sample_slot(d, w.y);
-      const Slot e2 = sample_slot(d, w.z), e3 = sample_slot(d, w.w);
+      const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+      const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
       keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
       x0 = e0.x; x1 = e1.x; x2 = e2.x; x3 = e3.x;
     }
@@ -728,57 +812,65 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
   }
   if (lane == 0) a.warp_off[static_cast<int64_t>(t) * W + warp] = warp_excl;
   if (warp == 0) {
-    const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(tile_cnt), a.status);
-    if (lane == 0) {
-      sh.base = base;
-      a.tile_prefix[t] = base;
-      if (t == __ldg(&a.tile_first[tg.b])) {
-        for (int dd = __ldg(&a.rowfill_lo[tg.b]); dd <= tg.b; ++dd) a.row_offsets[dd] = base;
-      }
-      if (t == a.tiles_total - 1) {
-        for (int dd = a.last_nonempty + 1; dd <= a.nd; ++dd) a.row_offsets[dd] = base + tile_cnt;
-      }
-    }
+    const int64_t base = publish_tile(a, t, tg, tile_cnt);
+    if (lane == 0) sh.base = base;
   }
   __syncthreads();
   const int64_t row0 = sh.base + warp_excl;
   warp_store(sw, a.events + row0, acc);
-  if (a.intervals) write_intervals<TPB, R>(a, tg, d, row0);
+  if (a.intervals) write_intervals<TPB, R, kMode>(a, tg, d, row0);
+}
+
+// kLarge: the plan has densities above the shared-memory limit (compiled
+// separately so that plans without them carry none of the global-memory path).
+template <int TPB, int R, bool kLarge>
+__device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
+                                            uint32_t* guide_s, float* stage, SampleShared& sh) {
+  const TileGeom tg = tile_geom<TPB, R>(a, t);
+  const DensView d = load_density(a, tg.b, tg.k0, tg.G, rec_s, guide_s, nullptr, true, sh);
+  if (kLarge && tg.G > a.gcap) {
+    if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, t, tg, d, sh);
+    else sample_tile_general<TPB, R, kL2>(a, t, tg, d, stage, sh);
+  } else {
+    if (d.accept_all) sample_tile_all<TPB, R, kShared>(a, t, tg, d, sh);
+    else sample_tile_general<TPB, R, kShared>(a, t, tg, d, stage, sh);
+  }
 }
 
 // --------------------------------------------------------- backward phase
 
-// Scatter of one kept slot's cotangent into the chunk's grad-CDF:
+// Scatter of one kept slot's cotangent into the grad-CDF:
 // d x / d c_j = m (w - 1), d x / d c_{j+1} = -m w, w = (u - c_j) / d_j
-// (cpp/loits_core.cpp:293-300).
-__device__ __forceinline__ void scatter_slot(const Slot& e, float g, const float* invd_s,
-                                             float* gacc_s) {
-  const float w = e.t * invd_s[e.j];
+// (cpp/loits_core.cpp:293-300).  Small densities: fp32 shared-memory
+// atomics into the chunk's grad-CDF; large densities: fp64 global atomics
+// into the density's grad-CDF.
+template <int kMode>
+__device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensView& d,
+                                             float* gacc_s, double* gc) {
+  float inv;
+  if constexpr (kMode == kShared) inv = d.invd[e.j];
+  else inv = __ldg(&d.invd[e.j]);
+  const float w = e.t * inv;
   const float mg = e.m * g;
-  atomicAdd(&gacc_s[e.j], mg * (w - 1.0f));
-  atomicAdd(&gacc_s[e.j + 1], -(mg * w));
+  if constexpr (kMode == kShared) {
+    atomicAdd(&gacc_s[e.j], mg * (w - 1.0f));
+    atomicAdd(&gacc_s[e.j + 1], -(mg * w));
+  } else {
+    atomicAdd(&gc[e.j], static_cast<double>(mg * (w - 1.0f)));
+    atomicAdd(&gc[e.j + 1], static_cast<double>(-(mg * w)));
+  }
 }
 
-// Chunk (density, run of sampling tiles).  Every warp replays its own slots
-// of each tile; the forward recorded where its kept rows start
-// (tile_prefix + warp_off), so no scan across warps and no barrier is needed
-// until the chunk's grad-CDF is flushed.
-template <int TPB, int R>
-__device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
-                                               uint32_t* guide_s, float* invd_s, float* gacc_s,
-                                               SampleShared& sh) {
+// The tiles [t_first, t_end) of one backward chunk.  Every warp replays its
+// own slots of each tile; the forward recorded where its kept rows start
+// (tile_prefix + warp_off), so no scan across warps and no barrier is needed.
+template <int TPB, int R, int kMode>
+__device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensView& d, TileGeom tg,
+                                                int32_t tb, int32_t t_first, int32_t t_end,
+                                                float* gacc_s, double* gc) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int b = find_owner(a.chunk_first, a.d_lo, a.d_hi, k);
-  const int32_t ki = k - __ldg(&a.chunk_first[b]);
-  const int32_t tb = __ldg(&a.tile_first[b]);
-  const int32_t t_first = tb + ki * a.tiles_per_chunk;
-  const int32_t t_end0 = t_first + a.tiles_per_chunk;
-  const int32_t t_end = t_end0 < __ldg(&a.tile_first[b + 1]) ? t_end0 : __ldg(&a.tile_first[b + 1]);
-  TileGeom tg = tile_geom<TPB, R>(a, t_first);
-  const int G = static_cast<int>(tg.G);
-  for (int i = threadIdx.x; i < G; i += TPB) gacc_s[i] = 0.0f;
-  const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
+  if (d.skip) return;
   if (d.accept_all) {
     // identity compaction: slot p of tile t is row p + (tile_prefix[t] - s_lo)
 #pragma unroll 1
@@ -803,13 +895,14 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
           g4.z = (range & 4u) ? __ldcs(a.grad + row0 + 2) : 0.0f;
           g4.w = (range & 8u) ? __ldcs(a.grad + row0 + 3) : 0.0f;
         }
-        if (range & 1u) scatter_slot(sample_slot(d, w.x), g4.x, invd_s, gacc_s);
-        if (range & 2u) scatter_slot(sample_slot(d, w.y), g4.y, invd_s, gacc_s);
-        if (range & 4u) scatter_slot(sample_slot(d, w.z), g4.z, invd_s, gacc_s);
-        if (range & 8u) scatter_slot(sample_slot(d, w.w), g4.w, invd_s, gacc_s);
+        if (range & 1u) scatter_slot<kMode>(sample_slot<kMode>(d, w.x), g4.x, d, gacc_s, gc);
+        if (range & 2u) scatter_slot<kMode>(sample_slot<kMode>(d, w.y), g4.y, d, gacc_s, gc);
+        if (range & 4u) scatter_slot<kMode>(sample_slot<kMode>(d, w.z), g4.z, d, gacc_s, gc);
+        if (range & 8u) scatter_slot<kMode>(sample_slot<kMode>(d, w.w), g4.w, d, gacc_s, gc);
       }
     }
-  } else {
+    return;
+  }
 #pragma unroll 1
   for (int32_t t = t_first; t < t_end; ++t) {
     tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
@@ -822,22 +915,49 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       uint32_t keep = 0;
       if (range) {
         const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
-        e0 = sample_slot(d, w.x);
-        e1 = sample_slot(d, w.y);
-        e2 = sample_slot(d, w.z);
-        e3 = sample_slot(d, w.w);
+        e0 = sample_slot<kMode>(d, w.x);
+        e1 = sample_slot<kMode>(d, w.y);
+        e2 = sample_slot<kMode>(d, w.z);
+        e3 = sample_slot<kMode>(d, w.w);
         keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
       }
       int total;
       int64_t my = row + warp_exclusive_count(__popc(keep), total);
-      if (keep & 1u) scatter_slot(e0, __ldcs(&a.grad[my++]), invd_s, gacc_s);
-      if (keep & 2u) scatter_slot(e1, __ldcs(&a.grad[my++]), invd_s, gacc_s);
-      if (keep & 4u) scatter_slot(e2, __ldcs(&a.grad[my++]), invd_s, gacc_s);
-      if (keep & 8u) scatter_slot(e3, __ldcs(&a.grad[my]), invd_s, gacc_s);
+      if (keep & 1u) scatter_slot<kMode>(e0, __ldcs(&a.grad[my++]), d, gacc_s, gc);
+      if (keep & 2u) scatter_slot<kMode>(e1, __ldcs(&a.grad[my++]), d, gacc_s, gc);
+      if (keep & 4u) scatter_slot<kMode>(e2, __ldcs(&a.grad[my++]), d, gacc_s, gc);
+      if (keep & 8u) scatter_slot<kMode>(e3, __ldcs(&a.grad[my]), d, gacc_s, gc);
       row += total;
     }
   }
+}
+
+// Backward chunk (density, run of sampling tiles).
+template <int TPB, int R, bool kLarge>
+__device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
+                                               uint32_t* guide_s, float* invd_s, float* gacc_s,
+                                               SampleShared& sh) {
+  const int b = find_owner(a.chunk_first, a.d_lo, a.d_hi, k);
+  const int32_t ki = k - __ldg(&a.chunk_first[b]);
+  const int32_t tb = __ldg(&a.tile_first[b]);
+  const int32_t t_first = tb + ki * a.tiles_per_chunk;
+  const int32_t t_end0 = t_first + a.tiles_per_chunk;
+  const int32_t t_end = t_end0 < __ldg(&a.tile_first[b + 1]) ? t_end0 : __ldg(&a.tile_first[b + 1]);
+  const TileGeom tg = tile_geom<TPB, R>(a, t_first);
+  const int G = static_cast<int>(tg.G);
+  if (kLarge && tg.G > a.gcap) {
+    const DensView d = load_density(a, b, tg.k0, tg.G, nullptr, nullptr, nullptr, false, sh);
+    vjp_chunk_tiles<TPB, R, kRO>(a, d, tg, tb, t_first, t_end, nullptr,
+                                 a.gcdf + __ldg(&a.gc_off[b]));
+    // the density's grad-CDF atomics are performed before the chunk counts
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
+    return;
   }
+  for (int i = threadIdx.x; i < G; i += TPB) gacc_s[i] = 0.0f;
+  const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
+  vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_s, nullptr);
   __syncthreads();
   float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;
   for (int i = threadIdx.x; i < G; i += TPB) __stcg(&part[i], gacc_s[i]);
@@ -861,8 +981,9 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
   const int32_t nch = __ldg(&a.chunk_first[b + 1]) - __ldg(&a.chunk_first[b]);
   const int64_t k0 = __ldg(&a.knot_off[b]);
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
+  if (G > a.gcap) return;  // large density: reverse-scan tiles instead
   if (threadIdx.x == 0) {
-    if (!wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch)))
+    if (!wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
     sh.carry = 0.0;
   }
@@ -938,11 +1059,123 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
   __syncthreads();
 }
 
+// Reverse-scan tiles of a large density.  Tile ti (ti = 0 is the LAST
+// segment of knots) covers [s1 - SEG, s1), s1 = G - ti * SEG, SEG = TPB * 4.
+template <int TPB>
+__device__ __forceinline__ void large_tile_range(int64_t G, int32_t ti, int64_t& s0, int64_t& s1) {
+  constexpr int64_t SEG = static_cast<int64_t>(TPB) * 4;
+  s1 = G - static_cast<int64_t>(ti) * SEG;
+  s0 = s1 - SEG > 0 ? s1 - SEG : 0;
+}
+
+// Phase 1 of a large density's reverse-mode chain, one tile: suffix sums of
+// the fp64 grad-CDF (in-thread, block, then a chained look-back over the
+// later tiles), grad_rho of the tile's knots, and the tile's share of
+// sum(grad_rho * value) for the normaliser VJP (cpp/loits_core.cpp:340-435).
+template <int TPB>
+__device__ __forceinline__ void vjp_large_scan_item(const BatchArgs& a, int32_t li, double* grho,
+                                                    FinShared<TPB>& sh) {
+  constexpr int E = 4;
+  const int b = find_owner(a.lfin_first, a.d_lo, a.d_hi, li);
+  const int32_t first = __ldg(&a.lfin_first[b]);
+  const int32_t nch = __ldg(&a.chunk_first[b + 1]) - __ldg(&a.chunk_first[b]);
+  const int64_t k0 = __ldg(&a.knot_off[b]);
+  const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
+  int64_t s0, s1;
+  large_tile_range<TPB>(G, li - first, s0, s1);
+  if (threadIdx.x == 0 && !wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status))
+    raise_status(a.status, LOITS_ERR_TIMEOUT);
+  __syncthreads();
+  const double* gc = a.gcdf + __ldg(&a.gc_off[b]);
+  const float* g = a.grid + k0;
+  const float* f = a.values + k0;
+  const int64_t my_lo = s0 + static_cast<int64_t>(threadIdx.x) * E;
+  const int64_t my_hi = my_lo + E < s1 ? my_lo + E : s1;
+  double S[E];
+  double tot = 0.0;
+#pragma unroll
+  for (int e = E - 1; e >= 0; --e) {
+    const int64_t t = my_lo + e;
+    tot += t < my_hi ? __ldcg(&gc[t]) : 0.0;
+    S[e] = tot;
+  }
+  double seg_tot;
+  const double later = block_exclusive_suffix_sum<double, TPB>(tot, seg_tot, sh.dscan);
+  if (threadIdx.x == 0) sh.carry = chained_lookback(a.lflag, a.lagg, a.linc, a.status, first, li, seg_tot);
+  __syncthreads();
+  const double carry = sh.carry;  // sum of grad-CDF over every knot >= s1
+#pragma unroll
+  for (int e = 0; e < E; ++e) S[e] += later + carry;
+  sh.sfirst[threadIdx.x] = my_lo < my_hi ? S[0] : 0.0;
+  __syncthreads();
+  double gn_local = 0.0;
+#pragma unroll
+  for (int e = 0; e < E; ++e) {
+    const int64_t t = my_lo + e;
+    if (t >= my_hi) break;
+    double s_next;
+    if (e + 1 < E && t + 1 < my_hi) s_next = S[e + 1];
+    else if (t + 1 >= G) s_next = 0.0;
+    else if (t + 1 >= s1) s_next = carry;
+    else s_next = sh.sfirst[threadIdx.x + 1];
+    const double h_t = t >= 1 ? 0.5 * (static_cast<double>(__ldg(&g[t])) - static_cast<double>(__ldg(&g[t - 1]))) : 0.0;
+    const double h_n = t + 1 < G ? 0.5 * (static_cast<double>(__ldg(&g[t + 1])) - static_cast<double>(__ldg(&g[t]))) : 0.0;
+    const double gr = h_n * s_next + h_t * S[e];
+    grho[k0 + t] = gr;
+    gn_local += gr * static_cast<double>(__ldg(&f[t]));
+  }
+  double gn_tile;
+  block_exclusive_sum<double, TPB>(gn_local, gn_tile, sh.red);
+  if (threadIdx.x == 0) {
+    __stcg(&a.lgn[li], gn_tile);
+    __threadfence();
+    atomicAdd(&a.lfin_done[b], 1u);
+  }
+  __syncthreads();
+}
+
+// Phase 2, one tile: once every tile of the density has its share, the
+// normaliser gradient (shares summed in tile order: deterministic) and the
+// value gradients of the tile's knots.
+template <int TPB>
+__device__ __forceinline__ void vjp_large_out_item(const BatchArgs& a, int32_t li,
+                                                   const double* grho, FinShared<TPB>& sh) {
+  const int b = find_owner(a.lfin_first, a.d_lo, a.d_hi, li);
+  const int32_t first = __ldg(&a.lfin_first[b]);
+  const int32_t nl = __ldg(&a.lfin_first[b + 1]) - first;
+  const int64_t k0 = __ldg(&a.knot_off[b]);
+  const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
+  int64_t s0, s1;
+  large_tile_range<TPB>(G, li - first, s0, s1);
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    if (lane == 0 && !wait_counter(&a.lfin_done[b], static_cast<uint32_t>(nl), a.status))
+      raise_status(a.status, LOITS_ERR_TIMEOUT);
+    __syncwarp();
+    double v = 0.0;
+    for (int32_t i = lane; i < nl; i += 32) v += __ldcg(&a.lgn[first + i]);
+    v = warp_sum(v);
+    if (lane == 0) sh.carry = v;
+  }
+  __syncthreads();
+  const double norm = __ldcg(&a.norm[b]);
+  const double inv_n = 1.0 / norm;
+  const double gnorm = -sh.carry * inv_n * inv_n;
+  const float* g = a.grid + k0;
+  for (int64_t t = s0 + threadIdx.x; t < s1; t += TPB) {
+    const double h_t = t >= 1 ? 0.5 * (static_cast<double>(__ldg(&g[t])) - static_cast<double>(__ldg(&g[t - 1]))) : 0.0;
+    const double h_n = t + 1 < G ? 0.5 * (static_cast<double>(__ldg(&g[t + 1])) - static_cast<double>(__ldg(&g[t]))) : 0.0;
+    const double v = __ldcg(&grho[k0 + t]) * inv_n + (h_t + h_n) * gnorm;
+    a.grad_values[k0 + t] = __double2float_rn(v);
+  }
+  __syncthreads();
+}
+
 // ---------------------------------------------------------------- kernels
 
 // Register cap: 1280 threads per SM, i.e. 48 registers for five resident
 // 256-thread CTAs, 64 for two 512-thread CTAs or one 1024-thread CTA.
-template <int TPB, int R>
+template <int TPB, int R, bool kLarge>
 __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
@@ -968,13 +1201,13 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
     } else if (item < static_cast<uint32_t>(nC + nF)) {
       cdf_finalize_item<TPB>(a, a.f_lo + static_cast<int32_t>(item) - nC, sh.cdf);
     } else {
-      sample_item<TPB, R>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s, guide_s, stage,
-                          sh.smp);
+      sample_item<TPB, R, kLarge>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s,
+                                  guide_s, stage, sh.smp);
     }
   }
 }
 
-template <int TPB, int R>
+template <int TPB, int R, bool kLarge>
 __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchArgs a, double* grho) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
@@ -986,8 +1219,8 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     SampleShared smp;
   } sh;
   __shared__ uint32_t s_item;
-  const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo;
-  const uint32_t n_items = static_cast<uint32_t>(nK + nD);
+  const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo, nL = a.l_hi - a.l_lo;
+  const uint32_t n_items = static_cast<uint32_t>(nK + nD + 2 * nL);
   while (true) {
     if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1u);
     __syncthreads();
@@ -995,40 +1228,17 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     __syncthreads();
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nK)) {
-      vjp_chunk_item<TPB, R>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s, invd_s, gacc_s,
-                             sh.smp);
-    } else {
+      vjp_chunk_item<TPB, R, kLarge>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s,
+                                     invd_s, gacc_s, sh.smp);
+    } else if (item < static_cast<uint32_t>(nK + nD)) {
       vjp_finalize_item<TPB>(a, a.d_lo + static_cast<int32_t>(item) - nK, grho, sh.fin);
+    } else if constexpr (kLarge) {
+      if (item < static_cast<uint32_t>(nK + nD + nL))
+        vjp_large_scan_item<TPB>(a, a.l_lo + static_cast<int32_t>(item) - nK - nD, grho, sh.fin);
+      else
+        vjp_large_out_item<TPB>(a, a.l_lo + static_cast<int32_t>(item) - nK - nD - nL, grho,
+                                sh.fin);
     }
-  }
-}
-
-// CDF export (hi + lo as fp64) and quantiles -----------------------------
-
-__global__ void batch_cdf_export_kernel(const float4* __restrict__ rec, int64_t n,
-                                        double* __restrict__ cdf) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    const float4 r = rec[i];
-    cdf[i] = static_cast<double>(r.x) + static_cast<double>(r.y);
-  }
-}
-
-__global__ void batch_quantile_kernel(const float4* __restrict__ rec,
-                                      const uint16_t* __restrict__ guide, int m, int G,
-                                      bool count_all, const float* __restrict__ u, int64_t n,
-                                      float* __restrict__ x, int32_t* __restrict__ intervals) {
-  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
-       i += (int64_t)gridDim.x * blockDim.x) {
-    // the guide bucket of u needs its 24-bit word: u = k * 2^-24 exactly
-    const float uc = fminf(fmaxf(u[i], 0.0f), 0x1.fffffep-1f);
-    const uint32_t bits = static_cast<uint32_t>(uc * 16777216.0f) << 8;
-    const uint32_t k = bits >> (32 - m);
-    const int j = count_all ? interval_count_all(rec, u[i], G)
-                            : interval_in_range(rec, guide[k], guide[k + 1], u[i], G);
-    float tv;
-    x[i] = interval_value(rec[j], u[i], tv);
-    if (intervals) intervals[i] = j;
   }
 }
 

@@ -12,17 +12,17 @@
 #include "batch_kernels.cuh"
 
 namespace loits_dev {
-template <int TPB, int R>
+template <int TPB, int R, bool kLarge>
 __global__ void batch_forward_kernel(BatchArgs a);
-template <int TPB, int R>
+template <int TPB, int R, bool kLarge>
 __global__ void batch_backward_kernel(BatchArgs a, double* grho);
 __global__ void batch_cdf_export_kernel(const float4* rec, int64_t n, double* cdf);
-__global__ void batch_quantile_kernel(const float4* rec, const uint16_t* guide, int m, int G,
+__global__ void batch_quantile_kernel(const float4* rec, const uint32_t* guide, int m, int G,
                                       bool count_all, const float* u, int64_t n, float* x,
                                       int32_t* intervals);
 }  // namespace loits_dev
 
-#include "batch_kernels.cu"  // template definitions (single translation unit)
+// template definitions: batch_kernels_impl.cuh, instantiated in batch_inst_*.cu
 
 using namespace loits_dev;
 
@@ -33,8 +33,9 @@ size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
 
 struct Layout {
   size_t status, tickets_fwd, dflags, cdf_ready, cdf_scanned, fin_done, cflag, tile_state;  // zeroed by forward
-  size_t tickets_bwd, chunks_done;                                                // zeroed by backward
+  size_t tickets_bwd, chunks_done, lfin_done, lflag, gcdf;                        // zeroed by backward
   size_t rec, invd, gl, gpk, norm, cagg, cinc, cmax, tile_prefix, warp_off, stage, partials, grho;
+  size_t lagg, linc, lgn;
   size_t fwd_zero_lo, fwd_zero_hi, bwd_zero_lo, bwd_zero_hi, total;
 };
 
@@ -43,16 +44,20 @@ struct Layout {
 struct loits_batch_plan {
   int64_t nd = 0;
   std::vector<int64_t> koff, nev;
-  int64_t nmax = 0, capacity = 0, total_knots = 0, max_g = 0, dbase = 0;
+  int64_t nmax = 0, capacity = 0, total_knots = 0, max_g = 0, small_max_g = 0, dbase = 0;
   loits_batch_config cfg{};
   int tpb = 256, r = 4, scan_knots = 8;
   int32_t n_tiles = 0, n_cdf = 0, n_fin = 0, n_chunks = 0, last_nonempty = -1;
-  int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1;
-  int64_t total_partials = 0, total_guide = 0;
+  int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1, n_lfin = 0;
+  bool has_large = false;  // densities above the shared-memory limit
+  int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
-  std::vector<int64_t> part_off, goff;
+  std::vector<int64_t> part_off, goff, pkoff, gc_off;
+  std::vector<int32_t> lfin_first;
   void* dtab = nullptr;
-  const int64_t *d_koff = nullptr, *d_nev = nullptr, *d_part_off = nullptr, *d_goff = nullptr;
+  const int64_t *d_koff = nullptr, *d_nev = nullptr, *d_part_off = nullptr, *d_goff = nullptr,
+                *d_pkoff = nullptr, *d_gc_off = nullptr;
+  const int32_t* d_lfin_first = nullptr;
   const int32_t *d_tile_first = nullptr, *d_cdf_first = nullptr, *d_fin_first = nullptr,
                 *d_chunk_first = nullptr, *d_rowfill_lo = nullptr, *d_gbits = nullptr;
   Layout lay{};
@@ -66,38 +71,49 @@ using FwdKernel = void (*)(BatchArgs);
 using BwdKernel = void (*)(BatchArgs, double*);
 
 template <int TPB, int R>
-void pick(FwdKernel& f, BwdKernel& b) {
-  f = batch_forward_kernel<TPB, R>;
-  b = batch_backward_kernel<TPB, R>;
+void pick(bool large, FwdKernel& f, BwdKernel& b) {
+  if (large) {
+    f = batch_forward_kernel<TPB, R, true>;
+    b = batch_backward_kernel<TPB, R, true>;
+  } else {
+    f = batch_forward_kernel<TPB, R, false>;
+    b = batch_backward_kernel<TPB, R, false>;
+  }
 }
 
-bool kernels_for(int tpb, int r, FwdKernel& f, BwdKernel& b) {
+// Kernels of a launch geometry; `large`: the plan has densities above the
+// shared-memory limit.
+bool kernels_for(int tpb, int r, bool large, FwdKernel& f, BwdKernel& b) {
   if (tpb == 256) {
     switch (r) {
-      case 2: pick<256, 2>(f, b); return true;
-      case 4: pick<256, 4>(f, b); return true;
-      case 8: pick<256, 8>(f, b); return true;
-      case 16: pick<256, 16>(f, b); return true;
+      case 2: pick<256, 2>(large, f, b); return true;
+      case 4: pick<256, 4>(large, f, b); return true;
+      case 8: pick<256, 8>(large, f, b); return true;
+      case 16: pick<256, 16>(large, f, b); return true;
     }
   } else if (tpb == 512) {
     switch (r) {
-      case 2: pick<512, 2>(f, b); return true;
-      case 4: pick<512, 4>(f, b); return true;
-      case 8: pick<512, 8>(f, b); return true;
-      case 16: pick<512, 16>(f, b); return true;
+      case 2: pick<512, 2>(large, f, b); return true;
+      case 4: pick<512, 4>(large, f, b); return true;
+      case 8: pick<512, 8>(large, f, b); return true;
+      case 16: pick<512, 16>(large, f, b); return true;
     }
   } else if (tpb == 1024) {
     switch (r) {
-      case 2: pick<1024, 2>(f, b); return true;
-      case 4: pick<1024, 4>(f, b); return true;
-      case 8: pick<1024, 8>(f, b); return true;
+      case 2: pick<1024, 2>(large, f, b); return true;
+      case 4: pick<1024, 4>(large, f, b); return true;
+      case 8: pick<1024, 8>(large, f, b); return true;
     }
   }
   return false;
 }
 
-// Largest number of knots a sampling CTA may hold in shared memory.
+// Largest number of knots a sampling CTA holds in shared memory; densities
+// with more knots are sampled from global memory.
 constexpr int64_t kMaxSmemKnots = 8192;
+// Largest density (knot indices are int32; guides of up to 2^22 buckets).
+constexpr int64_t kMaxKnots = int64_t(1) << 28;
+constexpr int kMaxLargeGuideBits = 22;
 constexpr size_t kSmemLimit = 227 * 1024;
 
 int default_blocks(int threads) { return threads == 1024 ? 8 : 16; }
@@ -143,10 +159,10 @@ struct SmemGeometry {
   size_t static_smem = 0, fwd = 0, bwd = 0;
 };
 
-int smem_geometry(int tpb, int r, int32_t gcap, int64_t max_g, SmemGeometry& g) {
+int smem_geometry(int tpb, int r, bool large, int32_t gcap, int64_t max_g, SmemGeometry& g) {
   FwdKernel fk;
   BwdKernel bk;
-  if (!kernels_for(tpb, r, fk, bk)) return LOITS_ERR_INVALID;
+  if (!kernels_for(tpb, r, large, fk, bk)) return LOITS_ERR_INVALID;
   cudaFuncAttributes fattr{}, battr{};
   if (cudaFuncGetAttributes(&fattr, fk) != cudaSuccess ||
       cudaFuncGetAttributes(&battr, bk) != cudaSuccess)
@@ -180,30 +196,30 @@ int smem_geometry(int tpb, int r, int32_t gcap, int64_t max_g, SmemGeometry& g) 
 }
 
 // Resident CTAs per SM of the forward and backward kernels of (tpb, r).
-void occupancy(int tpb, int r, const SmemGeometry& g, int& occ_f, int& occ_b) {
+void occupancy(int tpb, int r, bool large, const SmemGeometry& g, int& occ_f, int& occ_b) {
   FwdKernel fk;
   BwdKernel bk;
   occ_f = occ_b = 0;
-  if (!kernels_for(tpb, r, fk, bk)) return;
+  if (!kernels_for(tpb, r, large, fk, bk)) return;
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_f, fk, tpb, g.fwd);
   cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_b, bk, tpb, g.bwd);
 }
 
 // CTA size with the most resident threads per SM for both kernels (the
 // smaller CTA on a tie: fewer threads wait at each tile barrier).
-int choose_threads(int r_req, int32_t gcap, int64_t max_g, int& tpb_out) {
+int choose_threads(int r_req, bool large, int32_t gcap, int64_t max_g, int& tpb_out) {
   int best = -1, best_tpb = 0, last_rc = LOITS_ERR_UNSUPPORTED;
   for (int tpb : {256, 512, 1024}) {
     const int r = r_req ? r_req : default_blocks(tpb);
     if (tpb == 1024 && r == 16) continue;
     SmemGeometry g;
-    const int rc = smem_geometry(tpb, r, gcap, max_g, g);
+    const int rc = smem_geometry(tpb, r, large, gcap, max_g, g);
     if (rc != LOITS_OK) {
       last_rc = rc;
       continue;
     }
     int of = 0, ob = 0;
-    occupancy(tpb, r, g, of, ob);
+    occupancy(tpb, r, large, g, of, ob);
     const int resident = tpb * std::min(of, ob);
     if (resident > best) {
       best = resident;
@@ -231,7 +247,10 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.part_off = p->d_part_off;
   a.rowfill_lo = p->d_rowfill_lo;
   a.goff = p->d_goff;
+  a.pkoff = p->d_pkoff;
   a.gbits = p->d_gbits;
+  a.gc_off = p->d_gc_off;
+  a.lfin_first = p->d_lfin_first;
   a.mcap = p->mcap;
   a.nd = static_cast<int32_t>(p->nd);
   a.last_nonempty = p->last_nonempty;
@@ -244,7 +263,7 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   const Layout& L = p->lay;
   a.rec = carve<float4>(ws, L.rec);
   a.invd = carve<float>(ws, L.invd);
-  a.gl = carve<uint16_t>(ws, L.gl);
+  a.gl = carve<uint32_t>(ws, L.gl);
   a.gpk = carve<uint32_t>(ws, L.gpk);
   a.fin_done = carve<uint32_t>(ws, L.fin_done);
   a.norm = carve<double>(ws, L.norm);
@@ -261,6 +280,12 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.stage_g = carve<float>(ws, L.stage);
   a.status = carve<int32_t>(ws, L.status);
   a.chunks_done = carve<uint32_t>(ws, L.chunks_done);
+  a.gcdf = carve<double>(ws, L.gcdf);
+  a.lflag = carve<uint32_t>(ws, L.lflag);
+  a.lagg = carve<double>(ws, L.lagg);
+  a.linc = carve<double>(ws, L.linc);
+  a.lgn = carve<double>(ws, L.lgn);
+  a.lfin_done = carve<uint32_t>(ws, L.lfin_done);
   a.partials = carve<float>(ws, L.partials);
   return a;
 }
@@ -290,12 +315,13 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
     const int64_t g = p->koff[b + 1] - p->koff[b];
     if (g < 2 || p->nev[b] < 0) { delete p; return LOITS_ERR_INVALID; }
     p->max_g = std::max(p->max_g, g);
+    if (g <= kMaxSmemKnots) p->small_max_g = std::max(p->small_max_g, g);
     p->nmax = std::max(p->nmax, p->nev[b]);
     p->capacity += p->nev[b];
     if (p->nev[b] > 0) p->last_nonempty = static_cast<int32_t>(b);
   }
   p->total_knots = p->koff[n_densities];
-  if (p->max_g > kMaxSmemKnots) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  if (p->max_g > kMaxKnots) { delete p; return LOITS_ERR_UNSUPPORTED; }
   if (c.slot_stride > 0) {
     if (c.slot_stride < p->nmax) { delete p; return LOITS_ERR_INVALID; }
     p->nmax = c.slot_stride;
@@ -305,13 +331,15 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
     delete p;
     return LOITS_ERR_UNSUPPORTED;
   }
+  // knots a sampling CTA holds: the largest small density, rounded to a
   // multiple of 4 so that every shared-memory array after the records stays
-  // 16-byte aligned
-  p->gcap = static_cast<int32_t>((p->max_g + 3) & ~int64_t(3));
+  // 16-byte aligned (every large density has more knots than this)
+  p->gcap = static_cast<int32_t>((std::max<int64_t>(p->small_max_g, 4) + 3) & ~int64_t(3));
+  p->has_large = p->max_g > p->gcap;
   // ---- launch geometry: the CTA size (by occupancy unless given)
   if (c.threads == 0) {
     int tpb = 0;
-    rc = choose_threads(c.blocks_per_item, p->gcap, p->max_g, tpb);
+    rc = choose_threads(c.blocks_per_item, p->has_large, p->gcap, p->small_max_g, tpb);
     if (rc != LOITS_OK) { delete p; return rc; }
     c.threads = tpb;
   }
@@ -320,7 +348,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->tpb = c.threads;
   p->r = c.blocks_per_item;
   SmemGeometry sg;
-  rc = smem_geometry(p->tpb, p->r, p->gcap, p->max_g, sg);
+  rc = smem_geometry(p->tpb, p->r, p->has_large, p->gcap, p->small_max_g, sg);
   if (rc != LOITS_OK) { delete p; return rc; }
   // ---- work items
   const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;
@@ -359,26 +387,50 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->n_fin = static_cast<int32_t>(nf);
   // guide tables, M + 1 uint16 counts and M packed uint32 pairs per density
   // at the same entry offsets
+  // (small densities also keep the packed copy the sampling CTAs load); a
+  // large density's guide is capped by kMaxLargeGuideBits, not shared memory
   p->gbits.resize(n_densities);
   p->goff.resize(n_densities);
-  int64_t go = 0;
+  p->pkoff.resize(n_densities);
+  p->gc_off.resize(n_densities);
+  p->lfin_first.resize(n_densities + 1);
+  const int64_t lseg = static_cast<int64_t>(p->tpb) * 4;
+  int64_t go = 0, pko = 0, gco = 0, nl = 0;
   for (int64_t b = 0; b < n_densities; ++b) {
     const int64_t g = p->koff[b + 1] - p->koff[b];
+    const bool large = g > p->gcap;
+    const int cap = large ? kMaxLargeGuideBits : sg.m_cap;
     int m = 2;
-    while ((int64_t(1) << m) < 2 * g && m < sg.m_cap) ++m;
+    while ((int64_t(1) << m) < 2 * g && m < cap) ++m;
     p->gbits[b] = m;
     p->goff[b] = go;
     go += ((int64_t(1) << m) + 1 + 7) & ~int64_t(7);
-    p->mcap = std::max<int32_t>(p->mcap, static_cast<int32_t>(int64_t(1) << m));
+    p->lfin_first[b] = static_cast<int32_t>(nl);
+    if (large) {
+      p->pkoff[b] = -1;
+      p->gc_off[b] = gco;
+      gco += g;
+      nl += (g + lseg - 1) / lseg;
+    } else {
+      p->pkoff[b] = pko;
+      pko += ((int64_t(1) << m) + 7) & ~int64_t(7);
+      p->gc_off[b] = -1;
+      p->mcap = std::max<int32_t>(p->mcap, static_cast<int32_t>(int64_t(1) << m));
+    }
   }
+  if (nl > 0x3fffffff) { delete p; return LOITS_ERR_UNSUPPORTED; }
+  p->lfin_first[n_densities] = static_cast<int32_t>(nl);
+  p->n_lfin = static_cast<int32_t>(nl);
   p->total_guide = go;
+  p->total_pk = pko;
+  p->total_gc = gco;
   p->fwd_smem = sg.fwd;
   p->bwd_smem = sg.bwd;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
   cudaDeviceGetAttribute(&p->num_sms, cudaDevAttrMultiProcessorCount, dev);
   int occ_f = 0, occ_b = 0;
-  occupancy(p->tpb, p->r, sg, occ_f, occ_b);
+  occupancy(p->tpb, p->r, p->has_large, sg, occ_f, occ_b);
   if (occ_f < 1 || occ_b < 1) { delete p; return LOITS_ERR_UNSUPPORTED; }
   if (c.ctas_per_sm > 0) {
     occ_f = std::min(occ_f, static_cast<int>(c.ctas_per_sm));
@@ -405,7 +457,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->chunk_first[n_densities] = static_cast<int32_t>(nk);
   p->n_chunks = static_cast<int32_t>(nk);
   p->total_partials = po;
-  const int64_t items_b = nk + n_densities;
+  const int64_t items_b = nk + n_densities + 2 * static_cast<int64_t>(p->n_lfin);
   p->bwd_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items_b, resident_b)));
 
   // ---- workspace layout
@@ -426,12 +478,18 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   L.bwd_zero_lo = o;
   L.tickets_bwd = o; o = align_up(o + (nd + 1) * 4, 16);
   L.chunks_done = o; o = align_up(o + nd * 4, 16);
+  L.lfin_done = o; o = align_up(o + nd * 4, 16);
+  L.lflag = o; o = align_up(o + static_cast<size_t>(p->n_lfin) * 4, 16);
+  L.gcdf = o; o = align_up(o + static_cast<size_t>(p->total_gc) * 8, 16);
   L.bwd_zero_hi = o;
   o = align_up(o);
   L.rec = o; o = align_up(o + static_cast<size_t>(p->total_knots) * 16);
   L.invd = o; o = align_up(o + static_cast<size_t>(p->total_knots) * 4);
-  L.gl = o; o = align_up(o + static_cast<size_t>(p->total_guide) * 2);
-  L.gpk = o; o = align_up(o + static_cast<size_t>(p->total_guide) * 4);
+  L.gl = o; o = align_up(o + static_cast<size_t>(p->total_guide) * 4);
+  L.gpk = o; o = align_up(o + static_cast<size_t>(p->total_pk) * 4);
+  L.lagg = o; o = align_up(o + static_cast<size_t>(p->n_lfin) * 8);
+  L.linc = o; o = align_up(o + static_cast<size_t>(p->n_lfin) * 8);
+  L.lgn = o; o = align_up(o + static_cast<size_t>(p->n_lfin) * 8);
   L.norm = o; o = align_up(o + nd * 8);
   L.cagg = o; o = align_up(o + static_cast<size_t>(nc) * 8);
   L.cinc = o; o = align_up(o + static_cast<size_t>(nc) * 8);
@@ -461,6 +519,9 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   const size_t o_rf = push(p->rowfill_lo.data(), p->rowfill_lo.size() * 4);
   const size_t o_go = push(p->goff.data(), p->goff.size() * 8);
   const size_t o_gb = push(p->gbits.data(), p->gbits.size() * 4);
+  const size_t o_pk = push(p->pkoff.data(), p->pkoff.size() * 8);
+  const size_t o_gc = push(p->gc_off.data(), p->gc_off.size() * 8);
+  const size_t o_lf = push(p->lfin_first.data(), p->lfin_first.size() * 4);
   if (cudaMalloc(&p->dtab, host.size()) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
   if (cudaMemcpy(p->dtab, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(p->dtab);
@@ -478,6 +539,9 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->d_rowfill_lo = reinterpret_cast<const int32_t*>(d + o_rf);
   p->d_goff = reinterpret_cast<const int64_t*>(d + o_go);
   p->d_gbits = reinterpret_cast<const int32_t*>(d + o_gb);
+  p->d_pkoff = reinterpret_cast<const int64_t*>(d + o_pk);
+  p->d_gc_off = reinterpret_cast<const int64_t*>(d + o_gc);
+  p->d_lfin_first = reinterpret_cast<const int32_t*>(d + o_lf);
   *out = p;
   return LOITS_OK;
 }
@@ -532,7 +596,7 @@ extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
   a.intervals = intervals;
   FwdKernel fk;
   BwdKernel bk;
-  kernels_for(p->tpb, p->r, fk, bk);
+  kernels_for(p->tpb, p->r, p->has_large, fk, bk);
   uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_fwd);
   if (!p->cfg.plain) {
     a.c_lo = 0; a.c_hi = p->n_cdf;
@@ -582,11 +646,12 @@ extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid
   double* grho = carve<double>(workspace, L.grho);
   FwdKernel fk;
   BwdKernel bk;
-  kernels_for(p->tpb, p->r, fk, bk);
+  kernels_for(p->tpb, p->r, p->has_large, fk, bk);
   uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_bwd);
   if (!p->cfg.plain) {
     a.k_lo = 0; a.k_hi = p->n_chunks;
     a.d_lo = 0; a.d_hi = static_cast<int32_t>(p->nd);
+    a.l_lo = 0; a.l_hi = p->n_lfin;
     a.ticket = tickets + p->nd;
     bk<<<p->bwd_grid, p->tpb, p->bwd_smem, st>>>(a, grho);
     return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
@@ -594,8 +659,9 @@ extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid
   for (int64_t b = 0; b < p->nd; ++b) {
     a.k_lo = p->chunk_first[b]; a.k_hi = p->chunk_first[b + 1];
     a.d_lo = static_cast<int32_t>(b); a.d_hi = static_cast<int32_t>(b + 1);
+    a.l_lo = p->lfin_first[b]; a.l_hi = p->lfin_first[b + 1];
     a.ticket = tickets + b;
-    const int64_t items = (a.k_hi - a.k_lo) + 1;
+    const int64_t items = (a.k_hi - a.k_lo) + 1 + 2 * (a.l_hi - a.l_lo);
     const int grid_b = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, p->bwd_grid)));
     bk<<<grid_b, p->tpb, p->bwd_smem, st>>>(a, grho);
     if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
@@ -635,7 +701,7 @@ extern "C" int loits_batch_quantile(const loits_batch_plan* p, const void* works
       cudaStreamSynchronize(st) != cudaSuccess)
     return LOITS_ERR_CUDA;
   const float4* rec = reinterpret_cast<const float4*>(ws + p->lay.rec) + p->koff[density];
-  const uint16_t* guide = reinterpret_cast<const uint16_t*>(ws + p->lay.gl) + p->goff[density];
+  const uint32_t* guide = reinterpret_cast<const uint32_t*>(ws + p->lay.gl) + p->goff[density];
   const int G = static_cast<int>(p->koff[density + 1] - p->koff[density]);
   const int threads = 256;
   const int64_t grid = std::min<int64_t>((n + threads - 1) / threads, 148 * 32);

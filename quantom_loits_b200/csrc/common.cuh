@@ -165,10 +165,20 @@ __device__ __forceinline__ void raise_status(int32_t* status, int32_t code) {
   if (status) atomicCAS(reinterpret_cast<int*>(status), 0, code);
 }
 
-// Wait until *counter >= target (acquire).  Returns false on timeout.
-__device__ __forceinline__ bool wait_counter(const uint32_t* counter, uint32_t target) {
+// True once a wait of this launch has run out (its status word says so):
+// every other wait then gives up at once instead of running out in turn, so
+// a launch whose dependencies cannot be met ends after about one wait limit.
+__device__ __forceinline__ bool launch_timed_out(const int32_t* status) {
+  return status && *reinterpret_cast<const volatile int32_t*>(status) == LOITS_ERR_TIMEOUT;
+}
+
+// Wait until *counter >= target (acquire).  Returns false on timeout (or
+// when another wait of the launch has timed out).
+__device__ __forceinline__ bool wait_counter(const uint32_t* counter, uint32_t target,
+                                             const int32_t* status) {
   for (uint32_t it = 0; it < kSpinLimit; ++it) {
     if (ld_acquire_u32(counter) >= target) return true;
+    if ((it & 63u) == 63u && launch_timed_out(status)) return false;
     spin_pause(it);
   }
   return false;

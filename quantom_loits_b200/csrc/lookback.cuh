@@ -35,7 +35,8 @@ __device__ __forceinline__ int64_t lookback_exclusive(unsigned long long* states
     const unsigned long long s = idx >= 0 ? ld_acquire_u64(&states[idx]) : kFlagInclusive;
     const unsigned long long flag = s & ~kValueMask;
     if (__any_sync(0xffffffffu, flag == 0)) {
-      if (++polls >= kSpinLimit) {
+      if (++polls >= kSpinLimit ||
+          ((polls & 63u) == 0u && __any_sync(0xffffffffu, launch_timed_out(status)))) {
         timed_out = true;
         break;
       }

@@ -69,8 +69,8 @@ def test_batch_plan_rejects_bad_tables_on_host(native):
     # offsets not starting at zero
     rc, _ = _plan(native, [1, 3, 5], [1, 1])
     assert rc == native.LOITS_ERR_INVALID
-    # more knots than a sampling CTA holds
-    rc, _ = _plan(native, [0, 100000], [5])
+    # more knots than the sampler indexes (2^28 per density)
+    rc, _ = _plan(native, [0, 2**28 + 1], [5])
     assert rc == native.LOITS_ERR_UNSUPPORTED
     # slot stride smaller than the largest event count
     cfg = native.BatchConfig(0, 0, 0, 0, 0, 0, 3)

@@ -418,3 +418,96 @@ def test_autotuner_picks_a_geometry_that_samples_identically(B, tmp_path):
     sampler = B.BatchedLOITS(DEV, seed=spec.seed, config="auto")
     ev, rows = sampler.sample(batch, sequence=0)
     assert torch.equal(ev.cpu(), torch.from_numpy(a["events"]))
+
+
+def _large_case(rng, sizes, counts, cut=True, seed=77, seq=5):
+    grids, vals = [], []
+    for g in sizes:
+        x = np.linspace(1e-3, 1.0, g, dtype=np.float32)
+        mu, sig = rng.uniform(0.2, 0.8), 10 ** rng.uniform(-3, -1.5)
+        f = np.exp(-0.5 * ((x.astype(np.float64) - mu) / sig) ** 2) + 1e-3 * np.power(x, -0.5)
+        grids.append(x)
+        vals.append(f.astype(np.float32))
+    koff = np.concatenate([[0], np.cumsum(sizes)]).astype(np.int64)
+    case = dict(knot_offsets=koff, event_counts=np.asarray(counts, np.int64),
+                grid=np.concatenate(grids), values=np.concatenate(vals),
+                scalars=np.array([seed, seq]))
+    if cut:
+        case["x_cut"] = rng.uniform(0.01, 0.1, len(sizes)).astype(np.float32)
+    return case
+
+
+@pytest.mark.parametrize("threads", [256, 1024])
+def test_large_densities_sampled_from_global_memory(B, oracle_lib, threads):
+    """Densities above 8192 knots (here up to 70001, past 16-bit guide counts)
+    are sampled from records and guide in global memory, beside small ones in
+    the same batch; events, rows and intervals against the fp64 oracle, the
+    VJP (fp64 global atomics + multi-tile reverse scan) against the oracle's."""
+    rng = np.random.default_rng(31)
+    case = _large_case(rng, [20000, 300, 70001, 9000], [150_000, 20_000, 200_000, 50_000])
+    koff, counts = case["knot_offsets"], case["event_counts"]
+    eoff = np.concatenate([[0], np.cumsum(counts)])
+    ref = oracle_lib.d_forward(koff, eoff, case["grid"], case["values"], case["x_cut"], 77, 5)
+    case["cotangent"] = rng.standard_normal(len(ref["events"])).astype(np.float32)
+    out = run_batch(B, case, B.make_config(threads=threads))
+    assert np.array_equal(out["rows"], ref["row_offsets"])
+    np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+    for r in np.flatnonzero(out["intervals"] != ref["intervals"]):
+        b = np.searchsorted(ref["row_offsets"], r, side="right") - 1
+        assert near_knot(ref["u"][r:r + 1], ref["cdf"][koff[b]:koff[b + 1]])[0], r
+    gref = oracle_lib.d_backward(koff, eoff, case["grid"], case["values"], case["x_cut"], 77, 5,
+                                 case["cotangent"], fwd=ref)
+    for b in range(len(counts)):
+        o, e = koff[b], koff[b + 1]
+        scale = np.abs(gref[o:e]).max()
+        assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b
+    cdf, _ = out["plan"].cdf(out["ws"])
+    assert np.abs(cdf.cpu().numpy() - ref["cdf"]).max() <= CDF_TOL
+
+
+def test_large_densities_plain_and_persistent_agree(B):
+    rng = np.random.default_rng(32)
+    case = _large_case(rng, [12000, 40000], [80_000, 120_000])
+    a = run_batch(B, case)
+    b = run_batch(B, case, B.make_config(plain=1))
+    assert np.array_equal(a["rows"], b["rows"]) and np.array_equal(a["events"], b["events"])
+
+
+def test_large_non_monotone_density_is_reported_unsupported(B):
+    """Count semantics over every knot would cost O(G) per event for a large
+    density: the sampler reports LOITS_ERR_UNSUPPORTED instead of sampling."""
+    g = 10000
+    grid = np.linspace(0.0, 1.0, g, dtype=np.float32)
+    values = np.ones(g, np.float32)
+    values[5000] = -100.0
+    plan = B.BatchPlan(np.array([0, g]), np.array([1000]), None, DEV)
+    ws, ev, rows = plan.new_workspace(), plan.new_events(), plan.new_row_offsets()
+    plan.forward(torch.from_numpy(grid).to(DEV), torch.from_numpy(values).to(DEV), None, 1, 0,
+                 ev, rows, ws)
+    with pytest.raises(RuntimeError, match="supported|UNSUPPORTED|unsupported"):
+        plan.check_status(ws)
+    assert int(rows[-1].item()) == 0
+
+
+def test_precision_workload_shape_matches_oracle(B, oracle_lib):
+    """Two densities of the precision workload (2^20 knots over [1e-6, 1],
+    narrow Gaussian plus x^-0.5 tail) with 2e5 events each: CDF within 1e-6
+    of fp64, events within 1e-5, quantiles at p = 1e-6, 0.5, 1 - 1e-6."""
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.precision(scale=0.02, n_densities=2)
+    case = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, scalars=np.array([spec.seed, 0]))
+    out = run_batch(B, case)
+    eoff = spec.event_offsets
+    ref = oracle_lib.d_forward(spec.knot_offsets, eoff, spec.grid, spec.values, None, spec.seed, 0)
+    assert np.array_equal(out["rows"], ref["row_offsets"])
+    np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+    cdf, _ = out["plan"].cdf(out["ws"])
+    assert np.abs(cdf.cpu().numpy() - ref["cdf"]).max() <= CDF_TOL
+    p = np.array([1e-6, 0.5, 1 - 1e-6], dtype=np.float32)
+    for b in range(2):
+        x, j = out["plan"].quantile(out["ws"], b, torch.from_numpy(p))
+        xo, jo = oracle_lib.d_quantile(b, spec.knot_offsets, spec.grid, ref["cdf"],
+                                       p.astype(np.float64))
+        np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=EVENT_RTOL)
