@@ -416,7 +416,10 @@ def precision_report(plan, step, spec, n_check: int = 2) -> dict:
 def run_e2e(args, spec, dev, rank, world, dist) -> dict:
     """The user-facing call with host data: pinned host -> device copies of the
     step's inputs (density values, grid, cotangent), BatchedLOITS.sample +
-    autograd backward, device -> host copies of the events and the gradient."""
+    autograd backward, device -> host copies of the events and the gradient.
+    The cotangent's copy in and the events' copy out run on their own streams
+    (opposite PCIe directions) beside the forward; the backward waits for the
+    cotangent and the step ends when events and gradient are on the host."""
     import torch
 
     from quantom_loits_b200 import batched as B
@@ -433,18 +436,27 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
     h_events = torch.empty(spec.total_events, dtype=torch.float32).pin_memory()
     h_grad = torch.empty(spec.total_knots, dtype=torch.float32).pin_memory()
     stream = torch.cuda.current_stream(dev)
+    s_in, s_out = torch.cuda.Stream(dev), torch.cuda.Stream(dev)
 
     def one():
+        s_in.wait_stream(stream)
+        with torch.cuda.stream(s_in):
+            cot = h_cot.to(dev, non_blocking=True)
+        cot.record_stream(stream)
         values = h_vals.to(dev, non_blocking=True).requires_grad_(True)
         grid = h_grid.to(dev, non_blocking=True)
         cut = None if h_cut is None else h_cut.to(dev, non_blocking=True)
-        cot = h_cot.to(dev, non_blocking=True)
         batch = B.DensityBatch(grid, values, spec.knot_offsets, spec.event_counts, cut)
         events, rows = sampler.sample(batch, sequence=0)
         n = events.shape[0]
-        h_events[:n].copy_(events.detach(), non_blocking=True)
+        s_out.wait_stream(stream)
+        with torch.cuda.stream(s_out):
+            h_events[:n].copy_(events.detach(), non_blocking=True)
+        events.record_stream(s_out)
+        stream.wait_stream(s_in)
         events.backward(cot[:n])
         h_grad.copy_(values.grad, non_blocking=True)
+        stream.wait_stream(s_out)
         return n
 
     for _ in range(max(2, args.warmup // 2)):

@@ -12,7 +12,7 @@ __global__ void batch_cdf_export_kernel(const float4* __restrict__ rec, int64_t 
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
        i += (int64_t)gridDim.x * blockDim.x) {
     const float4 r = rec[i];
-    cdf[i] = static_cast<double>(r.x) + static_cast<double>(r.y);
+    cdf[i] = static_cast<double>(r.x) - static_cast<double>(r.y);  // key - (key - c)
   }
 }
 

@@ -9,21 +9,25 @@ namespace loits_dev {
 
 // Per-knot state written by the forward's CDF phase and read by sampling,
 // the backward and the quantile entry:
-//   rec[k]  = {c_hi, c_lo, grid_k, m_k}: the normalised CDF at knot k as a
-//             double-float (c = c_hi + c_lo), the knot position, and the
+//   rec[k]  = {key_k, d_k, grid_k, m_k}: key_k is the smallest fp32 >= c_k
+//             (the normalised fp64 CDF at knot k), so (u >= c_k) == (u >=
+//             key_k) exactly for every fp32 u; d_k = fl32(key_k - c_k) >= 0,
+//             so c_k = key_k - d_k to ~2^-48; the knot position; the
 //             inverse-CDF slope of interval k, m_k = (g_{k+1} - g_k) /
 //             (c_{k+1} - c_k + 1e-5) (0 on the last knot);
 //   invd[k] = 1 / (c_{k+1} - c_k + 1e-5), the backward's weight of interval k;
-//   guide   = per density with a non-decreasing CDF, M = 2^m >= G buckets of
-//             u: L[k] = number of knots with c_t <= k / M, so the interval of
+//   guide   = per density with a non-decreasing CDF, M = 2^m buckets of
+//             u: L[k] = number of knots with c_t <= k / M (M < 2G when
+//             shared memory or the large-density cap limits it), so the interval of
 //             u in [k/M, (k+1)/M) is found among knots [L[k], L[k+1]].
 //
 // Densities of at most `gcap` knots are sampled from shared memory (records
 // and packed guide copied per tile); larger ones ("large densities", more
 // than 8192 knots) are sampled straight from the records and the uint32
 // guide in global memory (L2-resident where the events concentrate), their
-// backward accumulates the grad-CDF with fp64 global atomics and finalizes
-// with a multi-tile reverse scan.
+// backward accumulates per interval the pair of grad-CDF sums it sends to its
+// two knots with one float2 global atomic per event, and finalizes with a
+// multi-tile reverse scan.
 struct BatchArgs {
   // plan tables (device)
   const int64_t* knot_off;     // [B+1]
@@ -37,7 +41,7 @@ struct BatchArgs {
   const int64_t* goff;         // [B] offset of a density's guide table (entries)
   const int64_t* pkoff;        // [B] offset of a small density's packed guide (-1: large)
   const int32_t* gbits;        // [B] log2 of a density's guide buckets M
-  const int64_t* gc_off;       // [B] offset of a large density's fp64 grad-CDF (-1: small)
+  const int64_t* gc_off;       // [B] offset of a large density's interval pairs (-1: small)
   const int32_t* lfin_first;   // [B+1] reverse-scan tiles of large densities
   int32_t nd;
   int32_t last_nonempty;       // last density with events (-1 if none)
@@ -52,6 +56,8 @@ struct BatchArgs {
   int32_t scan_knots;          // knots per thread per CDF tile
   int32_t gcap;                // knots a sampling CTA holds in shared memory
   int32_t mcap;                // guide entries (M + 1) a sampling CTA holds
+  int32_t gbits_cap;           // most guide bits this launch copies to shared memory
+                               // (a larger guide is read every 2^s-th count)
   int32_t tiles_per_chunk;
   int64_t nmax;                // Philox slots per density (slot stride)
   int64_t dbase;               // global index of plan density 0
@@ -83,7 +89,8 @@ struct BatchArgs {
   int32_t* status;
   uint32_t* chunks_done;       // per density
   float* partials;
-  double* gcdf;                // large densities: grad-CDF (zeroed per backward)
+  float2* gcdf;                // large densities, per interval j: (to knot j, to knot j+1)
+                               // grad-CDF sums (zeroed per backward)
   uint32_t* lflag;             // per reverse-scan tile: 1 aggregate, 2 inclusive
   double* lagg;
   double* linc;

@@ -17,11 +17,12 @@
 //   2. CDF finalize items for densities spanning several tiles.
 //      Finalising = clamp the prefix to be non-decreasing (unless an area is
 //      negative: then the exact count semantics of cpp/loits_core.cpp:12-18
-//      are used at sampling time), divide by the fp64 normaliser, store the
-//      CDF as (hi, lo) fp32 pairs with the slope of every interval.
+//      are used at sampling time), divide by the fp64 normaliser, store per
+//      knot the smallest fp32 >= c_k (the search key) with its offset from
+//      c_k and the slope of every interval.
 //   3. Sampling tiles (density, run of Philox blocks): in-register Philox
-//      (rng/philox.hpp), exact search of u against the double-float CDF with
-//      fp32 compares, linear interpolation (cpp/loits_core.cpp:193-196),
+//      (rng/philox.hpp), exact search of fp32 u against the fp64 CDF through
+//      the per-knot keys, linear interpolation (cpp/loits_core.cpp:193-196),
 //      acceptance (finite, non-zero, x > x_cut), warp scans + decoupled
 //      look-back for a stable (density, slot) compaction, coalesced 16-byte
 //      stores from a per-CTA staging run that stays in L2.
@@ -58,14 +59,8 @@ __device__ __forceinline__ int find_owner(const int32_t* __restrict__ table, int
 
 // ------------------------------------------------------------------ search
 
-// (u >= c) for the double-float knot c = (hi, lo), exactly, for fp32 u.
-__device__ __forceinline__ bool ge_knot(float u, float2 c) {
-  return u > c.x || (u == c.x && c.y <= 0.0f);
-}
-
-__device__ __forceinline__ float2 hilo(const float4* rec, int i) {
-  return *reinterpret_cast<const float2*>(&rec[i]);
-}
+// (u >= c_k) exactly, for fp32 u: a record's key is the smallest fp32 >= c_k.
+__device__ __forceinline__ bool ge_key(float u, const float4* rec, int i) { return u >= rec[i].x; }
 
 // Interval of u: (#knots t with u >= c_t) - 1, clamped to [0, G-2].
 // Non-decreasing CDF: the guide bucket k of u (top m bits of its Philox word)
@@ -75,11 +70,11 @@ __device__ __forceinline__ float2 hilo(const float4* rec, int i) {
 // (cpp/loits_core.cpp:12-18).
 __device__ __forceinline__ int interval_in_range(const float4* __restrict__ rec, int lo, int hi,
                                                  float u, int G) {
-  if (lo < hi && ge_knot(u, hilo(rec, lo))) {
+  if (lo < hi && ge_key(u, rec, lo)) {
     ++lo;
     while (lo < hi) {
       const int mid = (lo + hi) >> 1;
-      if (ge_knot(u, hilo(rec, mid))) lo = mid + 1; else hi = mid;
+      if (ge_key(u, rec, mid)) lo = mid + 1; else hi = mid;
     }
   }
   int j = lo - 1;
@@ -89,15 +84,16 @@ __device__ __forceinline__ int interval_in_range(const float4* __restrict__ rec,
 
 __device__ __forceinline__ int interval_count_all(const float4* __restrict__ rec, float u, int G) {
   int cnt = 0;
-  for (int t = 0; t < G; ++t) cnt += ge_knot(u, hilo(rec, t)) ? 1 : 0;
+  for (int t = 0; t < G; ++t) cnt += ge_key(u, rec, t) ? 1 : 0;
   int j = cnt - 1;
   j = j < 0 ? 0 : j;
   return j > G - 2 ? G - 2 : j;
 }
 
-// Inverse CDF on interval j: g_j + m_j * ((u - c_hi) - c_lo), fp32.
+// Inverse CDF on interval j: g_j + m_j * (u - c_j), with u - c_j formed as
+// (u - key_j) + (key_j - c_j), fp32.
 __device__ __forceinline__ float interval_value(float4 r, float u, float& t) {
-  t = __fsub_rn(__fsub_rn(u, r.x), r.y);
+  t = __fadd_rn(__fsub_rn(u, r.x), r.y);
   return __fmaf_rn(r.w, t, r.z);
 }
 
@@ -156,30 +152,30 @@ __device__ __forceinline__ int32_t bucket_start(float key, int m) {
   return static_cast<int32_t>(ceilf(scaled));
 }
 
-// Write the per-knot records of knot t given c_t and (if has_next) c_{t+1},
-// and the guide buckets whose knot count becomes t + 1 at this knot.
-// gd (guide of the density, nullptr when the CDF is not non-decreasing).
+// Write the per-knot record of knot t given c_t and (if has_next) c_{t+1}
+// (fp64), and the guide buckets whose knot count becomes t + 1 at this knot.
+// Record: {key, key - c, g_t, m_t}; key = the smallest fp32 >= c_t, so that
+// for every fp32 u, (u >= c_t) == (u >= key) exactly.
+// gd: guide of the density (nullptr when the CDF is not non-decreasing).
 __device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, int64_t t, double c,
                                             bool has_next, double c_next, uint32_t* gd, int m) {
-  const float2 h = split_df(c);
+  const float key = __double2float_ru(c);
+  const float dk = __double2float_rn(static_cast<double>(key) - c);
   const float gt = __ldg(&a.grid[k0 + t]);
-  float m_slope = 0.0f, inv = 0.0f;
-  float2 hn = make_float2(0.0f, 0.0f);
+  float m_slope = 0.0f, inv = 0.0f, key_next = 0.0f;
   if (has_next) {
-    hn = split_df(c_next);
-    const double C = static_cast<double>(h.x) + static_cast<double>(h.y);
-    const double Cn = static_cast<double>(hn.x) + static_cast<double>(hn.y);
-    const double inv_d = 1.0 / (Cn - C + kEps);
+    key_next = __double2float_ru(c_next);
+    const double inv_d = 1.0 / (c_next - c + kEps);
     const double md = (static_cast<double>(__ldg(&a.grid[k0 + t + 1])) - static_cast<double>(gt)) * inv_d;
     m_slope = __double2float_rn(md);
     inv = __double2float_rn(inv_d);
   }
-  a.rec[k0 + t] = make_float4(h.x, h.y, gt, m_slope);
+  a.rec[k0 + t] = make_float4(key, dk, gt, m_slope);
   a.invd[k0 + t] = inv;
   if (gd) {
     const int32_t M = 1 << m;
-    const int32_t k_lo = bucket_start(knot_key(h), m);
-    const int32_t k_hi = has_next ? bucket_start(knot_key(hn), m) : M + 1;
+    const int32_t k_lo = bucket_start(key, m);
+    const int32_t k_hi = has_next ? bucket_start(key_next, m) : M + 1;
     for (int32_t k = k_lo; k < k_hi; ++k) gd[k] = static_cast<uint32_t>(t + 1);
     if (t == 0)
       for (int32_t k = 0; k < k_lo; ++k) gd[k] = 0;
@@ -490,8 +486,8 @@ __device__ __forceinline__ float4 rec_at(const float4* rec, int i) {
 }
 
 template <int kMode>
-__device__ __forceinline__ float2 hilo_at(const float4* rec, int i) {
-  const float2* p = reinterpret_cast<const float2*>(rec + i);
+__device__ __forceinline__ float key_at(const float4* rec, int i) {
+  const float* p = reinterpret_cast<const float*>(rec + i);
   if constexpr (kMode == kL2) return __ldcg(p);
   else if constexpr (kMode == kRO) return __ldg(p);
   else return *p;
@@ -524,24 +520,31 @@ struct SampleShared {
   float cut;
 };
 
-// Wait until density b's CDF is final, then (small densities) copy its
-// records, packed guide and (backward) weights into shared memory.  Large
-// densities stay in global memory; count semantics over all of their knots
-// would cost O(G) per event, so a large density whose CDF is not
-// non-decreasing is not sampled and the launch reports LOITS_ERR_UNSUPPORTED.
-__device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
-                                                 float4* rec_s, uint32_t* guide_s, float* invd_s,
-                                                 bool wait_ready, SampleShared& sh) {
-  const bool large = G > a.gcap;
+// Wait until density b's CDF is final (thread 0) and share its flags and cut.
+// A large density whose CDF is not non-decreasing would need the count over
+// all of its knots, O(G) per event: it is not sampled and the launch reports
+// LOITS_ERR_UNSUPPORTED.
+__device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool large,
+                                              bool wait_ready, SampleShared& sh) {
   if (threadIdx.x == 0) {
-    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status)) raise_status(a.status, LOITS_ERR_TIMEOUT);
+    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status))
+      raise_status(a.status, LOITS_ERR_TIMEOUT);
     sh.flags = ld_acquire_u32(&a.dflags[b]);
     sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
     if (large && (sh.flags & kNonMonotone)) raise_status(a.status, LOITS_ERR_UNSUPPORTED);
   }
   __syncthreads();
+}
+
+// The density's sampling view: small densities copy their records, packed
+// guide and (backward) weights into shared memory; large densities stay in
+// global memory.  Ends with a barrier.
+__device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int64_t k0, int64_t G,
+                                                 bool large, float4* rec_s, uint32_t* guide_s,
+                                                 float* invd_s, const SampleShared& sh) {
   const bool nonmono = (sh.flags & kNonMonotone) != 0;
-  const int m = __ldg(&a.gbits[b]);
+  const int m_full = __ldg(&a.gbits[b]);
+  const int m = large ? m_full : min(m_full, a.gbits_cap);
   DensView v;
   if (large) {
     v.rec = a.rec + k0;
@@ -552,16 +555,22 @@ __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int6
       rec_s[i] = __ldcg(&a.rec[k0 + i]);
       if (invd_s) invd_s[i] = __ldcg(&a.invd[k0 + i]);
     }
-    if (!nonmono) {
+    if (!nonmono && m == m_full) {
       const uint4* src = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.pkoff[b]));
       uint4* dst = reinterpret_cast<uint4*>(guide_s);
       for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&src[i]);
+    } else if (!nonmono) {
+      // every 2^s-th count: the guide with 2^s-times wider buckets
+      const int sft = m_full - m;
+      const uint32_t* L = a.gl + __ldg(&a.goff[b]);
+      for (int k = threadIdx.x; k < (1 << m); k += blockDim.x)
+        guide_s[k] = __ldcg(&L[k << sft]) | (__ldcg(&L[(k + 1) << sft]) << 16);
     }
-    __syncthreads();
     v.rec = rec_s;
     v.guide = guide_s;
     v.invd = invd_s;
   }
+  __syncthreads();
   v.shift = 32 - m;
   v.G = static_cast<int>(G);
   v.count_all = nonmono && !large;
@@ -569,6 +578,14 @@ __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int6
   v.skip = nonmono && large;
   v.cut = sh.cut;
   return v;
+}
+
+__device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
+                                                 float4* rec_s, uint32_t* guide_s, float* invd_s,
+                                                 bool wait_ready, SampleShared& sh) {
+  const bool large = G > a.gcap;
+  density_flags(a, b, large, wait_ready, sh);
+  return density_view(a, b, k0, G, large, rec_s, guide_s, invd_s, sh);
 }
 
 // One slot: uniform from its Philox word, interval, value, acceptance.
@@ -590,7 +607,8 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
     // count = #{t : u >= c_t} lies in [lo, hi] (guide bucket of u); c_0 = 0,
     // so lo >= 1.  Both candidate records are loaded at once: interval lo-1
     // (count == lo) and knot/interval lo (count > lo); one exact compare
-    // selects.  Only a bucket holding several knots needs more compares.
+    // selects, without a branch.  Only a bucket holding several knots needs
+    // a search.
     const uint32_t k = bits >> d.shift;
     int lo, hi;
     if constexpr (kMode == kShared) {
@@ -604,21 +622,20 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
     const int ja = max(min(lo - 1, d.G - 2), 0);
     const float4 ra = rec_at<kMode>(d.rec, ja);
     const float4 rb = rec_at<kMode>(d.rec, ja + 1);
-    const bool step = (lo < hi) & ge_knot(u, make_float2(rb.x, rb.y));
-    j = ja;
-    r = ra;
-    if (step) {
-      int c = lo + 1;
-      if (hi - lo >= 2) {
-        int l = c, h = hi;
-        while (l < h) {
-          const int mid = (l + h) >> 1;
-          if (ge_knot(u, hilo_at<kMode>(d.rec, mid))) l = mid + 1; else h = mid;
-        }
-        c = l;
+    const bool step = (lo < hi) & (u >= rb.x);
+    // count == lo + 1 moves to interval lo, unless lo - 1 is the last one
+    const bool adv = step & (lo <= d.G - 2);
+    j = ja + (adv ? 1 : 0);
+    r = adv ? rb : ra;
+    if (step & (hi - lo >= 2)) {
+      // count in [lo + 1, hi]: first key above u
+      int l = lo + 1, h = hi;
+      while (l < h) {
+        const int mid = (l + h) >> 1;
+        if (u >= key_at<kMode>(d.rec, mid)) l = mid + 1; else h = mid;
       }
-      j = min(c - 1, d.G - 2);
-      r = j == ja + 1 ? rb : rec_at<kMode>(d.rec, j);
+      j = min(l - 1, d.G - 2);
+      r = rec_at<kMode>(d.rec, j);
     }
   }
   Slot o;
@@ -710,6 +727,14 @@ __device__ __forceinline__ void tile_slot_range(const TileGeom& tg, int64_t& s_l
   s_hi = pe < dend ? pe : dend;
 }
 
+// True when every slot of tile tg lies inside its density (all but a
+// density's first and last tiles): every block's range mask is then 0xf.
+template <int TPB, int R>
+__device__ __forceinline__ bool tile_full(const TileGeom& tg) {
+  const int64_t pb = tg.blk0 << 2, pe = (tg.blk0 + static_cast<int64_t>(TPB) * R) << 2;
+  return pb >= tg.P0 && pe <= tg.P0 + tg.n;
+}
+
 // Publish tile t's kept count, take its first row from the look-back, and
 // fill the row offsets its density (and trailing empty densities) own.
 // Called by warp 0; returns the base on every lane.
@@ -729,25 +754,21 @@ __device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, c
 }
 
 // Tile of a density whose every event is kept (kAcceptAll): the tile's count
-// is its number of slots, published before any event is computed, and slot p
-// lands in row p + (base - s_lo) -- the identity compaction, no staging.
+// is its number of slots, published (by the caller, before any event is
+// computed) with first row `base`, and slot p lands in row p + (base - s_lo)
+// -- the identity compaction, no staging.
 template <int TPB, int R, int kMode>
-__device__ __forceinline__ void sample_tile_all(const BatchArgs& a, int32_t t, const TileGeom& tg,
-                                                const DensView& d, SampleShared& sh) {
+__device__ __forceinline__ void sample_tile_all(const BatchArgs& a, const TileGeom& tg,
+                                                const DensView& d, int64_t base) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int64_t s_lo, s_hi;
   tile_slot_range<TPB, R>(tg, s_lo, s_hi);
-  const int cnt = static_cast<int>(s_hi - s_lo);
-  if (warp == 0) {
-    const int64_t base = publish_tile(a, t, tg, cnt);
-    if (lane == 0) sh.base = base;
-  }
-  __syncthreads();
-  const int64_t shiftrow = sh.base - s_lo;
+  const int64_t shiftrow = base - s_lo;
+  const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
-    const uint32_t range = block_range_mask(tg, blk);
+    const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
     if (!range) continue;
     const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
     const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
@@ -780,10 +801,11 @@ __device__ __forceinline__ void sample_tile_general(const BatchArgs& a, int32_t 
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float* sw = stage + warp * (R * 128);
   int acc = 0;
+  const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
-    const uint32_t range = d.skip ? 0u : block_range_mask(tg, blk);
+    const uint32_t range = d.skip ? 0u : (full ? 0xfu : block_range_mask(tg, blk));
     float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
     uint32_t keep = 0;
     if (range) {
@@ -827,12 +849,22 @@ template <int TPB, int R, bool kLarge>
 __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
                                             uint32_t* guide_s, float* stage, SampleShared& sh) {
   const TileGeom tg = tile_geom<TPB, R>(a, t);
-  const DensView d = load_density(a, tg.b, tg.k0, tg.G, rec_s, guide_s, nullptr, true, sh);
-  if (kLarge && tg.G > a.gcap) {
-    if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, t, tg, d, sh);
+  const bool large = kLarge && tg.G > a.gcap;
+  density_flags(a, tg.b, large, true, sh);
+  if ((sh.flags & kAcceptAll) && threadIdx.x < 32) {
+    // identity compaction: the count is known now, so the row look-back runs
+    // while the other warps copy the density
+    int64_t s_lo, s_hi;
+    tile_slot_range<TPB, R>(tg, s_lo, s_hi);
+    const int64_t base = publish_tile(a, t, tg, static_cast<int>(s_hi - s_lo));
+    if (threadIdx.x == 0) sh.base = base;
+  }
+  const DensView d = density_view(a, tg.b, tg.k0, tg.G, large, rec_s, guide_s, nullptr, sh);
+  if (large) {
+    if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, tg, d, sh.base);
     else sample_tile_general<TPB, R, kL2>(a, t, tg, d, stage, sh);
   } else {
-    if (d.accept_all) sample_tile_all<TPB, R, kShared>(a, t, tg, d, sh);
+    if (d.accept_all) sample_tile_all<TPB, R, kShared>(a, tg, d, sh.base);
     else sample_tile_general<TPB, R, kShared>(a, t, tg, d, stage, sh);
   }
 }
@@ -842,11 +874,11 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
 // Scatter of one kept slot's cotangent into the grad-CDF:
 // d x / d c_j = m (w - 1), d x / d c_{j+1} = -m w, w = (u - c_j) / d_j
 // (cpp/loits_core.cpp:293-300).  Small densities: fp32 shared-memory
-// atomics into the chunk's grad-CDF; large densities: fp64 global atomics
-// into the density's grad-CDF.
+// atomics into the chunk's grad-CDF; large densities: one float2 global
+// atomic into interval j's pair (sum to knot j, sum to knot j + 1).
 template <int kMode>
 __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensView& d,
-                                             float* gacc_s, double* gc) {
+                                             float* gacc_s, float2* gc) {
   float inv;
   if constexpr (kMode == kShared) inv = d.invd[e.j];
   else inv = __ldg(&d.invd[e.j]);
@@ -856,8 +888,7 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
     atomicAdd(&gacc_s[e.j], mg * (w - 1.0f));
     atomicAdd(&gacc_s[e.j + 1], -(mg * w));
   } else {
-    atomicAdd(&gc[e.j], static_cast<double>(mg * (w - 1.0f)));
-    atomicAdd(&gc[e.j + 1], static_cast<double>(-(mg * w)));
+    atomicAdd(&gc[e.j], make_float2(mg * (w - 1.0f), -(mg * w)));
   }
 }
 
@@ -867,7 +898,7 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
 template <int TPB, int R, int kMode>
 __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensView& d, TileGeom tg,
                                                 int32_t tb, int32_t t_first, int32_t t_end,
-                                                float* gacc_s, double* gc) {
+                                                float* gacc_s, float2* gc) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (d.skip) return;
@@ -879,10 +910,11 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
       int64_t s_lo, s_hi;
       tile_slot_range<TPB, R>(tg, s_lo, s_hi);
       const int64_t shiftrow = __ldcg(&a.tile_prefix[t]) - s_lo;
+      const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
       for (int r = 0; r < R; ++r) {
         const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
-        const uint32_t range = block_range_mask(tg, blk);
+        const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
         if (!range) continue;
         const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
         const int64_t row0 = (blk << 2) + shiftrow;
@@ -895,10 +927,14 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
           g4.z = (range & 4u) ? __ldcs(a.grad + row0 + 2) : 0.0f;
           g4.w = (range & 8u) ? __ldcs(a.grad + row0 + 3) : 0.0f;
         }
-        if (range & 1u) scatter_slot<kMode>(sample_slot<kMode>(d, w.x), g4.x, d, gacc_s, gc);
-        if (range & 2u) scatter_slot<kMode>(sample_slot<kMode>(d, w.y), g4.y, d, gacc_s, gc);
-        if (range & 4u) scatter_slot<kMode>(sample_slot<kMode>(d, w.z), g4.z, d, gacc_s, gc);
-        if (range & 8u) scatter_slot<kMode>(sample_slot<kMode>(d, w.w), g4.w, d, gacc_s, gc);
+        // all four slots first: their record loads must not wait behind the
+        // grad-CDF atomics (which the compiler cannot prove disjoint)
+        const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+        const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
+        if (range & 1u) scatter_slot<kMode>(e0, g4.x, d, gacc_s, gc);
+        if (range & 2u) scatter_slot<kMode>(e1, g4.y, d, gacc_s, gc);
+        if (range & 4u) scatter_slot<kMode>(e2, g4.z, d, gacc_s, gc);
+        if (range & 8u) scatter_slot<kMode>(e3, g4.w, d, gacc_s, gc);
       }
     }
     return;
@@ -907,10 +943,11 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
   for (int32_t t = t_first; t < t_end; ++t) {
     tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
     int64_t row = __ldcg(&a.tile_prefix[t]) + __ldcg(&a.warp_off[static_cast<int64_t>(t) * W + warp]);
+    const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
     for (int r = 0; r < R; ++r) {
       const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
-      const uint32_t range = block_range_mask(tg, blk);
+      const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
       Slot e0, e1, e2, e3;
       uint32_t keep = 0;
       if (range) {
@@ -955,12 +992,24 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
     if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
     return;
   }
-  for (int i = threadIdx.x; i < G; i += TPB) gacc_s[i] = 0.0f;
+  // The chunk's grad-CDF is replicated `rep` times in the shared slot sized
+  // for the largest density (copy c at c * (G + 1): copies of one knot fall
+  // in different banks); lane l adds into copy l % rep, so lanes whose events
+  // share an interval (small, peaked densities) rarely collide.
+  int rep = 1;
+  while (rep < 32 && 2 * rep * (G + 1) <= a.gcap) rep *= 2;
+  const int stride = rep > 1 ? G + 1 : G;  // rep * stride <= gcap
+  for (int i = threadIdx.x; i < rep * stride; i += TPB) gacc_s[i] = 0.0f;
   const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
-  vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_s, nullptr);
+  float* gacc_lane = gacc_s + ((threadIdx.x & 31) & (rep - 1)) * stride;
+  vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_lane, nullptr);
   __syncthreads();
   float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;
-  for (int i = threadIdx.x; i < G; i += TPB) __stcg(&part[i], gacc_s[i]);
+  for (int i = threadIdx.x; i < G; i += TPB) {
+    float v = gacc_s[i];
+    for (int c = 1; c < rep; ++c) v += gacc_s[c * stride + i];
+    __stcg(&part[i], v);
+  }
   __threadfence();
   __syncthreads();
   if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
@@ -1086,7 +1135,7 @@ __device__ __forceinline__ void vjp_large_scan_item(const BatchArgs& a, int32_t 
   if (threadIdx.x == 0 && !wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status))
     raise_status(a.status, LOITS_ERR_TIMEOUT);
   __syncthreads();
-  const double* gc = a.gcdf + __ldg(&a.gc_off[b]);
+  const float2* gc = a.gcdf + __ldg(&a.gc_off[b]);
   const float* g = a.grid + k0;
   const float* f = a.values + k0;
   const int64_t my_lo = s0 + static_cast<int64_t>(threadIdx.x) * E;
@@ -1096,7 +1145,13 @@ __device__ __forceinline__ void vjp_large_scan_item(const BatchArgs& a, int32_t 
 #pragma unroll
   for (int e = E - 1; e >= 0; --e) {
     const int64_t t = my_lo + e;
-    tot += t < my_hi ? __ldcg(&gc[t]) : 0.0;
+    // grad-CDF of knot t: interval t's share plus interval t-1's
+    double v = 0.0;
+    if (t < my_hi) {
+      v = static_cast<double>(__ldcg(&gc[t].x));
+      if (t >= 1) v += static_cast<double>(__ldcg(&gc[t - 1].y));
+    }
+    tot += v;
     S[e] = tot;
   }
   double seg_tot;

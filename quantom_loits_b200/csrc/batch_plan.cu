@@ -48,7 +48,7 @@ struct loits_batch_plan {
   loits_batch_config cfg{};
   int tpb = 256, r = 4, scan_knots = 8;
   int32_t n_tiles = 0, n_cdf = 0, n_fin = 0, n_chunks = 0, last_nonempty = -1;
-  int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1, n_lfin = 0;
+  int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1, n_lfin = 0, m_cap_b = 2;
   bool has_large = false;  // densities above the shared-memory limit
   int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
@@ -111,9 +111,12 @@ bool kernels_for(int tpb, int r, bool large, FwdKernel& f, BwdKernel& b) {
 // Largest number of knots a sampling CTA holds in shared memory; densities
 // with more knots are sampled from global memory.
 constexpr int64_t kMaxSmemKnots = 8192;
-// Largest density (knot indices are int32; guides of up to 2^22 buckets).
+// Largest density (knot indices are int32).
 constexpr int64_t kMaxKnots = int64_t(1) << 28;
-constexpr int kMaxLargeGuideBits = 22;
+// A large density's guide has at most 2^18 buckets: where u is likely the
+// knots are far apart in u, and the rarely hit buckets of the flat tails
+// (holding many knots) are finished by a short search.
+constexpr int kMaxLargeGuideBits = 18;
 constexpr size_t kSmemLimit = 227 * 1024;
 
 int default_blocks(int threads) { return threads == 1024 ? 8 : 16; }
@@ -150,11 +153,12 @@ bool allow_dynamic_smem(const void* fn, size_t bytes) {
                               static_cast<int>(bytes)) == cudaSuccess;
 }
 
-// Shared memory of the sampling kernels of (tpb, r) for densities of at most
-// max_g knots (gcap rounded to 4): the guide cap m_cap, the largest guide
+// Shared memory of the sampling kernels of (tpb, r) for small densities of at
+// most max_g knots (gcap rounded to 4): the guide caps, the largest guide
 // (mcap entries) and the dynamic bytes of the forward and backward CTAs.
 struct SmemGeometry {
-  int m_cap = 2;
+  int m_cap = 2;    // forward: log2 of the most guide buckets beside the records
+  int m_cap_b = 2;  // backward: the same beside records, weights and gradients
   int32_t mcap = 0;
   size_t static_smem = 0, fwd = 0, bwd = 0;
 };
@@ -168,25 +172,32 @@ int smem_geometry(int tpb, int r, bool large, int32_t gcap, int64_t max_g, SmemG
       cudaFuncGetAttributes(&battr, bk) != cudaSuccess)
     return LOITS_ERR_CUDA;
   g.static_smem = std::max(fattr.sharedSizeBytes, battr.sharedSizeBytes);
-  // a backward CTA holds per knot a record, a weight and a gradient slot (24
-  // bytes) plus the density's guide
-  const size_t knot_bytes = static_cast<size_t>(gcap) * (sizeof(float4) + 2 * sizeof(float));
-  if (knot_bytes + g.static_smem + 64 * sizeof(uint32_t) > kSmemLimit) return LOITS_ERR_UNSUPPORTED;
+  // a forward CTA holds per knot a record (16 bytes), a backward CTA also a
+  // weight and a gradient slot (24 bytes); each beside the density's guide
+  const size_t fwd_knots = static_cast<size_t>(gcap) * sizeof(float4);
+  const size_t bwd_knots = static_cast<size_t>(gcap) * (sizeof(float4) + 2 * sizeof(float));
+  if (bwd_knots + g.static_smem + 64 * sizeof(uint32_t) > kSmemLimit) return LOITS_ERR_UNSUPPORTED;
   // guide tables: M = 2^m buckets per density, 2G <= M < 4G, at most 2^14 and
-  // at most what shared memory leaves beside the records (a smaller guide
-  // only widens buckets: the search finishes them exactly)
-  g.m_cap = 14;
-  while (g.m_cap > 2 &&
-         knot_bytes + g.static_smem + (size_t(1) << g.m_cap) * sizeof(uint32_t) > kSmemLimit)
-    --g.m_cap;
+  // at most what the forward's shared memory leaves beside the records (a
+  // smaller guide only widens buckets: the search finishes them exactly).
+  // The backward reads every 2^s-th count when its budget is smaller: the
+  // same guide with 2^s-times wider buckets.
+  auto cap_for = [&](size_t knot_bytes, int from) {
+    int mc = from;
+    while (mc > 2 && knot_bytes + g.static_smem + (size_t(1) << mc) * sizeof(uint32_t) > kSmemLimit)
+      --mc;
+    return mc;
+  };
+  g.m_cap = cap_for(fwd_knots, 14);
+  g.m_cap_b = cap_for(bwd_knots, g.m_cap);
   int m = 2;
   while ((int64_t(1) << m) < 2 * max_g && m < g.m_cap) ++m;
   g.mcap = static_cast<int32_t>(int64_t(1) << m);
+  const int32_t mcap_b = std::min<int32_t>(g.mcap, int32_t(1) << g.m_cap_b);
   // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
   // kept events are staged in global memory, not here
-  const size_t guide_bytes = static_cast<size_t>((g.mcap + 7) & ~7) * sizeof(uint32_t);
-  g.fwd = static_cast<size_t>(gcap) * sizeof(float4) + guide_bytes;
-  g.bwd = knot_bytes + guide_bytes;
+  g.fwd = fwd_knots + static_cast<size_t>((g.mcap + 7) & ~7) * sizeof(uint32_t);
+  g.bwd = bwd_knots + static_cast<size_t>((mcap_b + 7) & ~7) * sizeof(uint32_t);
   if (g.fwd + g.static_smem > kSmemLimit || g.bwd + g.static_smem > kSmemLimit)
     return LOITS_ERR_UNSUPPORTED;
   if (!allow_dynamic_smem(reinterpret_cast<const void*>(fk), g.fwd) ||
@@ -252,6 +263,7 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.gc_off = p->d_gc_off;
   a.lfin_first = p->d_lfin_first;
   a.mcap = p->mcap;
+  a.gbits_cap = 30;  // forward: full guides (the backward lowers this)
   a.nd = static_cast<int32_t>(p->nd);
   a.last_nonempty = p->last_nonempty;
   a.tiles_total = p->n_tiles;
@@ -280,7 +292,7 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.stage_g = carve<float>(ws, L.stage);
   a.status = carve<int32_t>(ws, L.status);
   a.chunks_done = carve<uint32_t>(ws, L.chunks_done);
-  a.gcdf = carve<double>(ws, L.gcdf);
+  a.gcdf = carve<float2>(ws, L.gcdf);
   a.lflag = carve<uint32_t>(ws, L.lflag);
   a.lagg = carve<double>(ws, L.lagg);
   a.linc = carve<double>(ws, L.linc);
@@ -424,6 +436,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->total_guide = go;
   p->total_pk = pko;
   p->total_gc = gco;
+  p->m_cap_b = sg.m_cap_b;
   p->fwd_smem = sg.fwd;
   p->bwd_smem = sg.bwd;
   int dev = 0;
@@ -643,6 +656,7 @@ extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid
   a.x_cut = x_cut;
   a.grad = grad_events;
   a.grad_values = grad_values;
+  a.gbits_cap = p->m_cap_b;
   double* grho = carve<double>(workspace, L.grho);
   FwdKernel fk;
   BwdKernel bk;

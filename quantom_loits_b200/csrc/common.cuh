@@ -120,20 +120,6 @@ __device__ __forceinline__ void trapezoid_df(float g0, float g1, float f0, float
   lo = 0.5f * l;
 }
 
-// Split an fp64 value into (hi, lo) fp32 with hi = fl32(v), lo = fl32(v - hi).
-__device__ __forceinline__ float2 split_df(double v) {
-  const float hi = __double2float_rn(v);
-  const float lo = __double2float_rn(v - static_cast<double>(hi));
-  return make_float2(hi, lo);
-}
-
-// Search key of a double-float knot c = hi + lo: for every fp32 u,
-// (u >= key) == (u >= c) exactly.  hi is the nearest fp32 to c, so c lies
-// within half an ulp of hi; when lo > 0 the first fp32 >= c is the successor.
-__device__ __forceinline__ float knot_key(float2 c) {
-  return c.y > 0.0f ? nextafterf(c.x, __int_as_float(0x7f800000)) : c.x;
-}
-
 // ------------------------------------------------------- flags and spins
 
 __device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
