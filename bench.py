@@ -52,6 +52,12 @@ FWD_B_PER_EVENT, BWD_B_PER_EVENT = 4, 4
 FWD_B_PER_KNOT, BWD_B_PER_KNOT = 8, 12
 
 
+def max_over_ranks(ms: float) -> float:
+    from quantom_loits_b200.sharding import max_over_ranks as _max
+
+    return _max(ms)
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -273,9 +279,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     step.check_status()
     ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+        ms = max_over_ranks(ms)
     events_step = spec.total_events * world
     value = events_step / (ms * 1e-3)
     valid = int(step.row_offsets[-1].item())
@@ -300,9 +304,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     pstep.check_status()
     plain_ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
-        tt = torch.tensor([plain_ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        plain_ms = float(tt.item())
+        plain_ms = max_over_ranks(plain_ms)
     plain_value = events_step / (plain_ms * 1e-3)
     same = torch.equal(pstep.events[:valid], step.events[:valid])
     del pstep, pplan
@@ -474,9 +476,7 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
     torch.cuda.synchronize(dev)
     ms = t0.elapsed_time(t1) / steps
     if dist is not None:
-        tt = torch.tensor([ms], device=dev)
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms = float(tt.item())
+        ms = max_over_ranks(ms)
     h2d = 4 * (spec.total_knots * 2 + spec.total_events + (spec.n_densities if h_cut is not None else 0))
     d2h = 4 * (n + spec.total_knots)
     return {"value": spec.total_events * world / (ms * 1e-3), "unit": "events/s",

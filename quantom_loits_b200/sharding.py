@@ -66,3 +66,41 @@ def shard_spec(spec, world_size: int, rank: int):
                   values=spec.values[k0:k1], event_counts=spec.event_counts[lo:hi],
                   x_cut=None if spec.x_cut is None else spec.x_cut[lo:hi])
     return sub, lo, int(np.max(spec.event_counts)) if len(spec.event_counts) else 0
+
+
+def _collective_device():
+    """Tensors for collectives live where the process group's backend wants
+    them: the current CUDA device for NCCL, the host for gloo."""
+    import torch
+    import torch.distributed as dist
+
+    if dist.get_backend() == "nccl":
+        return torch.device("cuda", torch.cuda.current_device())
+    return torch.device("cpu")
+
+
+def max_over_ranks(value: float, group=None) -> float:
+    """Max of a per-rank float (step times are reported as the slowest rank's)."""
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=_collective_device())
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())
+
+
+def global_rows(local_rows: int, group=None) -> tuple[int, int]:
+    """(first global row of this rank's kept events, total kept rows): the
+    ranks' rows concatenate in rank order, so a consumer that needs the whole
+    batch's row numbering exchanges one count per rank and nothing else."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    dev = _collective_device()
+    mine = torch.tensor([int(local_rows)], dtype=torch.int64, device=dev)
+    counts = [torch.zeros(1, dtype=torch.int64, device=dev) for _ in range(world)]
+    dist.all_gather(counts, mine, group=group)
+    c = [int(x.item()) for x in counts]
+    r = dist.get_rank(group)
+    return sum(c[:r]), sum(c)
