@@ -1,7 +1,7 @@
 """Benchmark: fwd+VJP events/s of the batched LOITS sampler on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload uniform|single|ragged|precision]
+                    [--workload uniform|single|ragged|precision|tuple] [--events E]
 
 One step = forward (normalise, CDF, Philox, inverse-CDF search +
 interpolation, stable compaction) + VJP of the whole density batch.  The
@@ -20,6 +20,11 @@ Before timing, the launch geometry (threads per CTA, Philox blocks per thread,
 CDF scan width) is tuned on the workload itself by timing each candidate
 (quantom_loits_b200.tuning; untimed, reported as config.tuning_ms_per_step);
 --no-tune keeps the plan's default (CTA size by occupancy).
+
+--workload tuple runs the reference's own 2-D theory tuple at the scale of its
+GPU benchmark (99 x 99 cells, K = 10, 1e7 events; fp64, bit-exact with the
+reference) through LOITS(backend="cuda"); its reference arm is the reference's
+openmp core on the identical tuple.
 
 Under torchrun each rank (one GPU) samples its own 64 densities of a global
 batch (density_base = rank * 64, same Philox slot stride): weak scaling, no
@@ -65,9 +70,11 @@ def dist_env():
     return ws, rank, local
 
 
-def workload_spec(name: str):
+def workload_spec(name: str, events: int = 0):
     from quantom_loits_b200 import workloads
 
+    if name == "tuple":
+        return workloads.theory_tuple(n_events=events or 10_000_000)
     return workloads.WORKLOADS[name]()
 
 
@@ -484,6 +491,24 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
             "api": "BatchedLOITS.sample + autograd backward"}
 
 
+def tuple_cpu_baseline(args, spec) -> dict:
+    """The reference openmp core on the same tuple, rank 0 / N=1 only."""
+    try:
+        from oracle import oracle as O
+
+        ref = O.Reference("openmp")
+        ref.set_threads(cpu_cores())
+        reference_tuple_step(ref, spec)
+        dt = float(np.mean([reference_tuple_step(ref, spec) for _ in range(3)]))
+        return {"value": spec.n_events / dt, "unit": "events/s", "cores": cpu_cores(),
+                "kind": "reference",
+                "sample": f"the whole tuple workload ({spec.n_events} events), reference openmp "
+                          "core, forward + backward wall clock, mean of 3"}
+    except Exception as exc:
+        return {"value": None, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
+                "sample": f"unavailable: {exc}"}
+
+
 def cpu_baseline_leg(args, spec) -> dict:
     """The reference openmp core on a bounded sample, rank 0 / N=1 only."""
     if spec.name in REFERENCE_INFEASIBLE:
@@ -501,14 +526,197 @@ def cpu_baseline_leg(args, spec) -> dict:
                 "sample": f"unavailable: {exc}"}
 
 
+# ------------------------------------------------------------------ tuple
+
+TUPLE_B_PER_EVENT = 24  # events (2 x fp64) + packed slot (int64) out; cotangent + slot in
+
+
+def describe_tuple(spec) -> dict:
+    B, nx, kx = spec.x_bins.shape
+    return {"workload": "tuple", "batch": B, "cells": spec.cells, "knots": kx,
+            "n_events": spec.n_events, "layout": "reference theory tuple, fp64"}
+
+
+def reference_tuple_step(ref, spec):
+    t0 = time.perf_counter()
+    st = ref.forward(*spec.arrays, spec.n_events, spec.seed, spec.sequence)
+    g = np.ones_like(st["events"])
+    ref.backward(g, st, spec.x_bins, spec.xsec_x, spec.q_bins, spec.xsec_q, spec.acceptance)
+    return time.perf_counter() - t0
+
+
+def run_tuple_reference(args, spec) -> dict:
+    from oracle import oracle as O
+
+    ref = O.Reference("openmp")
+    ref.set_threads(cpu_cores())
+    for _ in range(args.warmup):
+        reference_tuple_step(ref, spec)
+    t = float(np.mean([reference_tuple_step(ref, spec) for _ in range(args.steps)]))
+    value = spec.n_events / t
+    sample = (f"the whole tuple workload ({spec.cells} cells, {spec.n_events} events) per step, "
+              "reference openmp core, forward + backward wall clock")
+    return {"metric": METRIC, "value": value, "unit": "events/s", "impl": "reference",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": describe_tuple(spec),
+            "cpu_baseline": {"value": value, "unit": "events/s", "cores": cpu_cores(),
+                             "kind": "reference", "sample": sample},
+            "e2e": {"value": value, "unit": "events/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+
+
+def run_tuple_b200(args, spec, rank, world, dist) -> dict:
+    """The reference tuple through the CUDA backend (replicas under torchrun:
+    rank r samples sequence r, no collective on the data path)."""
+    import torch
+
+    from quantom_loits_b200 import backend as BK
+    from quantom_loits_b200.loits import LOITS
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    seq = spec.sequence + rank
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(dev) for a in spec.arrays]
+    stream = torch.cuda.current_stream(dev)
+    gen = torch.Generator(device=dev).manual_seed(7)
+
+    def step():
+        ev, st = BK.tuple_forward(*t, spec.n_events, spec.seed, seq)
+        g = torch.randn(ev.shape, generator=gen, device=dev, dtype=torch.float64)
+        BK.tuple_backward(g, t[0], t[1], t[2], t[3], t[5], st, spec.seed, seq)
+        return ev
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    ev3 = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    f_ms, b_ms = [], []
+    for _ in range(args.steps):
+        ev3[0].record(stream)
+        ev, st = BK.tuple_forward(*t, spec.n_events, spec.seed, seq)
+        ev3[1].record(stream)
+        g = torch.ones(ev.shape, device=dev, dtype=torch.float64)
+        BK.tuple_backward(g, t[0], t[1], t[2], t[3], t[5], st, spec.seed, seq)
+        ev3[2].record(stream)
+        ev3[2].synchronize()
+        f_ms.append(ev3[0].elapsed_time(ev3[1]))
+        b_ms.append(ev3[1].elapsed_time(ev3[2]))
+    valid = int(ev.shape[0])
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        t0.record(stream)
+        for _ in range(args.steps):
+            step()
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        ms = max_over_ranks(ms)
+    value = spec.n_events * world / (ms * 1e-3)
+
+    # end to end through LOITS(backend="cuda") with host buffers
+    h = [torch.from_numpy(np.ascontiguousarray(a)).pin_memory() for a in spec.arrays]
+    h_cot = torch.randn((spec.n_events, 2), dtype=torch.float64,
+                        generator=torch.Generator().manual_seed(3)).pin_memory()
+    h_events = torch.empty((spec.n_events, 2), dtype=torch.float64).pin_memory()
+    h_gx = torch.empty(spec.xsec_x.shape, dtype=torch.float64).pin_memory()
+    h_gq = torch.empty(spec.xsec_q.shape, dtype=torch.float64).pin_memory()
+    sampler = LOITS(backend="cuda", device=dev)
+    s_in = torch.cuda.Stream(dev)
+
+    def one():
+        s_in.wait_stream(stream)
+        with torch.cuda.stream(s_in):
+            cot = h_cot.to(dev, non_blocking=True)
+        cot.record_stream(stream)
+        d = [x.to(dev, non_blocking=True) for x in h]
+        d[1].requires_grad_(True)
+        d[3].requires_grad_(True)
+        events = sampler(tuple(d), spec.n_events)
+        n = events.shape[0]
+        h_events[:n].copy_(events.detach(), non_blocking=True)
+        stream.wait_stream(s_in)
+        events.backward(cot[:n])
+        h_gx.copy_(d[1].grad, non_blocking=True)
+        h_gq.copy_(d[3].grad, non_blocking=True)
+        return n
+
+    for _ in range(max(2, args.warmup // 2)):
+        one()
+    torch.cuda.synchronize(dev)
+    e_steps = max(3, args.steps // 2)
+    t0.record(stream)
+    for _ in range(e_steps):
+        n = one()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    e_ms = t0.elapsed_time(t1) / e_steps
+    if dist is not None:
+        e_ms = max_over_ranks(e_ms)
+    h2d = sum(int(a.nbytes) for a in spec.arrays) + n * 16
+    d2h = n * 16 + int(spec.xsec_x.nbytes + spec.xsec_q.nbytes)
+
+    fm, bm = float(np.mean(f_ms)), float(np.mean(b_ms))
+    kname, k_ms = (("tuple_prepare+tuple_sample", fm) if fm >= bm else ("tuple_backward", bm))
+    peak, peak_kind = hbm_peak()
+    k_bytes = TUPLE_B_PER_EVENT * valid
+    achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    out = {
+        "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic",
+        "config": {**describe_tuple(spec), "accepted_events_per_step": valid * world,
+                   "parallelism": f"replicas x{world} (sequence = rank)",
+                   "l2": "events + cotangent " + ("larger" if 32 * valid > 126e6 else "smaller")
+                         + " than the 126 MB L2 (no flush)"},
+        "kernels_ms": {"forward (prepare + sample)": fm, "backward": bm},
+        "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "algorithmic_bytes": k_bytes},
+        "e2e": {"value": spec.n_events * world / (e_ms * 1e-3), "unit": "events/s",
+                "ms_per_step": e_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                "api": "LOITS(backend='cuda')(theory_outputs, n_events) + autograd backward"},
+        "gpu_launches": 3 * args.steps,
+        "clocks": clocks.summary(),
+    }
+    if rank == 0:
+        out["parity"] = tuple_parity(spec, t, dev)
+    return out
+
+
+def tuple_parity(spec, t, dev) -> dict:
+    """The sampler's events against the oracle's restatement of the reference
+    core on the same tuple, seed and sequence (bit-exact expected)."""
+    try:
+        from oracle import oracle as O
+        from quantom_loits_b200 import backend as BK
+
+        ev, st = BK.tuple_forward(*t, spec.n_events, spec.seed, spec.sequence)
+        ref = O.Oracle().r_forward(*spec.arrays, spec.n_events, spec.seed, spec.sequence)
+        mine = ev.cpu().numpy()
+        same = mine.shape == ref["events"].shape and bool(np.array_equal(mine, ref["events"]))
+        return {"events_bit_exact": same, "valid": int(mine.shape[0]),
+                "packed_equal": bool(np.array_equal(st["packed"].cpu().numpy(), ref["packed"]))}
+    except Exception as exc:  # pragma: no cover
+        return {"unavailable": str(exc)}
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["uniform", "single", "ragged", "precision"],
+    ap.add_argument("--workload", choices=["uniform", "single", "ragged", "precision", "tuple"],
                     default="uniform")
+    ap.add_argument("--events", type=int, default=0,
+                    help="events per step of the tuple workload (default 1e7)")
     ap.add_argument("--threads", type=int, default=0)
     ap.add_argument("--blocks", type=int, default=0)
     ap.add_argument("--ref-seconds", type=float, default=3.0,
@@ -520,12 +728,14 @@ def main(argv=None) -> int:
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world, rank, local = dist_env()
-    spec = workload_spec(args.workload)
+    spec = workload_spec(args.workload, args.events)
+    is_tuple = args.workload == "tuple"
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        print(json.dumps(run_reference(args, spec)), flush=True)
+        out = run_tuple_reference(args, spec) if is_tuple else run_reference(args, spec)
+        print(json.dumps(out), flush=True)
         return 0
 
     dist = None
@@ -540,10 +750,14 @@ def main(argv=None) -> int:
                                  device_id=torch.device("cuda", local))
         dist = tdist
     try:
-        out = run_b200(args, spec, rank, world, dist)
+        if is_tuple:
+            out = run_tuple_b200(args, spec, rank, world, dist)
+        else:
+            out = run_b200(args, spec, rank, world, dist)
         if rank == 0:
             if world == 1 and not args.no_cpu_baseline:
-                out["cpu_baseline"] = cpu_baseline_leg(args, spec)
+                out["cpu_baseline"] = (tuple_cpu_baseline(args, spec) if is_tuple
+                                       else cpu_baseline_leg(args, spec))
             print(json.dumps(out), flush=True)
     finally:
         if dist is not None:

@@ -680,7 +680,20 @@ __device__ __forceinline__ void warp_store(const float* __restrict__ src, float*
   if (lane < h) dst[lane] = __ldcg(&src[lane]);
   const int nv = (n - h) >> 2;
   float4* dv = reinterpret_cast<float4*>(dst + h);
-  for (int v = lane; v < nv; v += 32) {
+  // four 16-byte groups per lane in flight (the staging run is read from L2)
+  int v = lane;
+  for (; v + 96 < nv; v += 128) {
+    float4 q[4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+      const int s0 = h + 4 * (v + 32 * i);
+      q[i] = make_float4(__ldcg(&src[s0]), __ldcg(&src[s0 + 1]), __ldcg(&src[s0 + 2]),
+                         __ldcg(&src[s0 + 3]));
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) __stcs(&dv[v + 32 * i], q[i]);
+  }
+  for (; v < nv; v += 32) {
     const int s0 = h + 4 * v;
     __stcs(&dv[v], make_float4(__ldcg(&src[s0]), __ldcg(&src[s0 + 1]), __ldcg(&src[s0 + 2]),
                                __ldcg(&src[s0 + 3])));

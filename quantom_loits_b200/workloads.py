@@ -146,6 +146,75 @@ def precision(scale: float = 1.0, n_densities: int = 16, knots: int = 1 << 20) -
 WORKLOADS = {"single": single, "uniform": uniform, "ragged": ragged, "precision": precision}
 
 
+@dataclass
+class TupleSpec:
+    """The reference's 2-D theory tuple (pytorch/theory.py:118-126 layout):
+    x_bins (B,nx,kx), xsec_x (B,ny,nx,kx), q_bins (B,ny,kq), xsec_q (B,nx,ny,kq),
+    weights (B,nx,ny), acceptance (B,nx,ny), all fp64 but acceptance (bool)."""
+
+    name: str
+    x_bins: np.ndarray
+    xsec_x: np.ndarray
+    q_bins: np.ndarray
+    xsec_q: np.ndarray
+    weights: np.ndarray
+    acceptance: np.ndarray
+    n_events: int
+    seed: int = 1234
+    sequence: int = 0
+
+    @property
+    def arrays(self):
+        return (self.x_bins, self.xsec_x, self.q_bins, self.xsec_q, self.weights, self.acceptance)
+
+    @property
+    def cells(self) -> int:
+        return int(np.prod(self.weights.shape))
+
+    @property
+    def total_events(self) -> int:
+        return int(self.n_events)
+
+
+def theory_tuple(grid: int = 100, knots: int = 10, n_events: int = 1_000_000,
+                 batch: int = 1) -> TupleSpec:
+    """Seeded synthetic theory tuple with the shapes of the reference's GPU
+    benchmark (grid 100: 99 x 99 cells, K = 10 knots per curve): cell ix of
+    the x axis spans the ix-th of 99 log-spaced ranges of (1e-3, 1) with K
+    uniform knots, likewise q; cross sections are positive power laws
+    x^a (1-x)^b (a ~ U(-0.5, 1), b ~ U(1, 5) per curve) scaled by a smooth
+    factor of the other axis; weights are Dirichlet(1) over the cells;
+    acceptance is True with probability 0.95."""
+    gen = torch.Generator().manual_seed(4)
+    n = grid - 1
+    edges = np.geomspace(1e-3, 1.0, n + 1)
+
+    def bins():
+        out = np.empty((batch, n, knots))
+        for i in range(n):
+            out[:, i, :] = np.linspace(edges[i], edges[i + 1], knots)
+        return out
+
+    x_bins, q_bins = bins(), bins()
+
+    def curves(b_of, other):
+        shape = (batch, n, n, knots)
+        a = _uniform(gen, -0.5, 1.0, batch * n * n).reshape(batch, n, n, 1)
+        b = _uniform(gen, 1.0, 5.0, batch * n * n).reshape(batch, n, n, 1)
+        x = np.broadcast_to(b_of[:, None, :, :], shape)  # (B, other, cell, K)
+        scale = 1.0 + 0.3 * np.cos(np.arange(n) * 0.37)[None, :, None, None] * other
+        return np.ascontiguousarray(np.power(x, a) * np.power(1.0 - x + 1e-12, b) * scale)
+
+    xsec_x = curves(x_bins, 1.0)   # (B, ny, nx, kx)
+    xsec_q = curves(q_bins, -1.0)  # (B, nx, ny, kq)
+    e = -torch.log(torch.rand(batch * n * n, generator=gen, dtype=torch.float64)).numpy()
+    weights = (e.reshape(batch, n * n) / e.reshape(batch, n * n).sum(1, keepdims=True)).reshape(
+        batch, n, n)
+    acceptance = torch.rand(batch * n * n, generator=gen, dtype=torch.float64).numpy().reshape(
+        batch, n, n) < 0.95
+    return TupleSpec("tuple", x_bins, xsec_x, q_bins, xsec_q, weights, acceptance, n_events)
+
+
 def cotangent(n: int, seed: int = 0) -> np.ndarray:
     """Upstream cotangent ~ N(0, 1) of n events (fp32), from a fixed seed."""
     gen = torch.Generator().manual_seed(seed)
