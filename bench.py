@@ -1,7 +1,7 @@
 """Benchmark: fwd+VJP events/s of the batched LOITS sampler on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload uniform|single|ragged|precision|tuple] [--events E]
+                    [--workload uniform|single|ragged|precision|tuple|gan] [--events E]
 
 One step = forward (normalise, CDF, Philox, inverse-CDF search +
 interpolation, stable compaction) + VJP of the whole density batch.  The
@@ -20,6 +20,10 @@ Before timing, the launch geometry (threads per CTA, Philox blocks per thread,
 CDF scan width) is tuned on the workload itself by timing each candidate
 (quantom_loits_b200.tuning; untimed, reported as config.tuning_ms_per_step);
 --no-tune keeps the plan's default (CTA size by occupancy).
+
+--workload gan runs config 4: batched GAN steps (generator MLP -> power-law
+theory on 2048 knots -> 256 x 2e5 events binned into 64-bin histograms in the
+sampler's kernels -> discriminator), the sampler's share of the step reported.
 
 --workload tuple runs the reference's own 2-D theory tuple at the scale of its
 GPU benchmark (99 x 99 cells, K = 10, 1e7 events; fp64, bit-exact with the
@@ -87,56 +91,102 @@ def describe(spec) -> dict:
 
 
 class ClockSampler:
-    """nvidia-smi clocks and throttle reasons during the timed region."""
+    """SM clocks and throttle reasons sampled every ~2 ms during the timed
+    region through NVML (read-only queries), nvidia-smi when NVML is absent.
+    The device is found by its PCI address, so it is the GPU torch uses."""
 
+    REASONS = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
 
     def __init__(self, index: int):
-        import tempfile
-
         self.index = index
-        self.proc = None
-        self.out = None
-        self.path = os.path.join(tempfile.gettempdir(), f"loits_bench_clocks_{os.getpid()}.csv")
+        self.samples: list[tuple[float, float, set]] = []
+        self._stop = None
+        self._thread = None
+        self._proc = None
+        self._path = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+
+        pynvml.nvmlInit()
+        p = torch.cuda.get_device_properties(self.index)
+        bus = f"{p.pci_domain_id:08X}:{p.pci_bus_id:02X}:{p.pci_device_id:02X}.0"
+        try:
+            return pynvml, pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            return pynvml, pynvml.nvmlDeviceGetHandleByIndex(self.index)
 
     def __enter__(self):
+        import threading
+
         try:
-            self.out = open(self.path, "w")
-            self.proc = subprocess.Popen(
-                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
-                 "--format=csv,noheader,nounits", "-lms", "100"],
-                stdout=self.out, stderr=subprocess.DEVNULL)
+            nv, h = self._nvml_handle()
+            bits = {"hw_slowdown": nv.nvmlClocksEventReasonHwSlowdown,
+                    "hw_thermal_slowdown": nv.nvmlClocksEventReasonHwThermalSlowdown,
+                    "sw_thermal_slowdown": nv.nvmlClocksEventReasonSwThermalSlowdown,
+                    "sw_power_cap": nv.nvmlClocksEventReasonSwPowerCap}
+            mx = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            self._stop = threading.Event()
+
+            def poll():
+                while not self._stop.is_set():
+                    sm = float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM))
+                    r = nv.nvmlDeviceGetCurrentClocksEventReasons(h)
+                    self.samples.append((sm, mx, {k for k, b in bits.items() if r & b}))
+                    time.sleep(0.002)
+
+            self._thread = threading.Thread(target=poll, daemon=True)
+            self._thread.start()
+            time.sleep(0.01)
         except Exception:
-            self.proc = None
-        time.sleep(0.3)
+            self._start_smi()
         return self
 
+    def _start_smi(self):
+        import tempfile
+
+        self._path = os.path.join(tempfile.gettempdir(), f"loits_bench_clocks_{os.getpid()}.csv")
+        try:
+            self._out = open(self._path, "w")
+            self._proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "100"],
+                stdout=self._out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self._proc = None
+        time.sleep(0.3)
+
     def __exit__(self, *exc):
-        if self.proc is not None:
-            self.proc.terminate()
+        if self._thread is not None:
+            self._stop.set()
+            self._thread.join(timeout=5)
+        if self._proc is not None:
+            self._proc.terminate()
             try:
-                self.proc.wait(timeout=5)
+                self._proc.wait(timeout=5)
             except Exception:
-                self.proc.kill()
-        if self.out:
-            self.out.close()
+                self._proc.kill()
+            self._out.close()
+            for line in open(self._path):
+                f = line.split(",")
+                if len(f) < 9 or not f[1].strip().replace(".", "").isdigit():
+                    continue
+                reasons = {self.REASONS[i] for i in range(4)
+                           if "Active" in f[5 + i] and "Not" not in f[5 + i]}
+                self.samples.append((float(f[1]), float(f[2]), reasons))
 
     def summary(self) -> dict:
-        try:
-            lines = [l.split(",") for l in open(self.path) if l.strip()]
-        except Exception:
+        if not self.samples:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        if not lines:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
-        sm = [float(l[1]) for l in lines if l[1].strip().replace(".", "").isdigit()]
-        mx = [float(l[2]) for l in lines if l[2].strip().replace(".", "").isdigit()]
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        reasons = sorted({names[i] for l in lines for i in range(4)
-                          if len(l) > 5 + i and "Active" in l[5 + i] and "Not" not in l[5 + i]})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons, "samples": len(lines)}
+        reasons = sorted(set().union(*(r for _, _, r in self.samples)))
+        return {"sm_mhz": statistics.median(s for s, _, _ in self.samples),
+                "sm_max_mhz": max(m for _, m, _ in self.samples), "reasons": reasons,
+                "samples": len(self.samples),
+                "source": "nvml" if self._thread is not None else "nvidia-smi"}
 
 
 def hbm_peak() -> tuple[float, str]:
@@ -707,13 +757,112 @@ def tuple_parity(spec, t, dev) -> dict:
         return {"unavailable": str(exc)}
 
 
+# -------------------------------------------------------------------- gan
+
+def describe_gan(tr) -> dict:
+    return {"workload": "gan", "densities": tr.batch, "knots": int(tr.theory.grid.numel()),
+            "events_per_density": tr.n_events, "bins": tr.bins, "latent": tr.latent,
+            "sampler_calls_per_step": "2 forward (discriminator + generator step) + 1 VJP",
+            "generator": "64-256-256-6 SiLU bf16", "discriminator": "64-256-1 SiLU"}
+
+
+def run_gan_b200(args, rank, world, dist) -> dict:
+    """Config 4: batched GAN steps (replicas under torchrun: rank r seeds r)."""
+    import torch
+
+    from quantom_loits_b200.gan import BatchedGANTrainer
+
+    dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
+    torch.cuda.set_device(dev)
+    tr = BatchedGANTrainer(dev, seed=rank)
+    stream = torch.cuda.current_stream(dev)
+    for _ in range(args.warmup):
+        tr.step()
+    torch.cuda.synchronize(dev)
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(dev.index) as clocks:
+        if dist is not None:
+            dist.barrier()
+        t0.record(stream)
+        for _ in range(args.steps):
+            d_loss, g_loss = tr.step()
+        t1.record(stream)
+        torch.cuda.synchronize(dev)
+    ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        ms = max_over_ranks(ms)
+    # the sampler alone on the same shapes: 2 histogram forwards + 1 VJP
+    values = tr.theory(tr.generator(tr.latent_noise())).detach().requires_grad_(True)
+    w = torch.randn((tr.batch, tr.bins), device=dev)
+
+    def sampler_only():
+        with torch.no_grad():
+            tr.histogram(values)
+        (tr.histogram(values) * w).sum().backward()
+
+    for _ in range(3):
+        sampler_only()
+    torch.cuda.synchronize(dev)
+    t0.record(stream)
+    for _ in range(args.steps):
+        sampler_only()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    s_ms = t0.elapsed_time(t1) / args.steps
+    # end to end: latent noise from pinned host memory, losses read back
+    h_z = torch.randn((2, tr.batch, tr.latent), generator=torch.Generator().manual_seed(1)).pin_memory()
+    h_loss = torch.empty(2).pin_memory()
+
+    def one():
+        z = h_z.to(dev, non_blocking=True)
+        d_l, g_l = tr.step(z[0], z[1])
+        h_loss.copy_(torch.stack([d_l, g_l]), non_blocking=True)
+
+    for _ in range(2):
+        one()
+    torch.cuda.synchronize(dev)
+    t0.record(stream)
+    for _ in range(args.steps):
+        one()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    e_ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        e_ms = max_over_ranks(e_ms)
+    ev_step = 2 * tr.batch * tr.n_events
+    return {
+        "metric": METRIC, "value": ev_step * world / (ms * 1e-3), "unit": "events/s",
+        "n_gpus": world, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {**describe_gan(tr), "events_per_step": ev_step,
+                   "parallelism": f"replicas x{world}", "launch": None},
+        "gan": {"steps_per_s": 1e3 / ms, "sampler_ms_per_step": s_ms,
+                "sampler_share": s_ms / ms, "d_loss": float(d_loss), "g_loss": float(g_loss)},
+        "e2e": {"value": ev_step * world / (e_ms * 1e-3), "unit": "events/s", "ms_per_step": e_ms,
+                "h2d_bytes_per_step": int(h_z.nbytes), "d2h_bytes_per_step": int(h_loss.nbytes),
+                "api": "BatchedGANTrainer.step"},
+        # per step: theory x2, theory VJP, histogram forward x2, histogram VJP
+        "gpu_launches": 6 * args.steps,
+        "clocks": clocks.summary(),
+        "cpu_baseline": {"value": None, "unit": "events/s", "cores": cpu_cores(),
+                         "kind": "reference", "sample": GAN_NO_REFERENCE},
+    }
+
+
+GAN_NO_REFERENCE = ("no reference counterpart: the reference GAN (pytorch/gan.py) trains one "
+                    "2-D theory on raw events; the batched histogram GAN step has no CPU path "
+                    "in the reference")
+
+
 def main(argv=None) -> int:
     ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
-    ap.add_argument("--workload", choices=["uniform", "single", "ragged", "precision", "tuple"],
+    ap.add_argument("--workload",
+                    choices=["uniform", "single", "ragged", "precision", "tuple", "gan"],
                     default="uniform")
     ap.add_argument("--events", type=int, default=0,
                     help="events per step of the tuple workload (default 1e7)")
@@ -728,13 +877,17 @@ def main(argv=None) -> int:
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
     world, rank, local = dist_env()
-    spec = workload_spec(args.workload, args.events)
-    is_tuple = args.workload == "tuple"
+    is_tuple, is_gan = args.workload == "tuple", args.workload == "gan"
+    spec = None if is_gan else workload_spec(args.workload, args.events)
 
     if args.impl == "reference":
         if rank != 0:
             return 0
-        out = run_tuple_reference(args, spec) if is_tuple else run_reference(args, spec)
+        if is_gan:
+            out = {"impl": "reference", "unavailable": GAN_NO_REFERENCE, "metric": METRIC,
+                   "config": {"workload": "gan"}}
+        else:
+            out = run_tuple_reference(args, spec) if is_tuple else run_reference(args, spec)
         print(json.dumps(out), flush=True)
         return 0
 
@@ -750,12 +903,14 @@ def main(argv=None) -> int:
                                  device_id=torch.device("cuda", local))
         dist = tdist
     try:
-        if is_tuple:
+        if is_gan:
+            out = run_gan_b200(args, rank, world, dist)
+        elif is_tuple:
             out = run_tuple_b200(args, spec, rank, world, dist)
         else:
             out = run_b200(args, spec, rank, world, dist)
         if rank == 0:
-            if world == 1 and not args.no_cpu_baseline:
+            if world == 1 and not args.no_cpu_baseline and not is_gan:
                 out["cpu_baseline"] = (tuple_cpu_baseline(args, spec) if is_tuple
                                        else cpu_baseline_leg(args, spec))
             print(json.dumps(out), flush=True)

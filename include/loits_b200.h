@@ -206,6 +206,46 @@ int loits_batch_cdf(const loits_batch_plan* plan, const void* workspace, double*
 int loits_batch_quantile(const loits_batch_plan* plan, const void* workspace, int64_t density,
                          const float* u, int64_t n, float* x, int32_t* intervals, void* stream);
 
+/* ------------------------------------------- histogram mode and theory
+ *
+ * For consumers that only need per-density histograms of the events (the
+ * discriminator of the batched GAN step), the sampler bins the kept events
+ * instead of compacting and writing them: no reference counterpart (the
+ * reference's GAN feeds raw events to its discriminator, pytorch/gan.py:11-24,
+ * :84-94).  Event x adds (1 - f) to bin k and f to bin k + 1, where
+ * k + f = (x - lo) / h - 1/2 and h = (hi - lo) / bins (triangular weights of
+ * bins centred at lo + (k + 1/2) h; weight outside the bins is dropped).  hist
+ * is B x bins fp32 and kept B int64 (kept events per density), both written
+ * (zeroed first) by the call; the sampled events are those of
+ * loits_batch_forward with the same seed and sequence.  1 <= bins <= 1024. */
+int loits_batch_forward_hist(const loits_batch_plan* plan, const float* grid, const float* values,
+                             const float* x_cut, uint64_t seed, uint64_t sequence, int32_t bins,
+                             float lo, float hi, float* hist, int64_t* kept, void* workspace,
+                             void* stream);
+
+/* VJP of loits_batch_forward_hist: grad_hist (B x bins) -> grad_values; each
+ * kept event's cotangent is (grad_hist[k + 1] - grad_hist[k]) / h.  Needs the
+ * workspace of a forward (either form) of the same plan, seed and sequence. */
+int loits_batch_backward_hist(const loits_batch_plan* plan, const float* grid, const float* values,
+                              const float* x_cut, uint64_t seed, uint64_t sequence, int32_t bins,
+                              float lo, float hi, const float* grad_hist, float* grad_values,
+                              void* workspace, void* stream);
+
+/* Two-component power-law theory of the batched GAN step (replaces, for
+ * batched densities, the theory map of pytorch/theory.py:37-126): params is
+ * B x 6 fp32 raw generator outputs p; with s(z) = 1 / (1 + e^-z),
+ *   a_i = -1/2 + 3/2 s(p[2i]), b_i = 1 + 4 s(p[2i+1]), w_i = log(1 + e^p[4+i]),
+ *   values[b][t] = sum_i w_i grid[t]^a_i (1 - grid[t])^b_i   (i = 0, 1),
+ * on a grid of `knots` points inside (0, 1] shared by all densities. */
+int loits_theory_powerlaw(int64_t n_densities, int64_t knots, const float* params,
+                          const float* grid, float* values, void* stream);
+
+/* VJP of loits_theory_powerlaw: grad_params[b][j] = sum_t grad_values[b][t]
+ * d values[b][t] / d params[b][j], summed in a fixed order. */
+int loits_theory_powerlaw_vjp(int64_t n_densities, int64_t knots, const float* params,
+                              const float* grid, const float* grad_values, float* grad_params,
+                              void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -158,6 +158,25 @@ class BatchPlan:
                 int(sequence), grad_events.data_ptr(), grad_values.data_ptr(),
                 workspace.data_ptr(), N.stream_of(self.device)), "loits_batch_backward")
 
+    def forward_hist(self, grid, values, x_cut, seed, sequence, bins, lo, hi, hist, kept,
+                     workspace) -> None:
+        """Histogram mode: bin the kept events (triangular weights, see
+        include/loits_b200.h) into hist (B x bins fp32); kept (B int64)."""
+        with torch.cuda.device(self.device):
+            N.check(self._lib.loits_batch_forward_hist(
+                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed),
+                int(sequence), int(bins), float(lo), float(hi), hist.data_ptr(), kept.data_ptr(),
+                workspace.data_ptr(), N.stream_of(self.device)), "loits_batch_forward_hist")
+
+    def backward_hist(self, grid, values, x_cut, seed, sequence, bins, lo, hi, grad_hist,
+                      grad_values, workspace) -> None:
+        with torch.cuda.device(self.device):
+            N.check(self._lib.loits_batch_backward_hist(
+                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed),
+                int(sequence), int(bins), float(lo), float(hi), grad_hist.data_ptr(),
+                grad_values.data_ptr(), workspace.data_ptr(), N.stream_of(self.device)),
+                "loits_batch_backward_hist")
+
     def check_status(self, workspace) -> None:
         """Synchronising read of the device status word."""
         N.check(int(self.status_view(workspace).item()), "batched sampler (device)")
@@ -222,6 +241,32 @@ class _BatchFunction(torch.autograd.Function):
         return grad_values, None, None, None, None, None
 
 
+class _HistFunction(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, values, grid, x_cut, plan: BatchPlan, seed, sequence, bins, lo, hi):
+        hist = torch.empty((plan.n_densities, bins), dtype=torch.float32, device=values.device)
+        kept = torch.empty(plan.n_densities, dtype=torch.int64, device=values.device)
+        ws = plan.new_workspace()
+        plan.forward_hist(grid, values, x_cut, seed, sequence, bins, lo, hi, hist, kept, ws)
+        ctx.plan, ctx.seed, ctx.sequence = plan, int(seed), int(sequence)
+        ctx.bins, ctx.lo, ctx.hi, ctx.x_cut = int(bins), float(lo), float(hi), x_cut
+        ctx.save_for_backward(values, grid, ws)
+        ctx.mark_non_differentiable(kept)
+        return hist, kept
+
+    @staticmethod
+    def backward(ctx, grad_hist, grad_kept):
+        values, grid, ws = ctx.saved_tensors
+        grad_values = torch.empty_like(values)
+        if grad_hist is None:
+            grad_values.zero_()
+        else:
+            ctx.plan.backward_hist(grid, values, ctx.x_cut, ctx.seed, ctx.sequence, ctx.bins,
+                                   ctx.lo, ctx.hi, grad_hist.to(torch.float32).contiguous(),
+                                   grad_values, ws)
+        return grad_values, None, None, None, None, None, None, None, None
+
+
 class BatchedLOITS:
     """Autograd-facing batched sampler: ``sample(batch) -> (events, row_offsets)``.
 
@@ -273,6 +318,28 @@ class BatchedLOITS:
         return _BatchFunction.apply(batch.values, grid, x_cut, plan, self.seed, sequence)
 
     __call__ = sample
+
+    def histogram(self, batch: DensityBatch, bins: int = 64, lo: float = 0.0, hi: float = 1.0,
+                  n_events=None, sequence=None):
+        """Per-density histograms of the events ``sample`` would return, binned
+        in the kernels without writing the events: ``(hist, kept)``, hist
+        (B, bins) fp32 of triangular weights on bins centred at
+        lo + (k + 1/2)(hi - lo)/bins, differentiable w.r.t. ``batch.values``;
+        kept (B,) int64 kept events per density."""
+        counts = batch.event_counts
+        if n_events is not None:
+            if isinstance(n_events, (int, np.integer)):
+                counts = np.full(batch.n_densities, int(n_events), dtype=np.int64)
+            else:
+                counts = _host_i64(n_events)
+        if sequence is None:
+            sequence = self.sequence
+            self.sequence += 1
+        plan = self.plan_for(batch.knot_offsets, counts, batch)
+        grid = batch.grid.detach().contiguous()
+        x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
+        return _HistFunction.apply(batch.values.contiguous(), grid, x_cut, plan, self.seed,
+                                   sequence, int(bins), float(lo), float(hi))
 
 
 class BatchStep:

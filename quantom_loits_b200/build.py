@@ -33,7 +33,7 @@ COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", f"-I{INCLUDE}
 PER_FILE = {"tuple_kernels.cu": ["-fmad=false"]}
 # The batched kernels are instantiated per CTA size in batch_inst_*.cu.
 SOURCES = ["capi.cu", "tuple_kernels.cu", "batch_plan.cu", "batch_export.cu", "batch_inst_256.cu",
-           "batch_inst_512.cu", "batch_inst_1024.cu"]
+           "batch_inst_512.cu", "batch_inst_1024.cu", "theory_kernels.cu"]
 
 
 def nvcc() -> str:

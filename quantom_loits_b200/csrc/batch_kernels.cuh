@@ -103,7 +103,18 @@ struct BatchArgs {
   // backward
   const float* grad;
   float* grad_values;
+  // histogram mode (events are binned instead of written; see hist_bin)
+  float* hist;                 // forward: [B * hist_bins], accumulated
+  unsigned long long* kept;    // forward: [B] kept events per density
+  const float* grad_hist;      // backward: [B * hist_bins]
+  int32_t hist_bins;
+  int32_t hist_smem_off;       // floats from the start of dynamic shared memory
+  float hist_lo, hist_inv_h;
 };
+
+// Histogram mode: shared copies of a tile's histogram, and the most bins.
+constexpr int kHistRep = 8;
+constexpr int kMaxHistBins = 1024;
 
 // Per-density flags (dflags):
 constexpr uint32_t kNonMonotone = 1u;  // an area is negative/NaN: count semantics

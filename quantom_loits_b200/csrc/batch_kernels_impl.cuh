@@ -856,6 +856,82 @@ __device__ __forceinline__ void sample_tile_general(const BatchArgs& a, int32_t 
   if (a.intervals) write_intervals<TPB, R, kMode>(a, tg, d, row0);
 }
 
+// ------------------------------------------------------- histogram mode
+//
+// Instead of compacting and writing the kept events, a histogram-mode launch
+// bins them: event x adds (1 - f) to bin k and f to bin k + 1 of its
+// density's histogram, where k + f = (x - lo) / h - 1/2 (bins of width h
+// centred at lo + (k + 1/2) h; weight falling outside the bins is dropped).
+// The weights are piecewise linear in x, so d hist_k / d x is defined almost
+// everywhere and the backward forms each event's cotangent from the
+// histogram's cotangent: (gh[k + 1] - gh[k]) / h.  Order does not matter to a
+// histogram: no compaction, no look-back, no event traffic.
+
+__device__ __forceinline__ void hist_bin(const BatchArgs& a, float x, int& k, float& f) {
+  float sc = __fmaf_rn(x - a.hist_lo, a.hist_inv_h, -0.5f);
+  sc = fminf(fmaxf(sc, -2.0f), static_cast<float>(a.hist_bins) + 1.0f);
+  const float fk = floorf(sc);
+  k = static_cast<int>(fk);
+  f = sc - fk;
+}
+
+__device__ __forceinline__ void hist_add(const BatchArgs& a, float* h, float x) {
+  int k;
+  float f;
+  hist_bin(a, x, k, f);
+  if (k >= 0 && k < a.hist_bins) atomicAdd(&h[k], 1.0f - f);
+  if (k + 1 >= 0 && k + 1 < a.hist_bins) atomicAdd(&h[k + 1], f);
+}
+
+__device__ __forceinline__ float hist_cotangent(const BatchArgs& a, const float* gh, float x) {
+  int k;
+  float f;
+  hist_bin(a, x, k, f);
+  const float g0 = (k >= 0 && k < a.hist_bins) ? gh[k] : 0.0f;
+  const float g1 = (k + 1 >= 0 && k + 1 < a.hist_bins) ? gh[k + 1] : 0.0f;
+  return (g1 - g0) * a.hist_inv_h;
+}
+
+// One tile in histogram mode: kept events go into kHistRep shared copies of
+// the density's histogram, merged into the global histogram at the end.
+template <int TPB, int R, int kMode>
+__device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileGeom& tg,
+                                                 const DensView& d, float* hs) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int nb = a.hist_bins, stride = nb + 1;
+  for (int i = threadIdx.x; i < kHistRep * stride; i += TPB) hs[i] = 0.0f;
+  __syncthreads();
+  float* mine = hs + (lane & (kHistRep - 1)) * stride;
+  const bool full = tile_full<TPB, R>(tg);
+  int kept = 0;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    const uint32_t range = d.skip ? 0u : (full ? 0xfu : block_range_mask(tg, blk));
+    if (!range) continue;
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+    const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+    const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
+    const uint32_t keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+    if (keep & 1u) hist_add(a, mine, e0.x);
+    if (keep & 2u) hist_add(a, mine, e1.x);
+    if (keep & 4u) hist_add(a, mine, e2.x);
+    if (keep & 8u) hist_add(a, mine, e3.x);
+    kept += __popc(keep);
+  }
+  kept = warp_sum(kept);
+  if (lane == 0 && kept) atomicAdd(&a.kept[tg.b], static_cast<unsigned long long>(kept));
+  __syncthreads();
+  float* out = a.hist + static_cast<int64_t>(tg.b) * nb;
+  for (int k = threadIdx.x; k < nb; k += TPB) {
+    float v = hs[k];
+#pragma unroll
+    for (int c = 1; c < kHistRep; ++c) v += hs[c * stride + k];
+    if (v != 0.0f) atomicAdd(&out[k], v);
+  }
+  __syncthreads();
+}
+
 // kLarge: the plan has densities above the shared-memory limit (compiled
 // separately so that plans without them carry none of the global-memory path).
 template <int TPB, int R, bool kLarge>
@@ -864,6 +940,13 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
   const TileGeom tg = tile_geom<TPB, R>(a, t);
   const bool large = kLarge && tg.G > a.gcap;
   density_flags(a, tg.b, large, true, sh);
+  if (a.hist) {
+    float* hs = reinterpret_cast<float*>(rec_s) + a.hist_smem_off;
+    const DensView d = density_view(a, tg.b, tg.k0, tg.G, large, rec_s, guide_s, nullptr, sh);
+    if (large) sample_tile_hist<TPB, R, kL2>(a, tg, d, hs);
+    else sample_tile_hist<TPB, R, kShared>(a, tg, d, hs);
+    return;
+  }
   if ((sh.flags & kAcceptAll) && threadIdx.x < 32) {
     // identity compaction: the count is known now, so the row look-back runs
     // while the other warps copy the density
@@ -911,10 +994,33 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
 template <int TPB, int R, int kMode>
 __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensView& d, TileGeom tg,
                                                 int32_t tb, int32_t t_first, int32_t t_end,
-                                                float* gacc_s, float2* gc) {
+                                                float* gacc_s, float2* gc, const float* gh) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (d.skip) return;
+  if (gh) {
+    // histogram mode: every kept slot's cotangent comes from the histogram's
+#pragma unroll 1
+    for (int32_t t = t_first; t < t_end; ++t) {
+      tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
+      const bool full = tile_full<TPB, R>(tg);
+#pragma unroll 1
+      for (int r = 0; r < R; ++r) {
+        const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+        const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
+        if (!range) continue;
+        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+        const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+        const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
+        const uint32_t keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+        if (keep & 1u) scatter_slot<kMode>(e0, hist_cotangent(a, gh, e0.x), d, gacc_s, gc);
+        if (keep & 2u) scatter_slot<kMode>(e1, hist_cotangent(a, gh, e1.x), d, gacc_s, gc);
+        if (keep & 4u) scatter_slot<kMode>(e2, hist_cotangent(a, gh, e2.x), d, gacc_s, gc);
+        if (keep & 8u) scatter_slot<kMode>(e3, hist_cotangent(a, gh, e3.x), d, gacc_s, gc);
+      }
+    }
+    return;
+  }
   if (d.accept_all) {
     // identity compaction: slot p of tile t is row p + (tile_prefix[t] - s_lo)
 #pragma unroll 1
@@ -995,10 +1101,17 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   const int32_t t_end = t_end0 < __ldg(&a.tile_first[b + 1]) ? t_end0 : __ldg(&a.tile_first[b + 1]);
   const TileGeom tg = tile_geom<TPB, R>(a, t_first);
   const int G = static_cast<int>(tg.G);
+  // histogram mode: the density's histogram cotangent, in shared memory
+  float* gh = nullptr;
+  if (a.grad_hist) {
+    gh = reinterpret_cast<float*>(rec_s) + a.hist_smem_off;
+    const float* src = a.grad_hist + static_cast<int64_t>(b) * a.hist_bins;
+    for (int k = threadIdx.x; k < a.hist_bins; k += TPB) gh[k] = __ldg(&src[k]);
+  }
   if (kLarge && tg.G > a.gcap) {
     const DensView d = load_density(a, b, tg.k0, tg.G, nullptr, nullptr, nullptr, false, sh);
     vjp_chunk_tiles<TPB, R, kRO>(a, d, tg, tb, t_first, t_end, nullptr,
-                                 a.gcdf + __ldg(&a.gc_off[b]));
+                                 a.gcdf + __ldg(&a.gc_off[b]), gh);
     // the density's grad-CDF atomics are performed before the chunk counts
     __threadfence();
     __syncthreads();
@@ -1015,7 +1128,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   for (int i = threadIdx.x; i < rep * stride; i += TPB) gacc_s[i] = 0.0f;
   const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
   float* gacc_lane = gacc_s + ((threadIdx.x & 31) & (rep - 1)) * stride;
-  vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_lane, nullptr);
+  vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_lane, nullptr, gh);
   __syncthreads();
   float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;
   for (int i = threadIdx.x; i < G; i += TPB) {

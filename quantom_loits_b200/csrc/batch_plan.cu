@@ -1,6 +1,7 @@
 // batch_plan.cu -- host side of the batched sampler: plans, workspace layout,
 // launches (persistent and one-launch-per-density), CDF export, quantiles.
 #include <algorithm>
+#include <cmath>
 #include <cstdint>
 #include <cstring>
 #include <mutex>
@@ -581,35 +582,21 @@ extern "C" int loits_batch_plan_config(const loits_batch_plan* p, loits_batch_co
   return LOITS_OK;
 }
 
-extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
-                                   const float* values, const float* x_cut, uint64_t seed,
-                                   uint64_t sequence, float* events, int64_t* row_offsets,
-                                   int32_t* intervals, void* workspace, void* stream) {
-  if (!p || !grid || !values || !row_offsets || !workspace) return LOITS_ERR_INVALID;
-  if (p->capacity > 0 && (!events || !aligned16(events))) return LOITS_ERR_INVALID;
-  if (!aligned16(workspace)) return LOITS_ERR_INVALID;
-  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
+namespace {
+
+// Forward launch(es) of a prepared argument block: one persistent launch, or
+// one launch per density (plain form).
+int launch_forward(const loits_batch_plan* p, BatchArgs& a, void* workspace, size_t smem,
+                   cudaStream_t st) {
   const Layout& L = p->lay;
   if (cudaMemsetAsync(static_cast<char*>(workspace) + L.fwd_zero_lo, 0,
                       L.fwd_zero_hi - L.fwd_zero_lo, st) != cudaSuccess)
     return LOITS_ERR_CUDA;
-  if (p->n_tiles == 0 &&
-      cudaMemsetAsync(row_offsets, 0, (p->nd + 1) * sizeof(int64_t), st) != cudaSuccess)
-    return LOITS_ERR_CUDA;
-  BatchArgs a = base_args(p, workspace);
-  a.seed = seed;
-  a.rk = philox_key(seed);
-  a.stream_id = 2 * sequence;
-  a.grid = grid;
-  a.values = values;
-  a.x_cut = x_cut;
-  a.events = events;
-  a.row_offsets = row_offsets;
-  a.intervals = intervals;
   FwdKernel fk;
   BwdKernel bk;
   kernels_for(p->tpb, p->r, p->has_large, fk, bk);
+  if (smem > p->fwd_smem && !allow_dynamic_smem(reinterpret_cast<const void*>(fk), smem))
+    return LOITS_ERR_CUDA;
   uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_fwd);
   if (!p->cfg.plain) {
     a.c_lo = 0; a.c_hi = p->n_cdf;
@@ -617,7 +604,7 @@ extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
     a.t_lo = 0; a.t_hi = p->n_tiles;
     a.d_lo = 0; a.d_hi = static_cast<int32_t>(p->nd);
     a.ticket = tickets + p->nd;
-    fk<<<p->fwd_grid, p->tpb, p->fwd_smem, st>>>(a);
+    fk<<<p->fwd_grid, p->tpb, smem, st>>>(a);
     return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
   }
   for (int64_t b = 0; b < p->nd; ++b) {
@@ -628,10 +615,82 @@ extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
     a.ticket = tickets + b;
     const int64_t items = (a.c_hi - a.c_lo) + (a.f_hi - a.f_lo) + (a.t_hi - a.t_lo);
     const int grid_b = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, p->fwd_grid)));
-    fk<<<grid_b, p->tpb, p->fwd_smem, st>>>(a);
+    fk<<<grid_b, p->tpb, smem, st>>>(a);
     if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
   }
   return LOITS_OK;
+}
+
+int launch_backward(const loits_batch_plan* p, BatchArgs& a, void* workspace, size_t smem,
+                    cudaStream_t st) {
+  const Layout& L = p->lay;
+  if (cudaMemsetAsync(static_cast<char*>(workspace) + L.bwd_zero_lo, 0,
+                      L.bwd_zero_hi - L.bwd_zero_lo, st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  a.gbits_cap = p->m_cap_b;
+  double* grho = carve<double>(workspace, L.grho);
+  FwdKernel fk;
+  BwdKernel bk;
+  kernels_for(p->tpb, p->r, p->has_large, fk, bk);
+  if (smem > p->bwd_smem && !allow_dynamic_smem(reinterpret_cast<const void*>(bk), smem))
+    return LOITS_ERR_CUDA;
+  uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_bwd);
+  if (!p->cfg.plain) {
+    a.k_lo = 0; a.k_hi = p->n_chunks;
+    a.d_lo = 0; a.d_hi = static_cast<int32_t>(p->nd);
+    a.l_lo = 0; a.l_hi = p->n_lfin;
+    a.ticket = tickets + p->nd;
+    bk<<<p->bwd_grid, p->tpb, smem, st>>>(a, grho);
+    return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
+  }
+  for (int64_t b = 0; b < p->nd; ++b) {
+    a.k_lo = p->chunk_first[b]; a.k_hi = p->chunk_first[b + 1];
+    a.d_lo = static_cast<int32_t>(b); a.d_hi = static_cast<int32_t>(b + 1);
+    a.l_lo = p->lfin_first[b]; a.l_hi = p->lfin_first[b + 1];
+    a.ticket = tickets + b;
+    const int64_t items = (a.k_hi - a.k_lo) + 1 + 2 * (a.l_hi - a.l_lo);
+    const int grid_b = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, p->bwd_grid)));
+    bk<<<grid_b, p->tpb, smem, st>>>(a, grho);
+    if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
+  }
+  return LOITS_OK;
+}
+
+BatchArgs step_args(const loits_batch_plan* p, void* workspace, const float* grid,
+                    const float* values, const float* x_cut, uint64_t seed, uint64_t sequence) {
+  BatchArgs a = base_args(p, workspace);
+  a.seed = seed;
+  a.rk = philox_key(seed);
+  a.stream_id = 2 * sequence;
+  a.grid = grid;
+  a.values = values;
+  a.x_cut = x_cut;
+  return a;
+}
+
+bool hist_range_ok(int32_t bins, float lo, float hi) {
+  return bins >= 1 && bins <= kMaxHistBins && std::isfinite(lo) && std::isfinite(hi) && lo < hi;
+}
+
+}  // namespace
+
+extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
+                                   const float* values, const float* x_cut, uint64_t seed,
+                                   uint64_t sequence, float* events, int64_t* row_offsets,
+                                   int32_t* intervals, void* workspace, void* stream) {
+  if (!p || !grid || !values || !row_offsets || !workspace) return LOITS_ERR_INVALID;
+  if (p->capacity > 0 && (!events || !aligned16(events))) return LOITS_ERR_INVALID;
+  if (!aligned16(workspace)) return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (p->n_tiles == 0 &&
+      cudaMemsetAsync(row_offsets, 0, (p->nd + 1) * sizeof(int64_t), st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.events = events;
+  a.row_offsets = row_offsets;
+  a.intervals = intervals;
+  return launch_forward(p, a, workspace, p->fwd_smem, st);
 }
 
 extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid,
@@ -642,45 +701,52 @@ extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid
   if (p->capacity > 0 && (!grad_events || !aligned16(grad_events))) return LOITS_ERR_INVALID;
   if (!aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  const Layout& L = p->lay;
-  if (cudaMemsetAsync(static_cast<char*>(workspace) + L.bwd_zero_lo, 0,
-                      L.bwd_zero_hi - L.bwd_zero_lo, st) != cudaSuccess)
-    return LOITS_ERR_CUDA;
-  BatchArgs a = base_args(p, workspace);
-  a.seed = seed;
-  a.rk = philox_key(seed);
-  a.stream_id = 2 * sequence;
-  a.grid = grid;
-  a.values = values;
-  a.x_cut = x_cut;
+  BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
   a.grad = grad_events;
   a.grad_values = grad_values;
-  a.gbits_cap = p->m_cap_b;
-  double* grho = carve<double>(workspace, L.grho);
-  FwdKernel fk;
-  BwdKernel bk;
-  kernels_for(p->tpb, p->r, p->has_large, fk, bk);
-  uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_bwd);
-  if (!p->cfg.plain) {
-    a.k_lo = 0; a.k_hi = p->n_chunks;
-    a.d_lo = 0; a.d_hi = static_cast<int32_t>(p->nd);
-    a.l_lo = 0; a.l_hi = p->n_lfin;
-    a.ticket = tickets + p->nd;
-    bk<<<p->bwd_grid, p->tpb, p->bwd_smem, st>>>(a, grho);
-    return cudaGetLastError() == cudaSuccess ? LOITS_OK : LOITS_ERR_CUDA;
-  }
-  for (int64_t b = 0; b < p->nd; ++b) {
-    a.k_lo = p->chunk_first[b]; a.k_hi = p->chunk_first[b + 1];
-    a.d_lo = static_cast<int32_t>(b); a.d_hi = static_cast<int32_t>(b + 1);
-    a.l_lo = p->lfin_first[b]; a.l_hi = p->lfin_first[b + 1];
-    a.ticket = tickets + b;
-    const int64_t items = (a.k_hi - a.k_lo) + 1 + 2 * (a.l_hi - a.l_lo);
-    const int grid_b = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items, p->bwd_grid)));
-    bk<<<grid_b, p->tpb, p->bwd_smem, st>>>(a, grho);
-    if (cudaGetLastError() != cudaSuccess) return LOITS_ERR_CUDA;
-  }
-  return LOITS_OK;
+  return launch_backward(p, a, workspace, p->bwd_smem, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* grid,
+                                        const float* values, const float* x_cut, uint64_t seed,
+                                        uint64_t sequence, int32_t bins, float lo, float hi,
+                                        float* hist, int64_t* kept, void* workspace,
+                                        void* stream) {
+  if (!p || !grid || !values || !hist || !kept || !workspace) return LOITS_ERR_INVALID;
+  if (!hist_range_ok(bins, lo, hi) || !aligned16(workspace)) return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (cudaMemsetAsync(hist, 0, static_cast<size_t>(p->nd) * bins * sizeof(float), st) != cudaSuccess ||
+      cudaMemsetAsync(kept, 0, static_cast<size_t>(p->nd) * sizeof(int64_t), st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.hist = hist;
+  a.kept = reinterpret_cast<unsigned long long*>(kept);
+  a.hist_bins = bins;
+  a.hist_lo = lo;
+  a.hist_inv_h = static_cast<float>(bins / (static_cast<double>(hi) - lo));
+  a.hist_smem_off = static_cast<int32_t>(p->fwd_smem / sizeof(float));
+  const size_t smem = p->fwd_smem + static_cast<size_t>(kHistRep) * (bins + 1) * sizeof(float);
+  return launch_forward(p, a, workspace, smem, st);
+}
+
+extern "C" int loits_batch_backward_hist(const loits_batch_plan* p, const float* grid,
+                                         const float* values, const float* x_cut, uint64_t seed,
+                                         uint64_t sequence, int32_t bins, float lo, float hi,
+                                         const float* grad_hist, float* grad_values,
+                                         void* workspace, void* stream) {
+  if (!p || !grid || !values || !grad_hist || !grad_values || !workspace) return LOITS_ERR_INVALID;
+  if (!hist_range_ok(bins, lo, hi) || !aligned16(workspace)) return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.grad_hist = grad_hist;
+  a.grad_values = grad_values;
+  a.hist_bins = bins;
+  a.hist_lo = lo;
+  a.hist_inv_h = static_cast<float>(bins / (static_cast<double>(hi) - lo));
+  a.hist_smem_off = static_cast<int32_t>(p->bwd_smem / sizeof(float));
+  const size_t smem = p->bwd_smem + static_cast<size_t>(bins) * sizeof(float);
+  return launch_backward(p, a, workspace, smem, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int loits_batch_cdf(const loits_batch_plan* p, const void* workspace, double* cdf,
