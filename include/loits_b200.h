@@ -120,19 +120,24 @@ int loits_tuple_sample_noalloc(const loits_shape* shape, const double* x_bins,
                                int64_t* packed, int16_t* interval_x, int16_t* interval_q,
                                int64_t* valid, int32_t* status, void* stream);
 
+/* Bytes of device workspace loits_tuple_backward needs for nvalid rows. */
+size_t loits_tuple_backward_workspace(const loits_shape* shape, int64_t nvalid);
+
 /* Replaces the pybind backward of cpp/bindings.cpp:132-208
  * (interpolation_vjp_x/q cpp/loits_core.cpp:268-338, cdf_vjp_x/q :340-398,
  * density_vjp_x/q :400-472).  grad_events: nvalid rows of 2; packed: the
  * forward's packed rows (ascending); uniforms and intervals are recomputed
  * from (seed, sequence) instead of being stored.  Writes every entry of
- * grad_xsec_x / grad_xsec_q (same shapes as xsec_x / xsec_q). */
+ * grad_xsec_x / grad_xsec_q (same shapes as xsec_x / xsec_q).  workspace:
+ * loits_tuple_backward_workspace() bytes of caller device memory (no
+ * initial contents needed); deterministic. */
 int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
                          const int64_t* packed, int64_t nvalid, int64_t nmax, uint64_t seed,
                          uint64_t sequence, const double* x_bins, const double* xsec_x,
                          const double* q_bins, const double* xsec_q, const uint8_t* acceptance,
                          const double* norm_x, const double* norm_q, const double* cdf_x,
                          const double* cdf_q, double* grad_xsec_x, double* grad_xsec_q,
-                         void* stream);
+                         void* workspace, size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------ batch (fp32, ragged 1-D) */
 

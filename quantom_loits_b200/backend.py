@@ -165,6 +165,8 @@ def tuple_backward(grad_events, x_bins, xsec_x, q_bins, xsec_q, acceptance, stat
         gx = torch.empty_like(xsec_x)
         gq = torch.empty_like(xsec_q)
         with _region(profile_regions, "loits::backward::fused", dev):
+            ws_bytes = int(lib.loits_tuple_backward_workspace(C.byref(shape), packed.numel()))
+            ws = torch.empty(max(ws_bytes, 16), dtype=torch.uint8, device=dev)
             N.check(lib.loits_tuple_backward(C.byref(shape), g.data_ptr(), packed.data_ptr(),
                                              packed.numel(), int(state["nmax"]), int(seed),
                                              int(sequence), x_bins.data_ptr(), xsec_x.data_ptr(),
@@ -172,7 +174,8 @@ def tuple_backward(grad_events, x_bins, xsec_x, q_bins, xsec_q, acceptance, stat
                                              acceptance.view(torch.uint8).data_ptr(),
                                              state["norm_x"].data_ptr(), state["norm_q"].data_ptr(),
                                              state["cdf_x"].data_ptr(), state["cdf_q"].data_ptr(),
-                                             gx.data_ptr(), gq.data_ptr(), N.stream_of(dev)),
+                                             gx.data_ptr(), gq.data_ptr(), ws.data_ptr(),
+                                             ws.numel(), N.stream_of(dev)),
                     "loits_tuple_backward")
         with _region(profile_regions, "loits::backward::state_pack"):
             pass

@@ -17,9 +17,12 @@
 //   tuple_sample_kernel    fill_uniform + interpolate :167-237 + compact :239-266
 //                          fused; uniforms live in registers only; stable
 //                          compaction by decoupled look-back over ordered tiles
-//   tuple_backward_kernel  interpolation_vjp :268-338 + cdf_vjp :340-398 +
-//                          density_vjp :400-472, one warp per cell,
-//                          deterministic (fixed-order warp reductions)
+//   tuple_rows_kernel,     interpolation_vjp :268-338 + cdf_vjp :340-398 +
+//   tuple_chunk_kernel,    density_vjp :400-472: rows cut into chunks of at
+//   tuple_cell_kernel      most 256 rows per cell, one warp per chunk with
+//                          lane-private accumulators, per-cell ordered sum of
+//                          the chunk partials, then the reverse chain;
+//                          deterministic (every sum has a fixed order)
 #include <cmath>
 #include <cstdint>
 #include <mutex>
@@ -332,63 +335,165 @@ __device__ void curve_chain(const double* __restrict__ bins, const double* __res
   }
 }
 
-// dynamic smem: warps_per_block * (kx + kq) doubles
-__global__ void tuple_backward_kernel(TupleBackwardArgs a) {
+// The backward is balanced over rows, not cells (cell sizes follow the
+// weights and differ by an order of magnitude): a cell's kept rows are cut
+// into chunks of at most kChunkRows rows, each chunk's grad-CDF partial is
+// formed by one warp, and each cell sums its chunks' partials in chunk order
+// before the reverse chain -- every sum has a fixed order (deterministic).
+constexpr int kChunkRows = 256;
+
+// Per cell: first kept row (lower bound of its first padded slot in the
+// strictly increasing packed rows) and its number of chunks.
+__global__ void tuple_rows_kernel(TupleBackwardArgs a, int64_t* __restrict__ cell_rows,
+                                  int64_t* __restrict__ chunks) {
+  const int64_t ncell = a.g.batch * a.g.cells;
+  for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= ncell;
+       c += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t r0 = lower_bound_i64(a.packed, a.nvalid, c * a.nmax);
+    cell_rows[c] = r0;
+    if (c < ncell) {
+      const int64_t r1 = lower_bound_i64(a.packed, a.nvalid, (c + 1) * a.nmax);
+      chunks[c] = (r1 - r0 + kChunkRows - 1) / kChunkRows;
+    }
+  }
+}
+
+// Grad-CDF contributions of one row, in the order of its four targets
+// (x knot jx, jx+1, q knot jq, jq+1).
+struct RowVjp {
+  int jx, jq;
+  double ax, bx, aq, bq;
+};
+
+__device__ __forceinline__ RowVjp row_vjp(const TupleBackwardArgs& a, int64_t r, const double* xb,
+                                          const double* xc, const double* qb, const double* qc) {
+  RowVjp o;
+  const int64_t p = a.packed[r];
+  const uint64_t blk = static_cast<uint64_t>(p) >> 2;
+  const double ux =
+      static_cast<double>(uniform_from_bits(word_of(philox4x32_10(blk, a.stream_x, a.seed), p & 3)));
+  const double uq =
+      static_cast<double>(uniform_from_bits(word_of(philox4x32_10(blk, a.stream_q, a.seed), p & 3)));
+  o.jx = interval_count(xc, a.g.kx, ux);
+  o.jq = interval_count(qc, a.g.kq, uq);
+  value_vjp(xb, xc, o.jx, ux, a.grad[2 * r], o.ax, o.bx);
+  value_vjp(qb, qc, o.jq, uq, a.grad[2 * r + 1], o.aq, o.bq);
+  return o;
+}
+
+struct CellCurves {
+  int64_t xi;
+  const double *xc, *xb, *qc, *qb;
+};
+
+__device__ __forceinline__ CellCurves cell_curves(const TupleBackwardArgs& a, int64_t gc) {
+  CellCurves cc;
+  const int64_t b = gc / a.g.cells, cell = gc - b * a.g.cells;
+  const int64_t ix = cell / a.g.ny, iy = cell - ix * a.g.ny;
+  cc.xi = (b * a.g.ny + iy) * a.g.nx + ix;
+  cc.xc = a.cdf_x + cc.xi * a.g.kx;
+  cc.xb = a.x_bins + (b * a.g.nx + ix) * a.g.kx;
+  cc.qc = a.cdf_q + gc * a.g.kq;
+  cc.qb = a.q_bins + (b * a.g.ny + iy) * a.g.kq;
+  return cc;
+}
+
+// One warp per chunk.  Lane-private accumulators (kx + kq doubles per lane,
+// stride kx + kq + 1) in shared memory take each lane's rows in order; the
+// chunk partial is their fixed-order sum over lanes.  Large K (lane copies
+// would not fit) uses per-knot warp reductions instead.
+__global__ void tuple_chunk_kernel(TupleBackwardArgs a, const int64_t* __restrict__ cell_rows,
+                                   const int64_t* __restrict__ chunk_first,
+                                   const int64_t* __restrict__ n_chunks,
+                                   double* __restrict__ partials, int lane_private) {
   extern __shared__ double s_acc[];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int wpb = blockDim.x >> 5;
+  const int64_t k = static_cast<int64_t>(blockIdx.x) * wpb + warp;
+  if (k >= *n_chunks) return;  // whole warp leaves together
+  const int64_t ncell = a.g.batch * a.g.cells;
+  // owner cell: last c with chunk_first[c] <= k
+  int64_t lo = 0, hi = ncell;
+  while (hi - lo > 1) {
+    const int64_t mid = (lo + hi) >> 1;
+    if (chunk_first[mid] <= k) lo = mid; else hi = mid;
+  }
+  const int64_t gc = lo;
+  const int64_t r_begin = cell_rows[gc] + (k - chunk_first[gc]) * kChunkRows;
+  const int64_t r_end0 = r_begin + kChunkRows;
+  const int64_t r_end = r_end0 < cell_rows[gc + 1] ? r_end0 : cell_rows[gc + 1];
+  const CellCurves cc = cell_curves(a, gc);
+  const int64_t kx = a.g.kx, kq = a.g.kq, kt = kx + kq;
+  double* out = partials + k * kt;
+  if (lane_private) {
+    const int64_t stride = kt + 1;
+    double* base = s_acc + static_cast<int64_t>(warp) * 32 * stride;
+    double* mine = base + lane * stride;
+    for (int64_t t = 0; t < kt; ++t) mine[t] = 0.0;
+    for (int64_t r = r_begin + lane; r < r_end; r += 32) {
+      const RowVjp v = row_vjp(a, r, cc.xb, cc.xc, cc.qb, cc.qc);
+      mine[v.jx] += v.ax;
+      mine[v.jx + 1] += v.bx;
+      mine[kx + v.jq] += v.aq;
+      mine[kx + v.jq + 1] += v.bq;
+    }
+    __syncwarp();
+    for (int64_t t = lane; t < kt; t += 32) {
+      double sum = 0.0;
+      for (int l = 0; l < 32; ++l) sum += base[l * stride + t];
+      out[t] = sum;
+    }
+  } else {
+    double* acc = s_acc + static_cast<int64_t>(warp) * kt;
+    for (int64_t t = lane; t < kt; t += 32) acc[t] = 0.0;
+    __syncwarp();
+    for (int64_t r0 = r_begin; r0 < r_end; r0 += 32) {
+      const int64_t r = r0 + lane;
+      RowVjp v{-2, -2, 0.0, 0.0, 0.0, 0.0};
+      if (r < r_end) v = row_vjp(a, r, cc.xb, cc.xc, cc.qb, cc.qc);
+      for (int64_t t = 0; t < kx; ++t) {
+        double x = (v.jx == t ? v.ax : 0.0) + (v.jx + 1 == t ? v.bx : 0.0);
+        x = warp_sum(x);
+        if (lane == 0) acc[t] += x;
+      }
+      for (int64_t t = 0; t < kq; ++t) {
+        double x = (v.jq == t ? v.aq : 0.0) + (v.jq + 1 == t ? v.bq : 0.0);
+        x = warp_sum(x);
+        if (lane == 0) acc[kx + t] += x;
+      }
+    }
+    __syncwarp();
+    for (int64_t t = lane; t < kt; t += 32) out[t] = acc[t];
+  }
+}
+
+// One warp per cell: its chunks' partials summed in chunk order (lane t owns
+// knot t), then the reverse chain of each curve (cpp/loits_core.cpp:340-472).
+__global__ void tuple_cell_kernel(TupleBackwardArgs a, const int64_t* __restrict__ chunk_first,
+                                  const double* __restrict__ partials) {
+  extern __shared__ double s_gc[];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int wpb = blockDim.x >> 5;
   const int64_t gc = static_cast<int64_t>(blockIdx.x) * wpb + warp;
   const int64_t ncell = a.g.batch * a.g.cells;
-  if (gc >= ncell) return;  // whole warp leaves together
-  const int64_t kx = a.g.kx, kq = a.g.kq;
-  double* acc_x = s_acc + warp * (kx + kq);
-  double* acc_q = acc_x + kx;
-  for (int64_t t = lane; t < kx + kq; t += 32) acc_x[t] = 0.0;
-
-  const int64_t b = gc / a.g.cells, cell = gc - b * a.g.cells;
-  const int64_t ix = cell / a.g.ny, iy = cell - ix * a.g.ny;
-  const int64_t xi = (b * a.g.ny + iy) * a.g.nx + ix;
-  const double* xc = a.cdf_x + xi * kx;
-  const double* xb = a.x_bins + (b * a.g.nx + ix) * kx;
-  const double* qc = a.cdf_q + gc * kq;
-  const double* qb = a.q_bins + (b * a.g.ny + iy) * kq;
-  const int64_t r0 = lower_bound_i64(a.packed, a.nvalid, gc * a.nmax);
-  const int64_t r1 = lower_bound_i64(a.packed, a.nvalid, (gc + 1) * a.nmax);
-  __syncwarp();
-  for (int64_t base = r0; base < r1; base += 32) {
-    const int64_t r = base + lane;
-    int jx = -2, jq = -2;
-    double ax = 0.0, bx = 0.0, aq = 0.0, bq = 0.0;
-    if (r < r1) {
-      const int64_t p = a.packed[r];
-      const uint64_t blk = static_cast<uint64_t>(p) >> 2;
-      const double ux =
-          static_cast<double>(uniform_from_bits(word_of(philox4x32_10(blk, a.stream_x, a.seed), p & 3)));
-      const double uq =
-          static_cast<double>(uniform_from_bits(word_of(philox4x32_10(blk, a.stream_q, a.seed), p & 3)));
-      jx = interval_count(xc, kx, ux);
-      jq = interval_count(qc, kq, uq);
-      value_vjp(xb, xc, jx, ux, a.grad[2 * r], ax, bx);
-      value_vjp(qb, qc, jq, uq, a.grad[2 * r + 1], aq, bq);
-    }
-    // fixed-order warp reductions per knot: deterministic accumulation
-    for (int64_t t = 0; t < kx; ++t) {
-      double v = (jx == t ? ax : 0.0) + (jx + 1 == t ? bx : 0.0);
-      v = warp_sum(v);
-      if (lane == 0) acc_x[t] += v;
-    }
-    for (int64_t t = 0; t < kq; ++t) {
-      double v = (jq == t ? aq : 0.0) + (jq + 1 == t ? bq : 0.0);
-      v = warp_sum(v);
-      if (lane == 0) acc_q[t] += v;
-    }
+  if (gc >= ncell) return;
+  const int64_t kx = a.g.kx, kq = a.g.kq, kt = kx + kq;
+  double* acc = s_gc + static_cast<int64_t>(warp) * kt;
+  const int64_t k0 = chunk_first[gc], k1 = chunk_first[gc + 1];
+  for (int64_t t = lane; t < kt; t += 32) {
+    double sum = 0.0;
+    for (int64_t k = k0; k < k1; ++k) sum += partials[k * kt + t];
+    acc[t] = sum;
   }
   __syncwarp();
-  const double acc = a.acceptance[gc] ? 1.0 : 0.0;
+  const CellCurves cc = cell_curves(a, gc);
+  const double acc_cell = a.acceptance[gc] ? 1.0 : 0.0;
   if (lane == 0) {
-    curve_chain(xb, a.xsec_x + xi * kx, a.norm_x[xi], acc, acc_x, kx, a.grad_x + xi * kx);
+    curve_chain(cc.xb, a.xsec_x + cc.xi * kx, a.norm_x[cc.xi], acc_cell, acc, kx,
+                a.grad_x + cc.xi * kx);
   } else if (lane == 1) {
-    curve_chain(qb, a.xsec_q + gc * kq, a.norm_q[gc], acc, acc_q, kq, a.grad_q + gc * kq);
+    curve_chain(cc.qb, a.xsec_q + gc * kq, a.norm_q[gc], acc_cell, acc + kx, kq,
+                a.grad_q + gc * kq);
   }
 }
 
@@ -502,6 +607,41 @@ extern "C" int loits_tuple_sample(const loits_shape* shape, const double* x_bins
   return launch_status(cudaGetLastError());
 }
 
+namespace {
+
+// Workspace of the tuple backward: cell row starts, chunk counts and offsets,
+// the scan's {max, total}, and one grad-CDF partial per chunk.
+struct BackwardLayout {
+  size_t cell_rows, chunks, chunk_first, alloc, partials, total;
+  int64_t max_chunks;
+};
+
+BackwardLayout backward_layout(const TupleGeom& g, int64_t nvalid) {
+  BackwardLayout L{};
+  const int64_t ncell = g.batch * g.cells;
+  L.max_chunks = nvalid / kChunkRows + ncell;
+  size_t o = 0;
+  auto take = [&o](size_t bytes) {
+    const size_t at = o;
+    o = (o + bytes + 255) / 256 * 256;
+    return at;
+  };
+  L.cell_rows = take(static_cast<size_t>(ncell + 1) * 8);
+  L.chunks = take(static_cast<size_t>(ncell) * 8);
+  L.chunk_first = take(static_cast<size_t>(ncell + 1) * 8);
+  L.alloc = take(16);
+  L.partials = take(static_cast<size_t>(L.max_chunks) * (g.kx + g.kq) * 8);
+  L.total = o;
+  return L;
+}
+
+}  // namespace
+
+extern "C" size_t loits_tuple_backward_workspace(const loits_shape* shape, int64_t nvalid) {
+  if (!valid_shape(shape) || nvalid < 0) return 0;
+  return backward_layout(geom_of(shape), nvalid).total;
+}
+
 extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
                                     const int64_t* packed, int64_t nvalid, int64_t nmax,
                                     uint64_t seed, uint64_t sequence, const double* x_bins,
@@ -509,16 +649,19 @@ extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad
                                     const double* xsec_q, const uint8_t* acceptance,
                                     const double* norm_x, const double* norm_q,
                                     const double* cdf_x, const double* cdf_q,
-                                    double* grad_xsec_x, double* grad_xsec_q, void* stream) {
+                                    double* grad_xsec_x, double* grad_xsec_q, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
   if (!valid_shape(shape) || nvalid < 0 || nmax < 0) return LOITS_ERR_INVALID;
-  if (shape->kx > 32767 || shape->kq > 32767) return LOITS_ERR_UNSUPPORTED;
   const TupleGeom g = geom_of(shape);
   const int64_t ncell = g.batch * g.cells;
   if (ncell == 0) return LOITS_OK;
   if (!x_bins || !xsec_x || !q_bins || !xsec_q || !acceptance || !norm_x || !norm_q || !cdf_x ||
-      !cdf_q || !grad_xsec_x || !grad_xsec_q || (nvalid > 0 && (!grad_events || !packed)))
+      !cdf_q || !grad_xsec_x || !grad_xsec_q || !workspace ||
+      (nvalid > 0 && (!grad_events || !packed)))
     return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  const BackwardLayout L = backward_layout(g, nvalid);
+  if (workspace_bytes < L.total) return LOITS_ERR_CAPACITY;
   TupleBackwardArgs a;
   a.g = g;
   a.grad = grad_events;
@@ -539,20 +682,47 @@ extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad
   a.cdf_q = cdf_q;
   a.grad_x = grad_xsec_x;
   a.grad_q = grad_xsec_q;
-  const size_t per_warp = static_cast<size_t>(g.kx + g.kq) * sizeof(double);
+  char* ws = static_cast<char*>(workspace);
+  int64_t* cell_rows = reinterpret_cast<int64_t*>(ws + L.cell_rows);
+  int64_t* chunks = reinterpret_cast<int64_t*>(ws + L.chunks);
+  int64_t* chunk_first = reinterpret_cast<int64_t*>(ws + L.chunk_first);
+  int64_t* alloc = reinterpret_cast<int64_t*>(ws + L.alloc);
+  double* partials = reinterpret_cast<double*>(ws + L.partials);
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  const int64_t kt = g.kx + g.kq;
+  tuple_rows_kernel<<<grid_for(ncell + 1, 256), 256, 0, st>>>(a, cell_rows, chunks);
+  cell_scan_kernel<<<1, kScanThreads, 0, st>>>(chunks, ncell, chunk_first, alloc);
+  // chunk partials: lane-private accumulators when 32 copies fit
+  const size_t lane_bytes = static_cast<size_t>(32) * (kt + 1) * sizeof(double);
+  const bool lane_private = lane_bytes <= 24 * 1024;
+  const size_t per_warp = lane_private ? lane_bytes : static_cast<size_t>(kt) * sizeof(double);
   int wpb = 8;
   while (wpb > 1 && per_warp * wpb > 48 * 1024) wpb >>= 1;
-  const size_t smem = per_warp * wpb;
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
-  if (smem > 48 * 1024) {
-    if (smem > 200 * 1024) return LOITS_ERR_UNSUPPORTED;
-    if (cudaFuncSetAttribute(tuple_backward_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             static_cast<int>(smem)) != cudaSuccess)
-      return LOITS_ERR_CUDA;
-  }
-  const int64_t blocks = (ncell + wpb - 1) / wpb;
+  size_t smem = per_warp * wpb;
+  if (smem > 200 * 1024) return LOITS_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(tuple_chunk_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  const int64_t cblocks = (L.max_chunks + wpb - 1) / wpb;
+  if (cblocks > 0x7fffffff) return LOITS_ERR_UNSUPPORTED;
+  if (cblocks > 0)
+    tuple_chunk_kernel<<<static_cast<unsigned>(cblocks), wpb * 32, smem, st>>>(
+        a, cell_rows, chunk_first, alloc + 1, partials, lane_private ? 1 : 0);
+  // per cell: ordered sum of its chunks, reverse chain
+  const size_t cell_warp = static_cast<size_t>(kt) * sizeof(double);
+  int wpc = 8;
+  while (wpc > 1 && cell_warp * wpc > 48 * 1024) wpc >>= 1;
+  smem = cell_warp * wpc;
+  if (smem > 200 * 1024) return LOITS_ERR_UNSUPPORTED;
+  if (smem > 48 * 1024 &&
+      cudaFuncSetAttribute(tuple_cell_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                           static_cast<int>(smem)) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  const int64_t blocks = (ncell + wpc - 1) / wpc;
   if (blocks > 0x7fffffff) return LOITS_ERR_UNSUPPORTED;
-  tuple_backward_kernel<<<static_cast<unsigned>(blocks), wpb * 32, smem, st>>>(a);
+  tuple_cell_kernel<<<static_cast<unsigned>(blocks), wpc * 32, smem, st>>>(a, chunk_first,
+                                                                          partials);
   return launch_status(cudaGetLastError());
 }
 

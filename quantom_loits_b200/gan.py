@@ -120,8 +120,9 @@ class BatchedGANTrainer:
         self.knot_offsets = np.arange(batch + 1, dtype=np.int64) * grid_size
         self.event_counts = np.full(batch, self.n_events, dtype=np.int64)
         self.loss = nn.BCEWithLogitsLoss()
-        self.d_optimizer = torch.optim.Adam(self.discriminator.parameters(), lr=lr)
-        self.g_optimizer = torch.optim.Adam(self.generator.parameters(), lr=lr)
+        # one fused multi-tensor kernel per optimizer step instead of one per tensor
+        self.d_optimizer = torch.optim.Adam(self.discriminator.parameters(), lr=lr, fused=True)
+        self.g_optimizer = torch.optim.Adam(self.generator.parameters(), lr=lr, fused=True)
         self.gen = torch.Generator(device=self.device).manual_seed(int(seed) + 1)
         # target theory: fixed raw parameters, the same for every density
         target = torch.tensor([[0.4, -0.3, -1.2, 0.8, 0.5, -0.2]], dtype=torch.float32,

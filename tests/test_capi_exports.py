@@ -42,6 +42,18 @@ def test_library_exports_every_declared_symbol(native):
     assert set(declared_symbols()) <= set(native.SIGNATURES)
 
 
+def test_bindings_match_header_arity(native):
+    """Every ctypes binding passes as many arguments as the header declares."""
+    text = re.sub(r"/\*.*?\*/", "", HEADER.read_text(), flags=re.S)
+    seen = 0
+    for m in re.finditer(r"\b(loits_[a-z0-9_]+)\s*\(([^;{]*?)\)\s*;", text):
+        name, args = m.group(1), m.group(2).strip()
+        n = 0 if args in ("", "void") else len(args.split(","))
+        assert len(native.SIGNATURES[name][1]) == n, name
+        seen += 1
+    assert seen == len(declared_symbols())
+
+
 def test_status_strings(native):
     lib = native.lib()
     assert lib.loits_status_string(0) == b"ok"
