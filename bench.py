@@ -716,6 +716,13 @@ def run_tuple_b200(args, spec, rank, world, dist) -> dict:
     peak, peak_kind = hbm_peak()
     k_bytes = TUPLE_B_PER_EVENT * valid
     achieved = k_bytes / (k_ms * 1e-3) / 1e9
+    traffic = None
+    try:
+        entry = json.loads(TRAFFIC.read_text()).get("tuple", {}).get(kname)
+        if entry:
+            traffic = entry["bytes_per_launch"] * valid / entry["kept_events"]
+    except Exception:
+        pass
     out = {
         "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
@@ -728,7 +735,7 @@ def run_tuple_b200(args, spec, rank, world, dist) -> dict:
         "kernels_ms": {"forward (prepare + sample)": fm, "backward": bm},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "algorithmic_bytes": k_bytes},
+                     "traffic": traffic, "algorithmic_bytes": k_bytes},
         "e2e": {"value": spec.n_events * world / (e_ms * 1e-3), "unit": "events/s",
                 "ms_per_step": e_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "LOITS(backend='cuda')(theory_outputs, n_events) + autograd backward"},
