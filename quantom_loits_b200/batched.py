@@ -286,7 +286,7 @@ class BatchedLOITS:
         self.sequence = 0
         self._plans: dict = {}
 
-    def plan_for(self, knot_offsets, event_counts, batch=None) -> BatchPlan:
+    def plan_for(self, knot_offsets, event_counts, batch=None, hist=None) -> BatchPlan:
         key = (knot_offsets.tobytes(), event_counts.tobytes())
         plan = self._plans.get(key)
         if plan is None:
@@ -297,7 +297,7 @@ class BatchedLOITS:
                 from .tuning import default_tuner
 
                 config = make_config(**default_tuner(self.device).config_for(
-                    batch, event_counts, self.seed, self.sequence))
+                    batch, event_counts, self.seed, self.sequence, hist))
             plan = BatchPlan(knot_offsets, event_counts, config, self.device)
             self._plans[key] = plan
         return plan
@@ -335,7 +335,7 @@ class BatchedLOITS:
         if sequence is None:
             sequence = self.sequence
             self.sequence += 1
-        plan = self.plan_for(batch.knot_offsets, counts, batch)
+        plan = self.plan_for(batch.knot_offsets, counts, batch, (bins, lo, hi))
         grid = batch.grid.detach().contiguous()
         x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
         return _HistFunction.apply(batch.values.contiguous(), grid, x_cut, plan, self.seed,

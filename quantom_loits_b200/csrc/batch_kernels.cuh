@@ -108,13 +108,15 @@ struct BatchArgs {
   unsigned long long* kept;    // forward: [B] kept events per density
   const float* grad_hist;      // backward: [B * hist_bins]
   int32_t hist_bins;
+  int32_t hist_rep;            // shared copies of a tile's histogram (lane % rep), power of 2
   int32_t hist_smem_off;       // floats from the start of dynamic shared memory
   float hist_lo, hist_inv_h;
 };
 
-// Histogram mode: shared copies of a tile's histogram, and the most bins.
-constexpr int kHistRep = 8;
+// Histogram mode: the most bins, and the shared memory a tile's copies of
+// its histogram may take (one copy per lane when they fit).
 constexpr int kMaxHistBins = 1024;
+constexpr int kHistSmemBytes = 16 * 1024;
 
 // Per-density flags (dflags):
 constexpr uint32_t kNonMonotone = 1u;  // an area is negative/NaN: count semantics

@@ -892,16 +892,18 @@ __device__ __forceinline__ float hist_cotangent(const BatchArgs& a, const float*
   return (g1 - g0) * a.hist_inv_h;
 }
 
-// One tile in histogram mode: kept events go into kHistRep shared copies of
-// the density's histogram, merged into the global histogram at the end.
+// One tile in histogram mode: kept events go into `hist_rep` shared copies
+// of the density's histogram (lane l into copy l % rep; copies of one bin
+// fall in different banks), merged into the global histogram at the end.
 template <int TPB, int R, int kMode>
 __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileGeom& tg,
                                                  const DensView& d, float* hs) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nb = a.hist_bins, stride = nb + 1;
-  for (int i = threadIdx.x; i < kHistRep * stride; i += TPB) hs[i] = 0.0f;
+  const int rep = a.hist_rep;
+  for (int i = threadIdx.x; i < rep * stride; i += TPB) hs[i] = 0.0f;
   __syncthreads();
-  float* mine = hs + (lane & (kHistRep - 1)) * stride;
+  float* mine = hs + (lane & (rep - 1)) * stride;
   const bool full = tile_full<TPB, R>(tg);
   int kept = 0;
 #pragma unroll 1
@@ -925,8 +927,7 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   float* out = a.hist + static_cast<int64_t>(tg.b) * nb;
   for (int k = threadIdx.x; k < nb; k += TPB) {
     float v = hs[k];
-#pragma unroll
-    for (int c = 1; c < kHistRep; ++c) v += hs[c * stride + k];
+    for (int c = 1; c < rep; ++c) v += hs[c * stride + k];
     if (v != 0.0f) atomicAdd(&out[k], v);
   }
   __syncthreads();

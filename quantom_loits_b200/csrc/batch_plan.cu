@@ -726,7 +726,11 @@ extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* 
   a.hist_lo = lo;
   a.hist_inv_h = static_cast<float>(bins / (static_cast<double>(hi) - lo));
   a.hist_smem_off = static_cast<int32_t>(p->fwd_smem / sizeof(float));
-  const size_t smem = p->fwd_smem + static_cast<size_t>(kHistRep) * (bins + 1) * sizeof(float);
+  int rep = 1;
+  while (rep < 32 && 2 * rep * (bins + 1) * sizeof(float) <= static_cast<size_t>(kHistSmemBytes))
+    rep *= 2;
+  a.hist_rep = rep;
+  const size_t smem = p->fwd_smem + static_cast<size_t>(rep) * (bins + 1) * sizeof(float);
   return launch_forward(p, a, workspace, smem, st);
 }
 

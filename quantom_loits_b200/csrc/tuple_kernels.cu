@@ -181,7 +181,8 @@ struct TupleSampleArgs {
   int64_t n_tiles;
 };
 
-__global__ void __launch_bounds__(kSampleThreads) tuple_sample_kernel(TupleSampleArgs a) {
+// Three CTAs per SM (80 registers, no spills) instead of two at 118.
+__global__ void __launch_bounds__(kSampleThreads, 3) tuple_sample_kernel(TupleSampleArgs a) {
   __shared__ long long s_scan[kSampleThreads / 32 + 1];
   __shared__ long long s_base;
   __shared__ uint32_t s_tile;

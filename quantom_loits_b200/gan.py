@@ -103,7 +103,7 @@ class BatchedGANTrainer:
 
     def __init__(self, device="cuda", batch: int = 256, n_events: int = 200_000,
                  grid_size: int = 2048, bins: int = 64, latent: int = 64, lr: float = 1e-4,
-                 seed: int = 0, config=None, profile_regions: bool = False):
+                 seed: int = 0, config="auto", profile_regions: bool = False):
         self.device = torch.device(device)
         N.require_device(self.device)
         torch.manual_seed(int(seed))

@@ -70,23 +70,27 @@ class Autotuner:
             except (OSError, ValueError):
                 pass
 
-    def config_for(self, batch, event_counts=None, seed: int = 0, sequence: int = 0) -> dict:
+    def config_for(self, batch, event_counts=None, seed: int = 0, sequence: int = 0,
+                   hist=None) -> dict:
         """The tuned configuration (a dict for ``make_config``) for this
-        batch's shape bucket, timing the candidates on first use."""
+        batch's shape bucket, timing the candidates on first use.  hist:
+        (bins, lo, hi) to time the histogram mode instead of event writing."""
         counts = batch.event_counts if event_counts is None else np.asarray(event_counts, np.int64)
         key = shape_key(batch.knot_offsets, counts, batch.x_cut is not None)
+        if hist is not None:
+            key += f"-hist{int(hist[0])}"
         with self._lock:
             hit = self.table.get(key)
         if hit is not None:
             return dict(hit)
-        best, times = self.tune(batch, counts, seed, sequence)
+        best, times = self.tune(batch, counts, seed, sequence, hist)
         with self._lock:
             self.table[key] = best
             self.timings[key] = times
             self._save()
         return dict(best)
 
-    def tune(self, batch, event_counts, seed: int = 0, sequence: int = 0):
+    def tune(self, batch, event_counts, seed: int = 0, sequence: int = 0, hist=None):
         """Time every candidate; returns (best config dict, {label: ms})."""
         from .batched import BatchPlan, make_config
 
@@ -110,10 +114,22 @@ class Autotuner:
             except RuntimeError:
                 continue  # geometry not supported for this shape (shared memory)
             events, rows, ws = plan.new_events(), plan.new_row_offsets(), plan.new_workspace()
+            if hist is not None:
+                bins, lo, hi = int(hist[0]), float(hist[1]), float(hist[2])
+                hbuf = torch.empty((plan.n_densities, bins), dtype=torch.float32,
+                                   device=self.device)
+                kept = torch.empty(plan.n_densities, dtype=torch.int64, device=self.device)
+                ghist = torch.randn((plan.n_densities, bins), generator=gen, device=self.device)
 
-            def step():
-                plan.forward(grid, values, x_cut, seed, sequence, events, rows, ws)
-                plan.backward(grid, values, x_cut, seed, sequence, cot, grad_values, ws)
+                def step():
+                    plan.forward_hist(grid, values, x_cut, seed, sequence, bins, lo, hi, hbuf,
+                                      kept, ws)
+                    plan.backward_hist(grid, values, x_cut, seed, sequence, bins, lo, hi, ghist,
+                                       grad_values, ws)
+            else:
+                def step():
+                    plan.forward(grid, values, x_cut, seed, sequence, events, rows, ws)
+                    plan.backward(grid, values, x_cut, seed, sequence, cot, grad_values, ws)
 
             step()
             torch.cuda.synchronize(self.device)
