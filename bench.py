@@ -782,6 +782,7 @@ def run_gan_b200(args, rank, world, dist) -> dict:
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
     tr = BatchedGANTrainer(dev, seed=rank)
+    tr.capture()  # the whole step as one CUDA graph
     stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
         tr.step()
@@ -843,7 +844,8 @@ def run_gan_b200(args, rank, world, dist) -> dict:
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": {**describe_gan(tr), "events_per_step": ev_step,
-                   "parallelism": f"replicas x{world}", "launch": None},
+                   "parallelism": f"replicas x{world}", "form": "whole step in one CUDA graph",
+                   "launch": None},
         "gan": {"steps_per_s": 1e3 / ms, "sampler_ms_per_step": s_ms,
                 "sampler_share": s_ms / ms, "d_loss": float(d_loss), "g_loss": float(g_loss)},
         "e2e": {"value": ev_step * world / (e_ms * 1e-3), "unit": "events/s", "ms_per_step": e_ms,

@@ -222,11 +222,14 @@ int loits_batch_quantile(const loits_batch_plan* plan, const void* workspace, in
  * bins centred at lo + (k + 1/2) h; weight outside the bins is dropped).  hist
  * is B x bins fp32 and kept B int64 (kept events per density), both written
  * (zeroed first) by the call; the sampled events are those of
- * loits_batch_forward with the same seed and sequence.  1 <= bins <= 1024. */
+ * loits_batch_forward with the same seed and sequence.  1 <= bins <= 1024.
+ * sequence_dev (may be NULL): device address of the sequence, read by the
+ * kernels instead of `sequence` -- a CUDA graph replaying the call can then
+ * advance it between replays. */
 int loits_batch_forward_hist(const loits_batch_plan* plan, const float* grid, const float* values,
                              const float* x_cut, uint64_t seed, uint64_t sequence, int32_t bins,
                              float lo, float hi, float* hist, int64_t* kept, void* workspace,
-                             void* stream);
+                             const uint64_t* sequence_dev, void* stream);
 
 /* VJP of loits_batch_forward_hist: grad_hist (B x bins) -> grad_values; each
  * kept event's cotangent is (grad_hist[k + 1] - grad_hist[k]) / h.  Needs the
@@ -234,7 +237,7 @@ int loits_batch_forward_hist(const loits_batch_plan* plan, const float* grid, co
 int loits_batch_backward_hist(const loits_batch_plan* plan, const float* grid, const float* values,
                               const float* x_cut, uint64_t seed, uint64_t sequence, int32_t bins,
                               float lo, float hi, const float* grad_hist, float* grad_values,
-                              void* workspace, void* stream);
+                              void* workspace, const uint64_t* sequence_dev, void* stream);
 
 /* Two-component power-law theory of the batched GAN step (replaces, for
  * batched densities, the theory map of pytorch/theory.py:37-126): params is

@@ -81,9 +81,9 @@ SIGNATURES = {
     "loits_batch_cdf": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "loits_batch_quantile": (C.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "loits_batch_forward_hist": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _i32, C.c_float,
-                                           C.c_float, _vp, _vp, _vp, _vp]),
+                                           C.c_float, _vp, _vp, _vp, _vp, _vp]),
     "loits_batch_backward_hist": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _i32, C.c_float,
-                                            C.c_float, _vp, _vp, _vp, _vp]),
+                                            C.c_float, _vp, _vp, _vp, _vp, _vp]),
     "loits_theory_powerlaw": (C.c_int, [_i64, _i64, _vp, _vp, _vp, _vp]),
     "loits_theory_powerlaw_vjp": (C.c_int, [_i64, _i64, _vp, _vp, _vp, _vp, _vp]),
 }

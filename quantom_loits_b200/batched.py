@@ -161,20 +161,25 @@ class BatchPlan:
     def forward_hist(self, grid, values, x_cut, seed, sequence, bins, lo, hi, hist, kept,
                      workspace) -> None:
         """Histogram mode: bin the kept events (triangular weights, see
-        include/loits_b200.h) into hist (B x bins fp32); kept (B int64)."""
+        include/loits_b200.h) into hist (B x bins fp32); kept (B int64).
+        sequence: an int, or a one-element int64 device tensor read by the
+        kernels (so that a captured CUDA graph can advance it)."""
+        seq, seq_dev = _sequence_args(sequence)
         with torch.cuda.device(self.device):
             N.check(self._lib.loits_batch_forward_hist(
-                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed),
-                int(sequence), int(bins), float(lo), float(hi), hist.data_ptr(), kept.data_ptr(),
-                workspace.data_ptr(), N.stream_of(self.device)), "loits_batch_forward_hist")
+                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed), seq,
+                int(bins), float(lo), float(hi), hist.data_ptr(), kept.data_ptr(),
+                workspace.data_ptr(), seq_dev, N.stream_of(self.device)),
+                "loits_batch_forward_hist")
 
     def backward_hist(self, grid, values, x_cut, seed, sequence, bins, lo, hi, grad_hist,
                       grad_values, workspace) -> None:
+        seq, seq_dev = _sequence_args(sequence)
         with torch.cuda.device(self.device):
             N.check(self._lib.loits_batch_backward_hist(
-                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed),
-                int(sequence), int(bins), float(lo), float(hi), grad_hist.data_ptr(),
-                grad_values.data_ptr(), workspace.data_ptr(), N.stream_of(self.device)),
+                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed), seq,
+                int(bins), float(lo), float(hi), grad_hist.data_ptr(), grad_values.data_ptr(),
+                workspace.data_ptr(), seq_dev, N.stream_of(self.device)),
                 "loits_batch_backward_hist")
 
     def check_status(self, workspace) -> None:
@@ -202,6 +207,15 @@ class BatchPlan:
                                                    j.data_ptr(), N.stream_of(self.device)),
                     "loits_batch_quantile")
         return x, j
+
+
+def _sequence_args(sequence):
+    """(host sequence, device address or None) of an int or a device tensor."""
+    if isinstance(sequence, torch.Tensor):
+        if sequence.dtype != torch.int64 or sequence.numel() != 1 or not sequence.is_cuda:
+            raise ValueError("a device sequence is a one-element int64 CUDA tensor")
+        return 0, sequence.data_ptr()
+    return int(sequence), None
 
 
 def _aligned(t: torch.Tensor) -> torch.Tensor:
@@ -248,7 +262,7 @@ class _HistFunction(torch.autograd.Function):
         kept = torch.empty(plan.n_densities, dtype=torch.int64, device=values.device)
         ws = plan.new_workspace()
         plan.forward_hist(grid, values, x_cut, seed, sequence, bins, lo, hi, hist, kept, ws)
-        ctx.plan, ctx.seed, ctx.sequence = plan, int(seed), int(sequence)
+        ctx.plan, ctx.seed, ctx.sequence = plan, int(seed), sequence
         ctx.bins, ctx.lo, ctx.hi, ctx.x_cut = int(bins), float(lo), float(hi), x_cut
         ctx.save_for_backward(values, grid, ws)
         ctx.mark_non_differentiable(kept)
@@ -278,12 +292,17 @@ class BatchedLOITS:
     ``loits_batch_config`` / dict, or ``"auto"``: the launch geometry is timed
     on the first batch of each shape bucket (:mod:`quantom_loits_b200.tuning`)."""
 
-    def __init__(self, device="cuda", seed=None, config=None):
+    def __init__(self, device="cuda", seed=None, config=None, device_sequence=False):
         self.device = torch.device(device)
         N.require_device(self.device)
         self.seed = torch.initial_seed() if seed is None else int(seed)
         self.config = config
         self.sequence = 0
+        # histogram calls may keep the sequence counter on the device: each
+        # call takes a device snapshot and advances the counter there, so a
+        # captured CUDA graph draws fresh uniforms on every replay
+        self.sequence_dev = (torch.zeros(1, dtype=torch.int64, device=self.device)
+                             if device_sequence else None)
         self._plans: dict = {}
 
     def plan_for(self, knot_offsets, event_counts, batch=None, hist=None) -> BatchPlan:
@@ -333,8 +352,12 @@ class BatchedLOITS:
             else:
                 counts = _host_i64(n_events)
         if sequence is None:
-            sequence = self.sequence
-            self.sequence += 1
+            if self.sequence_dev is not None:
+                sequence = self.sequence_dev.clone()
+                self.sequence_dev.add_(1)
+            else:
+                sequence = self.sequence
+                self.sequence += 1
         plan = self.plan_for(batch.knot_offsets, counts, batch, (bins, lo, hi))
         grid = batch.grid.detach().contiguous()
         x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()

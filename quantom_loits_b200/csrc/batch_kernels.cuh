@@ -62,6 +62,7 @@ struct BatchArgs {
   int64_t nmax;                // Philox slots per density (slot stride)
   int64_t dbase;               // global index of plan density 0
   uint64_t seed, stream_id;
+  const uint64_t* seq_dev;     // when set: the sequence, read on the device
   PhiloxKey rk;                // round keys of `seed`
   // inputs
   const float* grid;

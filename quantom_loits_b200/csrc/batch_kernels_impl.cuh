@@ -57,6 +57,12 @@ __device__ __forceinline__ int find_owner(const int32_t* __restrict__ table, int
   return lo;
 }
 
+// Philox stream of the launch: 2 * sequence, the sequence read from device
+// memory when the launch was given one (graph replays that advance it).
+__device__ __forceinline__ uint64_t stream_of(const BatchArgs& a) {
+  return a.seq_dev ? 2 * __ldg(a.seq_dev) : a.stream_id;
+}
+
 // ------------------------------------------------------------------ search
 
 // (u >= c_k) exactly, for fp32 u: a record's key is the smallest fp32 >= c_k.
@@ -715,7 +721,7 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
     int js[4] = {0, 0, 0, 0};
     uint32_t keep = 0;
     if (range) {
-      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
       const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
       const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
       keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
@@ -783,7 +789,7 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, const TileGe
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
     const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
     if (!range) continue;
-    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
     const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
     const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
     const int64_t row0 = (blk << 2) + shiftrow;
@@ -822,7 +828,7 @@ __device__ __forceinline__ void sample_tile_general(const BatchArgs& a, int32_t 
     float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
     uint32_t keep = 0;
     if (range) {
-      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
       const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
       const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
       keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
@@ -911,7 +917,7 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
     const uint32_t range = d.skip ? 0u : (full ? 0xfu : block_range_mask(tg, blk));
     if (!range) continue;
-    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
     const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
     const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
     const uint32_t keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
@@ -1010,7 +1016,7 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
         const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
         const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
         if (!range) continue;
-        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
         const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
         const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
         const uint32_t keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
@@ -1036,7 +1042,7 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
         const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
         const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
         if (!range) continue;
-        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
         const int64_t row0 = (blk << 2) + shiftrow;
         float4 g4;
         if (range == 0xfu && (row0 & 3) == 0) {
@@ -1071,7 +1077,7 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
       Slot e0, e1, e2, e3;
       uint32_t keep = 0;
       if (range) {
-        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), a.stream_id, a.rk);
+        const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
         e0 = sample_slot<kMode>(d, w.x);
         e1 = sample_slot<kMode>(d, w.y);
         e2 = sample_slot<kMode>(d, w.z);

@@ -63,6 +63,10 @@ struct loits_batch_plan {
                 *d_chunk_first = nullptr, *d_rowfill_lo = nullptr, *d_gbits = nullptr;
   Layout lay{};
   size_t fwd_smem = 0, bwd_smem = 0;
+  // dynamic shared memory already allowed for the kernels (histogram mode
+  // launches with more; raised once, so that later launches -- and CUDA
+  // graph captures -- make no attribute calls)
+  mutable size_t fwd_smem_allowed = 0, bwd_smem_allowed = 0;
   int fwd_grid = 1, bwd_grid = 1, num_sms = 148;
 };
 
@@ -439,6 +443,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->total_gc = gco;
   p->m_cap_b = sg.m_cap_b;
   p->fwd_smem = sg.fwd;
+  p->fwd_smem_allowed = sg.fwd;
+  p->bwd_smem_allowed = sg.bwd;
   p->bwd_smem = sg.bwd;
   int dev = 0;
   if (cudaGetDevice(&dev) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
@@ -595,8 +601,10 @@ int launch_forward(const loits_batch_plan* p, BatchArgs& a, void* workspace, siz
   FwdKernel fk;
   BwdKernel bk;
   kernels_for(p->tpb, p->r, p->has_large, fk, bk);
-  if (smem > p->fwd_smem && !allow_dynamic_smem(reinterpret_cast<const void*>(fk), smem))
-    return LOITS_ERR_CUDA;
+  if (smem > p->fwd_smem_allowed) {
+    if (!allow_dynamic_smem(reinterpret_cast<const void*>(fk), smem)) return LOITS_ERR_CUDA;
+    p->fwd_smem_allowed = smem;
+  }
   uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_fwd);
   if (!p->cfg.plain) {
     a.c_lo = 0; a.c_hi = p->n_cdf;
@@ -632,8 +640,10 @@ int launch_backward(const loits_batch_plan* p, BatchArgs& a, void* workspace, si
   FwdKernel fk;
   BwdKernel bk;
   kernels_for(p->tpb, p->r, p->has_large, fk, bk);
-  if (smem > p->bwd_smem && !allow_dynamic_smem(reinterpret_cast<const void*>(bk), smem))
-    return LOITS_ERR_CUDA;
+  if (smem > p->bwd_smem_allowed) {
+    if (!allow_dynamic_smem(reinterpret_cast<const void*>(bk), smem)) return LOITS_ERR_CUDA;
+    p->bwd_smem_allowed = smem;
+  }
   uint32_t* tickets = carve<uint32_t>(workspace, L.tickets_bwd);
   if (!p->cfg.plain) {
     a.k_lo = 0; a.k_hi = p->n_chunks;
@@ -711,7 +721,7 @@ extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* 
                                         const float* values, const float* x_cut, uint64_t seed,
                                         uint64_t sequence, int32_t bins, float lo, float hi,
                                         float* hist, int64_t* kept, void* workspace,
-                                        void* stream) {
+                                        const uint64_t* sequence_dev, void* stream) {
   if (!p || !grid || !values || !hist || !kept || !workspace) return LOITS_ERR_INVALID;
   if (!hist_range_ok(bins, lo, hi) || !aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
@@ -720,6 +730,7 @@ extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* 
       cudaMemsetAsync(kept, 0, static_cast<size_t>(p->nd) * sizeof(int64_t), st) != cudaSuccess)
     return LOITS_ERR_CUDA;
   BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.seq_dev = sequence_dev;
   a.hist = hist;
   a.kept = reinterpret_cast<unsigned long long*>(kept);
   a.hist_bins = bins;
@@ -738,11 +749,13 @@ extern "C" int loits_batch_backward_hist(const loits_batch_plan* p, const float*
                                          const float* values, const float* x_cut, uint64_t seed,
                                          uint64_t sequence, int32_t bins, float lo, float hi,
                                          const float* grad_hist, float* grad_values,
-                                         void* workspace, void* stream) {
+                                         void* workspace, const uint64_t* sequence_dev,
+                                         void* stream) {
   if (!p || !grid || !values || !grad_hist || !grad_values || !workspace) return LOITS_ERR_INVALID;
   if (!hist_range_ok(bins, lo, hi) || !aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
   BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.seq_dev = sequence_dev;
   a.grad_hist = grad_hist;
   a.grad_values = grad_values;
   a.hist_bins = bins;

@@ -113,16 +113,21 @@ class BatchedGANTrainer:
         self.theory = PowerLawTheory(grid1).to(self.device)
         self.generator = Generator(latent).to(self.device)
         self.discriminator = Discriminator(bins).to(self.device)
-        self.sampler = BatchedLOITS(self.device, seed=int(seed), config=config)
+        self.sampler = BatchedLOITS(self.device, seed=int(seed), config=config,
+                                    device_sequence=True)
         self.lo, self.hi = 1e-3, 1.0
         # the batch's knots: every density on the same grid
         self.grid = self.theory.grid.repeat(batch)
         self.knot_offsets = np.arange(batch + 1, dtype=np.int64) * grid_size
         self.event_counts = np.full(batch, self.n_events, dtype=np.int64)
         self.loss = nn.BCEWithLogitsLoss()
-        # one fused multi-tensor kernel per optimizer step instead of one per tensor
-        self.d_optimizer = torch.optim.Adam(self.discriminator.parameters(), lr=lr, fused=True)
-        self.g_optimizer = torch.optim.Adam(self.generator.parameters(), lr=lr, fused=True)
+        # one fused multi-tensor kernel per optimizer step instead of one per
+        # tensor; step counts on the device so that the step can be captured
+        self.d_optimizer = torch.optim.Adam(self.discriminator.parameters(), lr=lr, fused=True,
+                                            capturable=True)
+        self.g_optimizer = torch.optim.Adam(self.generator.parameters(), lr=lr, fused=True,
+                                            capturable=True)
+        self.graph = None
         self.gen = torch.Generator(device=self.device).manual_seed(int(seed) + 1)
         # target theory: fixed raw parameters, the same for every density
         target = torch.tensor([[0.4, -0.3, -1.2, 0.8, 0.5, -0.2]], dtype=torch.float32,
@@ -145,9 +150,7 @@ class BatchedGANTrainer:
     def generate(self, z: torch.Tensor) -> torch.Tensor:
         return self.histogram(self.theory(self.generator(z)))
 
-    def step(self, z_d: torch.Tensor | None = None, z_g: torch.Tensor | None = None):
-        z_d = self.latent_noise() if z_d is None else z_d
-        z_g = self.latent_noise() if z_g is None else z_g
+    def _step_body(self, z_d: torch.Tensor, z_g: torch.Tensor):
         with self._region("gan::discriminator_step"):
             self.d_optimizer.zero_grad(set_to_none=True)
             with torch.no_grad():
@@ -159,9 +162,54 @@ class BatchedGANTrainer:
             d_loss.backward()
             self.d_optimizer.step()
         with self._region("gan::generator_step"):
-            self.g_optimizer.zero_grad(set_to_none=True)
+            # gradients of the generator only (pytorch/gan.py:117-121)
             logits = self.discriminator(self.generate(z_g))
             g_loss = self.loss(logits, torch.ones_like(logits))
-            g_loss.backward()
+            params = list(self.generator.parameters())
+            for p, g in zip(params, torch.autograd.grad(g_loss, params)):
+                p.grad = g
             self.g_optimizer.step()
         return d_loss.detach(), g_loss.detach()
+
+    def step(self, z_d: torch.Tensor | None = None, z_g: torch.Tensor | None = None):
+        """One discriminator step and one generator step; (d_loss, g_loss)."""
+        if self.graph is not None:
+            return self.replay(z_d, z_g)
+        z_d = self.latent_noise() if z_d is None else z_d
+        z_g = self.latent_noise() if z_g is None else z_g
+        return self._step_body(z_d, z_g)
+
+    def capture(self, warmup: int = 3):
+        """Capture the whole training step (both networks' forward and
+        backward, the theory, the sampler's histogram forwards and VJP, both
+        optimizer steps) as one CUDA graph; later steps replay it.  The
+        sampler reads its sequence from device memory, so every replay draws
+        fresh events; latents are inputs filled before each replay."""
+        self.static_zd = self.latent_noise()
+        self.static_zg = self.latent_noise()
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            for _ in range(warmup):
+                self._step_body(self.static_zd, self.static_zg)
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            self.static_losses = self._step_body(self.static_zd, self.static_zg)
+        self.graph = graph
+        return graph
+
+    def replay(self, z_d: torch.Tensor | None = None, z_g: torch.Tensor | None = None):
+        if z_d is None:
+            torch.randn(self.static_zd.shape, generator=self.gen, device=self.device,
+                        out=self.static_zd)
+        else:
+            self.static_zd.copy_(z_d, non_blocking=True)
+        if z_g is None:
+            torch.randn(self.static_zg.shape, generator=self.gen, device=self.device,
+                        out=self.static_zg)
+        else:
+            self.static_zg.copy_(z_g, non_blocking=True)
+        self.graph.replay()
+        return self.static_losses

@@ -166,3 +166,26 @@ def test_gan_trainer_steps():
     assert any(not torch.equal(a, b) for a, b in zip(g0, tr.generator.parameters()))
     assert any(not torch.equal(a, b) for a, b in zip(d0, tr.discriminator.parameters()))
     assert tr.real_hist.shape == (8, 64)
+
+
+def test_gan_step_captured_in_one_graph():
+    """The captured step replays with finite losses, advances the sampler's
+    device-side sequence by two histogram calls per step, and later calls
+    draw fresh uniforms."""
+    from quantom_loits_b200.gan import BatchedGANTrainer
+
+    tr = BatchedGANTrainer(DEV, batch=8, n_events=20_000, grid_size=512, seed=5)
+    tr.capture()
+    seq0 = int(tr.sampler.sequence_dev.item())
+    zs = [torch.randn((2, 8, 64), device=DEV) for _ in range(3)]
+    out = [tr.replay(z[0], z[1]) for z in zs]
+    torch.cuda.synchronize()
+    # two histogram calls per step advance the device sequence
+    assert int(tr.sampler.sequence_dev.item()) == seq0 + 2 * len(zs)
+    losses = [(float(d), float(g)) for d, g in out]
+    assert all(np.isfinite(v).all() for v in losses)
+    # fresh uniforms each replay: the same latents give different fake histograms
+    with torch.no_grad():
+        h1 = tr.generate(zs[0][0])
+        h2 = tr.generate(zs[0][0])
+    assert not torch.equal(h1, h2)
