@@ -123,5 +123,6 @@ constexpr int kHistSmemBytes = 16 * 1024;
 constexpr uint32_t kNonMonotone = 1u;  // an area is negative/NaN: count semantics
 constexpr uint32_t kBadGrid = 2u;      // grid not ascending or not finite
 constexpr uint32_t kAcceptAll = 4u;    // every event provably kept (see accept_all_flag)
+constexpr uint32_t kThreshold = 8u;    // kept events = uniforms above one threshold (threshold_flag)
 
 }  // namespace loits_dev

@@ -205,6 +205,22 @@ __device__ __forceinline__ uint32_t accept_all_flag(const BatchArgs& a, int b, i
   return kAcceptAll;
 }
 
+// kThreshold when the kept events of density b are exactly those whose
+// uniform lies above one threshold: with a non-decreasing CDF and an
+// ascending finite grid (finite slopes m_j >= 0), the fp32 value
+// x(u) = g_j + m_j ((u - key_j) + d_j) is non-decreasing in u -- each step is
+// a correctly rounded monotone operation, and across a knot the next
+// interval starts at or above where the previous one ends -- so for a cut
+// >= 0 (x > cut >= 0 is non-zero and finite) {u : x(u) > cut} = {u > u*}.
+__device__ __forceinline__ uint32_t threshold_flag(const BatchArgs& a, int b, int64_t k0,
+                                                   int64_t G, double norm, uint32_t flags) {
+  if (flags & (kNonMonotone | kBadGrid | kAcceptAll)) return 0u;
+  if (!(norm > 0.0) || !isfinite(norm)) return 0u;
+  if (!(__ldg(&a.grid[k0 + G - 1]) < 1e30f) || !(__ldg(&a.grid[k0]) > -1e30f)) return 0u;
+  if (!a.x_cut || !(__ldg(&a.x_cut[b]) >= 0.0f)) return 0u;
+  return kThreshold;
+}
+
 // Pack small density b's guide for sampling from shared memory: gpk[k] =
 // L[k] | L[k+1] << 16 (counts of a small density fit 16 bits).  Every L entry
 // was written (and fenced) before this runs.  Large densities are sampled
@@ -341,8 +357,9 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
     __syncthreads();
     if (threadIdx.x == 0) {
       a.norm[b] = tile_tot;
-      const uint32_t fl = (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u);
-      a.dflags[b] = fl | accept_all_flag(a, b, k0, G, tile_tot, fl);
+      uint32_t fl = (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u);
+      fl |= accept_all_flag(a, b, k0, G, tile_tot, fl);
+      a.dflags[b] = fl | threshold_flag(a, b, k0, G, tile_tot, fl);
       __threadfence();
       atomicAdd(&a.cdf_ready[b], 1u);
     }
@@ -445,8 +462,9 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
     if (!nonmono) pack_guide<TPB>(a, b);
     __syncthreads();
     if (threadIdx.x == 0) {
-      const uint32_t fl = ld_acquire_u32(&a.dflags[b]) & (kNonMonotone | kBadGrid);
-      a.dflags[b] = fl | accept_all_flag(a, b, k0, G, norm, fl);
+      uint32_t fl = ld_acquire_u32(&a.dflags[b]) & (kNonMonotone | kBadGrid);
+      fl |= accept_all_flag(a, b, k0, G, norm, fl);
+      a.dflags[b] = fl | threshold_flag(a, b, k0, G, norm, fl);
       __threadfence();
       atomicAdd(&a.cdf_ready[b], 1u);
     }
@@ -515,6 +533,7 @@ struct DensView {
   int G;
   bool count_all;
   bool accept_all;
+  bool threshold;         // kept = uniforms above one threshold (kThreshold)
   bool skip;              // large density whose CDF is not non-decreasing: not sampled
   float cut;
 };
@@ -581,6 +600,7 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
   v.G = static_cast<int>(G);
   v.count_all = nonmono && !large;
   v.accept_all = (sh.flags & kAcceptAll) != 0;
+  v.threshold = (sh.flags & kThreshold) != 0;
   v.skip = nonmono && large;
   v.cut = sh.cut;
   return v;
@@ -772,6 +792,104 @@ __device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, c
   return base;
 }
 
+// The threshold of a kThreshold density: the largest k in [-1, 2^24) with
+// x(k 2^-24) <= cut, found by one warp with a 33-ary search that evaluates
+// the sampler's own arithmetic (sample_slot) -- so slot p is kept exactly
+// when (word >> 8) > k, in the forward and in the backward alike.
+template <int kMode>
+__device__ __forceinline__ int kept_threshold(const DensView& d) {
+  const int lane = threadIdx.x & 31;
+  int lo = -1, hi = 1 << 24;  // x(lo) <= cut (lo = -1: none), x(hi) > cut (hi = 2^24: all)
+  while (hi - lo > 1) {
+    const int64_t span = hi - lo;
+    const int p = lo + static_cast<int>(span * (lane + 1) / 33);
+    bool le = true;
+    if (p > lo && p < hi) le = !(sample_slot<kMode>(d, static_cast<uint32_t>(p) << 8).x > d.cut);
+    const int lo2 = __reduce_max_sync(0xffffffffu, le ? p : lo);
+    int hi2 = __reduce_min_sync(0xffffffffu, le ? hi : p);
+    if (hi2 <= lo2) hi2 = lo2 + 1;  // only if x were not monotone: still ends
+    lo = lo2;
+    hi = hi2;
+  }
+  return lo;
+}
+
+__device__ __forceinline__ uint32_t threshold_keep(uint4 w, int kstar) {
+  return (static_cast<int>(w.x >> 8) > kstar ? 1u : 0u) |
+         (static_cast<int>(w.y >> 8) > kstar ? 2u : 0u) |
+         (static_cast<int>(w.z >> 8) > kstar ? 4u : 0u) |
+         (static_cast<int>(w.w >> 8) > kstar ? 8u : 0u);
+}
+
+// Tile of a kThreshold density: each warp counts its kept slots from the
+// Philox words alone, the tile publishes its count and takes its first row
+// from the look-back, then every warp samples and stores its kept events
+// straight to their final rows (no staging).
+template <int TPB, int R, int kMode>
+__device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_t t,
+                                                      const TileGeom& tg, const DensView& d,
+                                                      SampleShared& sh) {
+  constexpr int W = TPB / 32;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int kstar = kept_threshold<kMode>(d);
+  const bool full = tile_full<TPB, R>(tg);
+  int cnt = 0;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
+    if (!range) continue;
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
+    cnt += __popc(threshold_keep(w, kstar) & range);
+  }
+  cnt = warp_sum(cnt);
+  if (lane == 0) sh.warp_cnt[warp] = cnt;
+  __syncthreads();
+  int tile_cnt = 0, warp_excl = 0;
+#pragma unroll
+  for (int w = 0; w < W; ++w) {
+    const int c = sh.warp_cnt[w];
+    warp_excl += w < warp ? c : 0;
+    tile_cnt += c;
+  }
+  if (lane == 0) a.warp_off[static_cast<int64_t>(t) * W + warp] = warp_excl;
+  if (warp == 0) {
+    const int64_t base = publish_tile(a, t, tg, tile_cnt);
+    if (lane == 0) sh.base = base;
+  }
+  __syncthreads();
+  int64_t row = sh.base + warp_excl;
+#pragma unroll 1
+  for (int r = 0; r < R; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
+    uint32_t keep = 0;
+    Slot e0, e1, e2, e3;
+    if (range) {
+      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
+      keep = threshold_keep(w, kstar) & range;
+      e0 = sample_slot<kMode>(d, w.x);
+      e1 = sample_slot<kMode>(d, w.y);
+      e2 = sample_slot<kMode>(d, w.z);
+      e3 = sample_slot<kMode>(d, w.w);
+    }
+    int total;
+    int64_t pos = row + warp_exclusive_count(__popc(keep), total);
+    if (a.intervals) {
+      int64_t q = pos;
+      if (keep & 1u) a.intervals[q++] = e0.j;
+      if (keep & 2u) a.intervals[q++] = e1.j;
+      if (keep & 4u) a.intervals[q++] = e2.j;
+      if (keep & 8u) a.intervals[q] = e3.j;
+    }
+    if (keep & 1u) __stcs(&a.events[pos++], e0.x);
+    if (keep & 2u) __stcs(&a.events[pos++], e1.x);
+    if (keep & 4u) __stcs(&a.events[pos++], e2.x);
+    if (keep & 8u) __stcs(&a.events[pos], e3.x);
+    row += total;
+  }
+}
+
 // Tile of a density whose every event is kept (kAcceptAll): the tile's count
 // is its number of slots, published (by the caller, before any event is
 // computed) with first row `base`, and slot p lands in row p + (base - s_lo)
@@ -911,6 +1029,7 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   __syncthreads();
   float* mine = hs + (lane & (rep - 1)) * stride;
   const bool full = tile_full<TPB, R>(tg);
+  const int kstar = d.threshold ? kept_threshold<kMode>(d) : 0;
   int kept = 0;
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
@@ -920,7 +1039,9 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
     const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
     const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
     const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
-    const uint32_t keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+    const uint32_t keep = (d.threshold ? threshold_keep(w, kstar)
+                                       : (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3))) &
+                          range;
     if (keep & 1u) hist_add(a, mine, e0.x);
     if (keep & 2u) hist_add(a, mine, e1.x);
     if (keep & 4u) hist_add(a, mine, e2.x);
@@ -965,9 +1086,11 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
   const DensView d = density_view(a, tg.b, tg.k0, tg.G, large, rec_s, guide_s, nullptr, sh);
   if (large) {
     if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, tg, d, sh.base);
+    else if (d.threshold) sample_tile_threshold<TPB, R, kL2>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kL2>(a, t, tg, d, stage, sh);
   } else {
     if (d.accept_all) sample_tile_all<TPB, R, kShared>(a, tg, d, sh.base);
+    else if (d.threshold) sample_tile_threshold<TPB, R, kShared>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kShared>(a, t, tg, d, stage, sh);
   }
 }
@@ -1005,6 +1128,8 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (d.skip) return;
+  // kThreshold densities keep exactly the slots the forward kept by threshold
+  const int kstar = d.threshold ? kept_threshold<kMode>(d) : 0;
   if (gh) {
     // histogram mode: every kept slot's cotangent comes from the histogram's
 #pragma unroll 1
@@ -1019,7 +1144,9 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
         const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
         const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
         const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
-        const uint32_t keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+        const uint32_t keep = (d.threshold ? threshold_keep(w, kstar)
+                                           : (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3))) &
+                              range;
         if (keep & 1u) scatter_slot<kMode>(e0, hist_cotangent(a, gh, e0.x), d, gacc_s, gc);
         if (keep & 2u) scatter_slot<kMode>(e1, hist_cotangent(a, gh, e1.x), d, gacc_s, gc);
         if (keep & 4u) scatter_slot<kMode>(e2, hist_cotangent(a, gh, e2.x), d, gacc_s, gc);
@@ -1082,7 +1209,9 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
         e1 = sample_slot<kMode>(d, w.y);
         e2 = sample_slot<kMode>(d, w.z);
         e3 = sample_slot<kMode>(d, w.w);
-        keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
+        keep = (d.threshold ? threshold_keep(w, kstar)
+                            : (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3))) &
+               range;
       }
       int total;
       int64_t my = row + warp_exclusive_count(__popc(keep), total);
