@@ -284,40 +284,55 @@ __device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_
   __syncthreads();
 }
 
-// Chained look-back over tiles [first, ct) of one density (thread 0 only):
-// publishes tile ct's aggregate, returns the fp64 sum of the earlier tiles
-// and publishes tile ct's inclusive sum.  flag: 1 aggregate, 2 inclusive.
+// Chained look-back over tiles [first, ct) of one density, by one whole
+// warp: publishes tile ct's aggregate, then reads 32 predecessors per step
+// until it meets an inclusive sum, and publishes tile ct's inclusive sum.
+// Returns the fp64 sum of the earlier tiles on every lane.  flag: 1
+// aggregate, 2 inclusive.  Every poll is bounded.
 __device__ __forceinline__ double chained_lookback(uint32_t* flag, double* agg_arr, double* inc_arr,
                                                    int32_t* status, int32_t first, int32_t ct,
                                                    double agg) {
+  const int lane = threadIdx.x & 31;
   double excl = 0.0;
   if (ct > first) {
-    __stcg(&agg_arr[ct], agg);
-    __threadfence();
-    atomicExch(&flag[ct], 1u);
-    int32_t i = ct - 1;
+    if (lane == 0) {
+      __stcg(&agg_arr[ct], agg);
+      __threadfence();
+      atomicExch(&flag[ct], 1u);
+    }
+    __syncwarp();
+    int32_t base = ct - 1;
     uint32_t polls = 0;
-    while (i >= first) {
-      const uint32_t fl = ld_acquire_u32(&flag[i]);
-      if (fl == 0) {
-        if (++polls >= kSpinLimit || ((polls & 63u) == 0u && launch_timed_out(status))) {
-          raise_status(status, LOITS_ERR_TIMEOUT);
+    while (base >= first) {
+      const int32_t i = base - lane;
+      // tiles before `first` do not exist: an inclusive zero
+      const uint32_t fl = i >= first ? ld_acquire_u32(&flag[i]) : 2u;
+      if (__any_sync(0xffffffffu, fl == 0)) {
+        if (++polls >= kSpinLimit ||
+            ((polls & 63u) == 0u && __any_sync(0xffffffffu, launch_timed_out(status)))) {
+          if (lane == 0) raise_status(status, LOITS_ERR_TIMEOUT);
           break;
         }
         spin_pause(polls);
         continue;
       }
-      if (fl == 2) {
-        excl += __ldcg(&inc_arr[i]);
-        break;
-      }
-      excl += __ldcg(&agg_arr[i]);
-      --i;
+      const unsigned inc = __ballot_sync(0xffffffffu, fl == 2);
+      const int stop = inc ? __ffs(inc) - 1 : 32;  // nearest inclusive predecessor
+      double v = 0.0;
+      if (i >= first && lane < stop) v = __ldcg(&agg_arr[i]);
+      else if (i >= first && lane == stop) v = __ldcg(&inc_arr[i]);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      excl += v;
+      if (inc) break;
+      base -= 32;
     }
   }
-  __stcg(&inc_arr[ct], excl + agg);
-  __threadfence();
-  atomicExch(&flag[ct], 2u);
+  if (lane == 0) {
+    __stcg(&inc_arr[ct], excl + agg);
+    __threadfence();
+    atomicExch(&flag[ct], 2u);
+  }
   return excl;
 }
 
@@ -370,7 +385,10 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   if (threadIdx.x == 0) {
     if (any_neg || any_bad)
       atomicOr(&a.dflags[b], (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u));
-    sh.tile_excl = cdf_lookback(a, first, ct, tile_tot);
+  }
+  if (threadIdx.x < 32) {
+    const double excl_t = cdf_lookback(a, first, ct, tile_tot);
+    if (threadIdx.x == 0) sh.tile_excl = excl_t;
   }
   __syncthreads();
   // largest unnormalised prefix of this tile, formed exactly as pass 2 forms
@@ -1418,7 +1436,10 @@ __device__ __forceinline__ void vjp_large_scan_item(const BatchArgs& a, int32_t 
   }
   double seg_tot;
   const double later = block_exclusive_suffix_sum<double, TPB>(tot, seg_tot, sh.dscan);
-  if (threadIdx.x == 0) sh.carry = chained_lookback(a.lflag, a.lagg, a.linc, a.status, first, li, seg_tot);
+  if (threadIdx.x < 32) {
+    const double carry_t = chained_lookback(a.lflag, a.lagg, a.linc, a.status, first, li, seg_tot);
+    if (threadIdx.x == 0) sh.carry = carry_t;
+  }
   __syncthreads();
   const double carry = sh.carry;  // sum of grad-CDF over every knot >= s1
 #pragma unroll

@@ -460,8 +460,10 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   const int64_t items_f = nc + nf + nt;
   p->fwd_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items_f, int64_t(occ_f) * p->num_sms)));
   const int64_t resident_b = int64_t(occ_b) * p->num_sms;
-  // backward chunks: ~2 per resident CTA
-  const int64_t target_chunks = std::max<int64_t>(1, 2 * resident_b);
+  // backward chunks: ~4 per resident CTA keeps the last wave short; plans
+  // with large densities (global atomics, no per-chunk shared histogram)
+  // measured faster with ~2
+  const int64_t target_chunks = std::max<int64_t>(1, (p->has_large ? 2 : 4) * resident_b);
   p->tiles_per_chunk = static_cast<int32_t>(std::max<int64_t>(1, nt / target_chunks));
   p->chunk_first.resize(n_densities + 1);
   p->part_off.resize(n_densities);
