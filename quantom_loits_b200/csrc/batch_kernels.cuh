@@ -57,6 +57,7 @@ struct BatchArgs {
   int32_t gcap;                // knots a sampling CTA holds in shared memory
   int32_t mcap;                // guide entries (M + 1) a sampling CTA holds
   int32_t gbits_cap;           // most guide bits this launch copies to shared memory
+  int32_t lguide_bits;         // large densities: bits of the coarse guide in shared memory
                                // (a larger guide is read every 2^s-th count)
   int32_t tiles_per_chunk;
   int64_t nmax;                // Philox slots per density (slot stride)

@@ -535,17 +535,11 @@ __device__ __forceinline__ float key_at(const float4* rec, int i) {
   else return *p;
 }
 
-template <int kMode>
-__device__ __forceinline__ uint32_t guide_at(const uint32_t* g, uint32_t k) {
-  if constexpr (kMode == kL2) return __ldcg(g + k);
-  else if constexpr (kMode == kRO) return __ldg(g + k);
-  else return g[k];
-}
-
 // A density's sampling state.
 struct DensView {
   const float4* rec;      // records (shared or global)
-  const uint32_t* guide;  // shared: packed (L[k], L[k+1]); global: L itself
+  const uint32_t* guide;  // small: packed (L[k], L[k+1]) in shared memory; large: L, global
+  const uint32_t* cguide; // large, coarse: every 2^s-th count of L in shared memory
   const float* invd;      // backward weights (shared or global)
   int shift;              // 32 - m: bucket of a Philox word = word >> shift
   int G;
@@ -553,6 +547,7 @@ struct DensView {
   bool accept_all;
   bool threshold;         // kept = uniforms above one threshold (kThreshold)
   bool skip;              // large density whose CDF is not non-decreasing: not sampled
+  bool coarse;            // large: search from cguide (shift covers its bits)
   float cut;
 };
 
@@ -580,19 +575,33 @@ __device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool la
 }
 
 // The density's sampling view: small densities copy their records, packed
-// guide and (backward) weights into shared memory; large densities stay in
-// global memory.  Ends with a barrier.
+// guide and (backward) weights into shared memory; large densities keep
+// records and weights in global memory and read their guide in place
+// (forward: lguide_bits == 0) or copy a coarse guide (backward).  Ends with
+// a barrier.  guide_key (shared) names the density whose coarse guide
+// guide_s holds, so a CTA's consecutive items on one large density copy it
+// once.
 __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int64_t k0, int64_t G,
                                                  bool large, float4* rec_s, uint32_t* guide_s,
-                                                 float* invd_s, const SampleShared& sh) {
+                                                 float* invd_s, const SampleShared& sh,
+                                                 int& guide_key) {
   const bool nonmono = (sh.flags & kNonMonotone) != 0;
   const int m_full = __ldg(&a.gbits[b]);
-  const int m = large ? m_full : min(m_full, a.gbits_cap);
+  const bool coarse = large && a.lguide_bits > 0;
+  const int m = large ? (coarse ? min(m_full, a.lguide_bits) : m_full) : min(m_full, a.gbits_cap);
   DensView v;
   if (large) {
     v.rec = a.rec + k0;
-    v.guide = a.gl + __ldg(&a.goff[b]);
     v.invd = a.invd + k0;
+    const uint32_t* L = a.gl + __ldg(&a.goff[b]);
+    if (coarse && !nonmono && guide_key != b) {
+      // every 2^s-th count of the guide (the guide with 2^s-times wider
+      // buckets), 2^m + 1 uint32
+      const int sft = m_full - m;
+      for (int k = threadIdx.x; k <= (1 << m); k += blockDim.x) guide_s[k] = __ldcg(&L[k << sft]);
+    }
+    v.guide = L;
+    v.cguide = guide_s;
   } else {
     for (int64_t i = threadIdx.x; i < G; i += blockDim.x) {
       rec_s[i] = __ldcg(&a.rec[k0 + i]);
@@ -611,25 +620,32 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
     }
     v.rec = rec_s;
     v.guide = guide_s;
+    v.cguide = guide_s;
     v.invd = invd_s;
   }
   __syncthreads();
+  // every thread has read guide_key above; the next read follows the item
+  // loop's barriers
+  if (threadIdx.x == 0) guide_key = large ? (nonmono || !coarse ? guide_key : b) : -1;
   v.shift = 32 - m;
   v.G = static_cast<int>(G);
   v.count_all = nonmono && !large;
   v.accept_all = (sh.flags & kAcceptAll) != 0;
   v.threshold = (sh.flags & kThreshold) != 0;
   v.skip = nonmono && large;
+  v.coarse = coarse;
   v.cut = sh.cut;
   return v;
 }
 
+// `large` is a constant at every call site, so that after inlining each
+// view's pointers are known to be shared (LDS) or global memory.
 __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
-                                                 float4* rec_s, uint32_t* guide_s, float* invd_s,
-                                                 bool wait_ready, SampleShared& sh) {
-  const bool large = G > a.gcap;
+                                                 bool large, float4* rec_s, uint32_t* guide_s,
+                                                 float* invd_s, bool wait_ready, SampleShared& sh,
+                                                 int& guide_key) {
   density_flags(a, b, large, wait_ready, sh);
-  return density_view(a, b, k0, G, large, rec_s, guide_s, invd_s, sh);
+  return density_view(a, b, k0, G, large, rec_s, guide_s, invd_s, sh, guide_key);
 }
 
 // One slot: uniform from its Philox word, interval, value, acceptance.
@@ -659,9 +675,17 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
       const uint32_t pk = d.guide[k];
       lo = static_cast<int>(pk & 0xffffu);
       hi = static_cast<int>(pk >> 16);
+    } else if constexpr (kMode == kL2) {
+      // the full guide in global memory (written earlier in this launch)
+      lo = static_cast<int>(__ldcg(d.guide + k));
+      hi = static_cast<int>(__ldcg(d.guide + k + 1));
+    } else if (d.coarse) {
+      // the coarse guide in shared memory
+      lo = static_cast<int>(d.cguide[k]);
+      hi = static_cast<int>(d.cguide[k + 1]);
     } else {
-      lo = static_cast<int>(guide_at<kMode>(d.guide, k));
-      hi = static_cast<int>(guide_at<kMode>(d.guide, k + 1));
+      lo = static_cast<int>(__ldg(d.guide + k));
+      hi = static_cast<int>(__ldg(d.guide + k + 1));
     }
     const int ja = max(min(lo - 1, d.G - 2), 0);
     const float4 ra = rec_at<kMode>(d.rec, ja);
@@ -1082,15 +1106,22 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
 // separately so that plans without them carry none of the global-memory path).
 template <int TPB, int R, bool kLarge>
 __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
-                                            uint32_t* guide_s, float* stage, SampleShared& sh) {
+                                            uint32_t* guide_s, float* stage, SampleShared& sh,
+                                            int& guide_key) {
   const TileGeom tg = tile_geom<TPB, R>(a, t);
   const bool large = kLarge && tg.G > a.gcap;
   density_flags(a, tg.b, large, true, sh);
   if (a.hist) {
     float* hs = reinterpret_cast<float*>(rec_s) + a.hist_smem_off;
-    const DensView d = density_view(a, tg.b, tg.k0, tg.G, large, rec_s, guide_s, nullptr, sh);
-    if (large) sample_tile_hist<TPB, R, kL2>(a, tg, d, hs);
-    else sample_tile_hist<TPB, R, kShared>(a, tg, d, hs);
+    if (large) {
+      const DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
+                                     guide_key);
+      sample_tile_hist<TPB, R, kL2>(a, tg, d, hs);
+    } else {
+      const DensView d = density_view(a, tg.b, tg.k0, tg.G, false, rec_s, guide_s, nullptr, sh,
+                                     guide_key);
+      sample_tile_hist<TPB, R, kShared>(a, tg, d, hs);
+    }
     return;
   }
   if ((sh.flags & kAcceptAll) && threadIdx.x < 32) {
@@ -1101,12 +1132,16 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
     const int64_t base = publish_tile(a, t, tg, static_cast<int>(s_hi - s_lo));
     if (threadIdx.x == 0) sh.base = base;
   }
-  const DensView d = density_view(a, tg.b, tg.k0, tg.G, large, rec_s, guide_s, nullptr, sh);
+  // one view per branch: each sees constant `large` (shared or global loads)
   if (large) {
+    const DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
+                                   guide_key);
     if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, tg, d, sh.base);
     else if (d.threshold) sample_tile_threshold<TPB, R, kL2>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kL2>(a, t, tg, d, stage, sh);
   } else {
+    const DensView d = density_view(a, tg.b, tg.k0, tg.G, false, rec_s, guide_s, nullptr, sh,
+                                   guide_key);
     if (d.accept_all) sample_tile_all<TPB, R, kShared>(a, tg, d, sh.base);
     else if (d.threshold) sample_tile_threshold<TPB, R, kShared>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kShared>(a, t, tg, d, stage, sh);
@@ -1246,7 +1281,7 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
 template <int TPB, int R, bool kLarge>
 __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
                                                uint32_t* guide_s, float* invd_s, float* gacc_s,
-                                               SampleShared& sh) {
+                                               SampleShared& sh, int& guide_key) {
   const int b = find_owner(a.chunk_first, a.d_lo, a.d_hi, k);
   const int32_t ki = k - __ldg(&a.chunk_first[b]);
   const int32_t tb = __ldg(&a.tile_first[b]);
@@ -1263,7 +1298,8 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
     for (int k = threadIdx.x; k < a.hist_bins; k += TPB) gh[k] = __ldg(&src[k]);
   }
   if (kLarge && tg.G > a.gcap) {
-    const DensView d = load_density(a, b, tg.k0, tg.G, nullptr, nullptr, nullptr, false, sh);
+    const DensView d = load_density(a, b, tg.k0, tg.G, true, nullptr, guide_s, nullptr, false,
+                                    sh, guide_key);
     vjp_chunk_tiles<TPB, R, kRO>(a, d, tg, tb, t_first, t_end, nullptr,
                                  a.gcdf + __ldg(&a.gc_off[b]), gh);
     // the density's grad-CDF atomics are performed before the chunk counts
@@ -1280,7 +1316,8 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   while (rep < 32 && 2 * rep * (G + 1) <= a.gcap) rep *= 2;
   const int stride = rep > 1 ? G + 1 : G;  // rep * stride <= gcap
   for (int i = threadIdx.x; i < rep * stride; i += TPB) gacc_s[i] = 0.0f;
-  const DensView d = load_density(a, b, tg.k0, tg.G, rec_s, guide_s, invd_s, false, sh);
+  const DensView d = load_density(a, b, tg.k0, tg.G, false, rec_s, guide_s, invd_s, false, sh,
+                                  guide_key);
   float* gacc_lane = gacc_s + ((threadIdx.x & 31) & (rep - 1)) * stride;
   vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_lane, nullptr, gh);
   __syncthreads();
@@ -1526,6 +1563,8 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
     SampleShared smp;
   } sh;
   __shared__ uint32_t s_item;
+  __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
+  if (threadIdx.x == 0) s_guide_key = -1;
   const int32_t nC = a.c_hi - a.c_lo, nF = a.f_hi - a.f_lo, nT = a.t_hi - a.t_lo;
   const uint32_t n_items = static_cast<uint32_t>(nC + nF + nT);
   while (true) {
@@ -1540,7 +1579,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
       cdf_finalize_item<TPB>(a, a.f_lo + static_cast<int32_t>(item) - nC, sh.cdf);
     } else {
       sample_item<TPB, R, kLarge>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s,
-                                  guide_s, stage, sh.smp);
+                                  guide_s, stage, sh.smp, s_guide_key);
     }
   }
 }
@@ -1557,6 +1596,8 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     SampleShared smp;
   } sh;
   __shared__ uint32_t s_item;
+  __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
+  if (threadIdx.x == 0) s_guide_key = -1;
   const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo, nL = a.l_hi - a.l_lo;
   const uint32_t n_items = static_cast<uint32_t>(nK + nD + 2 * nL);
   while (true) {
@@ -1567,7 +1608,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nK)) {
       vjp_chunk_item<TPB, R, kLarge>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s,
-                                     invd_s, gacc_s, sh.smp);
+                                     invd_s, gacc_s, sh.smp, s_guide_key);
     } else if (item < static_cast<uint32_t>(nK + nD)) {
       vjp_finalize_item<TPB>(a, a.d_lo + static_cast<int32_t>(item) - nK, grho, sh.fin);
     } else if constexpr (kLarge) {

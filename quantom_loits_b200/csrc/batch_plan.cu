@@ -50,6 +50,7 @@ struct loits_batch_plan {
   int tpb = 256, r = 4, scan_knots = 8;
   int32_t n_tiles = 0, n_cdf = 0, n_fin = 0, n_chunks = 0, last_nonempty = -1;
   int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1, n_lfin = 0, m_cap_b = 2;
+  int32_t lbits_f = 0, lbits_b = 0;  // coarse large-density guide bits in shared memory
   bool has_large = false;  // densities above the shared-memory limit
   int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
@@ -164,11 +165,26 @@ bool allow_dynamic_smem(const void* fn, size_t bytes) {
 struct SmemGeometry {
   int m_cap = 2;    // forward: log2 of the most guide buckets beside the records
   int m_cap_b = 2;  // backward: the same beside records, weights and gradients
+  int lbits_f = 0;  // large densities: log2 of the coarse guide a forward CTA holds
+  int lbits_b = 0;  // ... and a backward CTA
   int32_t mcap = 0;
   size_t static_smem = 0, fwd = 0, bwd = 0;
 };
 
-int smem_geometry(int tpb, int r, bool large, int32_t gcap, int64_t max_g, SmemGeometry& g) {
+// Shared memory of one SM, and what the driver reserves per resident CTA.
+constexpr size_t kSmemPerSM = 228 * 1024;
+constexpr size_t kSmemPerCtaReserved = 1024;
+
+// Guide bits of a density of g knots: M = 2^m buckets, 2g <= M, at most 2^cap.
+int guide_bits(int64_t g, int cap) {
+  int m = 2;
+  while ((int64_t(1) << m) < 2 * g && m < cap) ++m;
+  return m;
+}
+
+// large_g: knots of the largest density above the shared-memory limit (0: none).
+int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, SmemGeometry& g) {
+  const bool large = large_g > 0;
   FwdKernel fk;
   BwdKernel bk;
   if (!kernels_for(tpb, r, large, fk, bk)) return LOITS_ERR_INVALID;
@@ -201,8 +217,32 @@ int smem_geometry(int tpb, int r, bool large, int32_t gcap, int64_t max_g, SmemG
   const int32_t mcap_b = std::min<int32_t>(g.mcap, int32_t(1) << g.m_cap_b);
   // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
   // kept events are staged in global memory, not here
-  g.fwd = fwd_knots + static_cast<size_t>((g.mcap + 7) & ~7) * sizeof(uint32_t);
-  g.bwd = bwd_knots + static_cast<size_t>((mcap_b + 7) & ~7) * sizeof(uint32_t);
+  size_t guide_f = static_cast<size_t>((g.mcap + 7) & ~7) * sizeof(uint32_t);
+  size_t guide_b = static_cast<size_t>((mcap_b + 7) & ~7) * sizeof(uint32_t);
+  if (large) {
+    // backward CTAs of large densities (records in global memory) read a
+    // coarse copy of the guide (every 2^s-th count, 2^lbits + 1 uint32) from
+    // shared memory, sized not to lower the residency the register cap
+    // allows and to leave room for a histogram-mode cotangent (16 KB); the
+    // forward reads the full guide through L2 (lbits_f = 0), which measured
+    // faster than the coarser buckets' longer searches
+    auto bytes = [](int b) { return ((size_t(1) << b) + 1 + 7) / 8 * 8 * sizeof(uint32_t); };
+    size_t ctas = static_cast<size_t>(std::max(1, 1280 / tpb));
+    while (ctas > 1 && ctas * (bwd_knots + g.static_smem + bytes(6) + kSmemPerCtaReserved) > kSmemPerSM)
+      --ctas;
+    const size_t per_cta = kSmemPerSM / ctas - kSmemPerCtaReserved;
+    int lb = kMaxLargeGuideBits;
+    while (lb > 6 && (bwd_knots + bytes(lb) + g.static_smem > per_cta ||
+                      bwd_knots + bytes(lb) + g.static_smem + 16 * 1024 > kSmemLimit))
+      --lb;
+    g.lbits_f = 0;
+    // a copy more than 16 times coarser than the largest guide costs more
+    // search steps than it saves: the full guide is read in place instead
+    g.lbits_b = lb >= guide_bits(large_g, kMaxLargeGuideBits) - 4 ? lb : 0;
+    if (g.lbits_b > 0) guide_b = std::max(guide_b, bytes(lb));
+  }
+  g.fwd = fwd_knots + guide_f;
+  g.bwd = bwd_knots + guide_b;
   if (g.fwd + g.static_smem > kSmemLimit || g.bwd + g.static_smem > kSmemLimit)
     return LOITS_ERR_UNSUPPORTED;
   if (!allow_dynamic_smem(reinterpret_cast<const void*>(fk), g.fwd) ||
@@ -223,19 +263,19 @@ void occupancy(int tpb, int r, bool large, const SmemGeometry& g, int& occ_f, in
 
 // CTA size with the most resident threads per SM for both kernels (the
 // smaller CTA on a tie: fewer threads wait at each tile barrier).
-int choose_threads(int r_req, bool large, int32_t gcap, int64_t max_g, int& tpb_out) {
+int choose_threads(int r_req, int64_t large_g, int32_t gcap, int64_t max_g, int& tpb_out) {
   int best = -1, best_tpb = 0, last_rc = LOITS_ERR_UNSUPPORTED;
   for (int tpb : {256, 512, 1024}) {
     const int r = r_req ? r_req : default_blocks(tpb);
     if (tpb == 1024 && r == 16) continue;
     SmemGeometry g;
-    const int rc = smem_geometry(tpb, r, large, gcap, max_g, g);
+    const int rc = smem_geometry(tpb, r, large_g, gcap, max_g, g);
     if (rc != LOITS_OK) {
       last_rc = rc;
       continue;
     }
     int of = 0, ob = 0;
-    occupancy(tpb, r, large, g, of, ob);
+    occupancy(tpb, r, large_g > 0, g, of, ob);
     const int resident = tpb * std::min(of, ob);
     if (resident > best) {
       best = resident;
@@ -269,6 +309,7 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.lfin_first = p->d_lfin_first;
   a.mcap = p->mcap;
   a.gbits_cap = 30;  // forward: full guides (the backward lowers this)
+  a.lguide_bits = p->lbits_f;
   a.nd = static_cast<int32_t>(p->nd);
   a.last_nonempty = p->last_nonempty;
   a.tiles_total = p->n_tiles;
@@ -353,10 +394,11 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   // 16-byte aligned (every large density has more knots than this)
   p->gcap = static_cast<int32_t>((std::max<int64_t>(p->small_max_g, 4) + 3) & ~int64_t(3));
   p->has_large = p->max_g > p->gcap;
+  const int64_t large_g = p->has_large ? p->max_g : 0;
   // ---- launch geometry: the CTA size (by occupancy unless given)
   if (c.threads == 0) {
     int tpb = 0;
-    rc = choose_threads(c.blocks_per_item, p->has_large, p->gcap, p->small_max_g, tpb);
+    rc = choose_threads(c.blocks_per_item, large_g, p->gcap, p->small_max_g, tpb);
     if (rc != LOITS_OK) { delete p; return rc; }
     c.threads = tpb;
   }
@@ -365,7 +407,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->tpb = c.threads;
   p->r = c.blocks_per_item;
   SmemGeometry sg;
-  rc = smem_geometry(p->tpb, p->r, p->has_large, p->gcap, p->small_max_g, sg);
+  rc = smem_geometry(p->tpb, p->r, large_g, p->gcap, p->small_max_g, sg);
   if (rc != LOITS_OK) { delete p; return rc; }
   // ---- work items
   const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;
@@ -416,9 +458,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   for (int64_t b = 0; b < n_densities; ++b) {
     const int64_t g = p->koff[b + 1] - p->koff[b];
     const bool large = g > p->gcap;
-    const int cap = large ? kMaxLargeGuideBits : sg.m_cap;
-    int m = 2;
-    while ((int64_t(1) << m) < 2 * g && m < cap) ++m;
+    const int m = guide_bits(g, large ? kMaxLargeGuideBits : sg.m_cap);
     p->gbits[b] = m;
     p->goff[b] = go;
     go += ((int64_t(1) << m) + 1 + 7) & ~int64_t(7);
@@ -442,6 +482,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->total_pk = pko;
   p->total_gc = gco;
   p->m_cap_b = sg.m_cap_b;
+  p->lbits_f = sg.lbits_f;
+  p->lbits_b = sg.lbits_b;
   p->fwd_smem = sg.fwd;
   p->fwd_smem_allowed = sg.fwd;
   p->bwd_smem_allowed = sg.bwd;
@@ -638,6 +680,7 @@ int launch_backward(const loits_batch_plan* p, BatchArgs& a, void* workspace, si
                       L.bwd_zero_hi - L.bwd_zero_lo, st) != cudaSuccess)
     return LOITS_ERR_CUDA;
   a.gbits_cap = p->m_cap_b;
+  a.lguide_bits = p->lbits_b;
   double* grho = carve<double>(workspace, L.grho);
   FwdKernel fk;
   BwdKernel bk;

@@ -465,6 +465,30 @@ def test_large_densities_sampled_from_global_memory(B, oracle_lib, threads):
     assert np.abs(cdf.cpu().numpy() - ref["cdf"]).max() <= CDF_TOL
 
 
+@pytest.mark.parametrize("threads,cut", [(256, True), (512, True), (1024, True), (1024, False)])
+def test_large_densities_across_many_chunks(B, oracle_lib, threads, cut):
+    """Large densities with millions of events beside small ones: each CTA
+    takes several forward tiles and backward chunks in turn, on different
+    densities (the backward's coarse shared guide is reloaded when the
+    density changes).  Events, rows and the VJP against the fp64 oracle."""
+    rng = np.random.default_rng(33)
+    case = _large_case(rng, [20000, 300, 70001, 9000, 15000],
+                       [2_000_000, 200_000, 2_500_000, 800_000, 1_500_000], cut=cut)
+    koff, counts = case["knot_offsets"], case["event_counts"]
+    eoff = np.concatenate([[0], np.cumsum(counts)])
+    ref = oracle_lib.d_forward(koff, eoff, case["grid"], case["values"], case.get("x_cut"), 77, 5)
+    case["cotangent"] = rng.standard_normal(len(ref["events"])).astype(np.float32)
+    out = run_batch(B, case, B.make_config(threads=threads), with_intervals=False)
+    assert np.array_equal(out["rows"], ref["row_offsets"])
+    np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+    gref = oracle_lib.d_backward(koff, eoff, case["grid"], case["values"], case.get("x_cut"), 77,
+                                 5, case["cotangent"], fwd=ref)
+    for b in range(len(counts)):
+        o, e = koff[b], koff[b + 1]
+        scale = np.abs(gref[o:e]).max()
+        assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b
+
+
 def test_large_densities_plain_and_persistent_agree(B):
     rng = np.random.default_rng(32)
     case = _large_case(rng, [12000, 40000], [80_000, 120_000])
