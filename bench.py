@@ -366,6 +366,56 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     same = torch.equal(pstep.events[:valid], step.events[:valid])
     del pstep, pplan
 
+    # ---- saved-state form: the forward also writes (interval, offset) per
+    # kept row, the backward reads them instead of replaying the uniforms
+    sstep = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None, saved_state=True)
+    sstep.grid.copy_(step.grid); sstep.values.copy_(step.values)
+    if spec.x_cut is not None:
+        sstep.x_cut.copy_(step.x_cut)
+    sstep.grad_events.copy_(step.grad_events)
+    for _ in range(max(args.warmup, 3)):
+        sstep.forward()
+        sstep.backward()
+    torch.cuda.synchronize(dev)
+    sstep.check_status()
+    s_fwd, s_bwd = [], []
+    for _ in range(args.steps):
+        ev[0].record(stream)
+        sstep.forward()
+        ev[1].record(stream)
+        sstep.backward()
+        ev[2].record(stream)
+        ev[2].synchronize()
+        s_fwd.append(ev[0].elapsed_time(ev[1]))
+        s_bwd.append(ev[1].elapsed_time(ev[2]))
+    sstep.capture()
+    for _ in range(args.warmup):
+        sstep.step()
+    barrier()
+    t0.record(stream)
+    for _ in range(args.steps):
+        sstep.step()
+    t1.record(stream)
+    barrier()
+    sstep.check_status()
+    state_ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        state_ms = max_over_ranks(state_ms)
+    gscale = float(step.grad_values.abs().max().item()) or 1.0
+    saved_state = {
+        "value": events_step / (state_ms * 1e-3), "ms_per_step": state_ms,
+        "kernels_ms": {"batch_forward_kernel": float(np.mean(s_fwd)),
+                       "batch_backward_kernel": float(np.mean(s_bwd))},
+        "form": "forward writes interval (int32) + offset u - c_j (fp32) per kept row; "
+                "backward reads them, one CUDA graph",
+        "state_bytes": 8 * valid,
+        "events_identical": bool(torch.equal(sstep.events[:valid], step.events[:valid])),
+        "grad_max_diff_over_scale": float((sstep.grad_values - step.grad_values).abs().max()
+                                          .item()) / gscale,
+    }
+    sstep.graph = None
+    del sstep
+
     # ---- end to end through the public autograd API, host buffers
     e2e = run_e2e(args, spec, dev, rank, world, dist)
 
@@ -406,6 +456,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
                   "form": "one forward + one backward launch per density, no graph",
                   "batched_over_plain": value / plain_value, "events_identical": bool(same)},
         "kernels_ms": {"batch_forward_kernel": f_ms, "batch_backward_kernel": b_ms},
+        "saved_state": saved_state,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,

@@ -201,6 +201,29 @@ int loits_batch_backward(const loits_batch_plan* plan, const float* grid, const 
                          const float* grad_events, float* grad_values, void* workspace,
                          void* stream);
 
+/* Saved-state forward: loits_batch_forward plus, for every kept row, the
+ * two per-event quantities its VJP needs besides the cotangent -- the
+ * interval j (int32) and the offset t = u - c_j inside it (fp32, the value
+ * the sampler interpolated with).  This is the compact form of the state the
+ * reference saves for its backward (u_x / interval_x / packed / row_offsets,
+ * openmp/bindings.cpp:85-131, read by interpolation_vjp_x,
+ * cpp/loits_core.cpp:268-338): 8 bytes per kept row in row order instead of
+ * padded per-slot arrays.  intervals, offsets: capacity entries each. */
+int loits_batch_forward_state(const loits_batch_plan* plan, const float* grid,
+                              const float* values, const float* x_cut, uint64_t seed,
+                              uint64_t sequence, float* events, int64_t* row_offsets,
+                              int32_t* intervals, float* offsets, void* workspace, void* stream);
+
+/* VJP from a saved state: the same gradient as loits_batch_backward (up to
+ * fp32 accumulation order), reading each kept row's interval, offset and
+ * cotangent instead of regenerating its uniform and searching its interval.
+ * intervals / offsets: as written by loits_batch_forward_state with this
+ * workspace (intervals are clamped to the density's range). */
+int loits_batch_backward_state(const loits_batch_plan* plan, const float* grid,
+                               const float* values, const float* x_cut, const int32_t* intervals,
+                               const float* offsets, const float* grad_events, float* grad_values,
+                               void* workspace, void* stream);
+
 /* The forward's CDF of every knot as fp64 (hi + lo), total_knots entries;
  * norm: B fp64 normalisers (may be NULL). */
 int loits_batch_cdf(const loits_batch_plan* plan, const void* workspace, double* cdf,

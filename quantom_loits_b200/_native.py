@@ -78,6 +78,9 @@ SIGNATURES = {
     "loits_batch_plan_config": (C.c_int, [_vp, C.POINTER(BatchConfig)]),
     "loits_batch_forward": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _vp, _vp, _vp, _vp, _vp]),
     "loits_batch_backward": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _vp, _vp, _vp, _vp]),
+    "loits_batch_forward_state": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _vp, _vp, _vp, _vp,
+                                            _vp, _vp]),
+    "loits_batch_backward_state": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "loits_batch_cdf": (C.c_int, [_vp, _vp, _vp, _vp, _vp]),
     "loits_batch_quantile": (C.c_int, [_vp, _vp, _i64, _vp, _i64, _vp, _vp, _vp]),
     "loits_batch_forward_hist": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _i32, C.c_float,

@@ -138,6 +138,12 @@ class BatchPlan:
     def new_row_offsets(self) -> torch.Tensor:
         return torch.empty(self.n_densities + 1, dtype=torch.int64, device=self.device)
 
+    def new_state(self) -> tuple[torch.Tensor, torch.Tensor]:
+        """Buffers of a saved state: (intervals int32, offsets fp32), capacity rows."""
+        n = max(self.capacity, 4)
+        return (torch.empty(n, dtype=torch.int32, device=self.device),
+                torch.empty(n, dtype=torch.float32, device=self.device))
+
     def status_view(self, workspace: torch.Tensor) -> torch.Tensor:
         return workspace[self.status_offset:self.status_offset + 4].view(torch.int32)
 
@@ -157,6 +163,27 @@ class BatchPlan:
                 self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed),
                 int(sequence), grad_events.data_ptr(), grad_values.data_ptr(),
                 workspace.data_ptr(), N.stream_of(self.device)), "loits_batch_backward")
+
+    def forward_state(self, grid, values, x_cut, seed, sequence, events, row_offsets, intervals,
+                      offsets, workspace) -> None:
+        """Forward that also saves, per kept row, its interval and its offset
+        u - c_j (the saved state ``backward_state`` reads)."""
+        with torch.cuda.device(self.device):
+            N.check(self._lib.loits_batch_forward_state(
+                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut), int(seed),
+                int(sequence), events.data_ptr(), row_offsets.data_ptr(), intervals.data_ptr(),
+                offsets.data_ptr(), workspace.data_ptr(), N.stream_of(self.device)),
+                "loits_batch_forward_state")
+
+    def backward_state(self, grid, values, x_cut, intervals, offsets, grad_events, grad_values,
+                       workspace) -> None:
+        """VJP from the saved state of ``forward_state`` (same workspace)."""
+        with torch.cuda.device(self.device):
+            N.check(self._lib.loits_batch_backward_state(
+                self.handle, grid.data_ptr(), values.data_ptr(), N.ptr(x_cut),
+                intervals.data_ptr(), offsets.data_ptr(), grad_events.data_ptr(),
+                grad_values.data_ptr(), workspace.data_ptr(), N.stream_of(self.device)),
+                "loits_batch_backward_state")
 
     def forward_hist(self, grid, values, x_cut, seed, sequence, bins, lo, hi, hist, kept,
                      workspace) -> None:
@@ -255,6 +282,38 @@ class _BatchFunction(torch.autograd.Function):
         return grad_values, None, None, None, None, None
 
 
+class _StateFunction(torch.autograd.Function):
+    """Saved-state form of _BatchFunction: the forward keeps each kept row's
+    interval and offset (8 bytes per row) and the backward reads them."""
+
+    @staticmethod
+    def forward(ctx, values, grid, x_cut, plan: BatchPlan, seed, sequence):
+        events = plan.new_events()
+        rows = plan.new_row_offsets()
+        ws = plan.new_workspace()
+        ints, offs = plan.new_state()
+        plan.forward_state(grid, values, x_cut, seed, sequence, events, rows, ints, offs, ws)
+        status = plan.status_view(ws)
+        head = torch.cat([rows[-1:], status.to(torch.int64)]).tolist()  # one sync
+        valid, st = int(head[0]), int(head[1])
+        N.check(st, "loits_batch_forward_state (device)")
+        ctx.plan, ctx.x_cut, ctx.valid = plan, x_cut, valid
+        ctx.save_for_backward(values, grid, ws, ints, offs)
+        ctx.mark_non_differentiable(rows)
+        return events[:valid], rows
+
+    @staticmethod
+    def backward(ctx, grad_events, grad_rows):
+        values, grid, ws, ints, offs = ctx.saved_tensors
+        plan: BatchPlan = ctx.plan
+        g = torch.zeros(max(plan.capacity, 4), dtype=torch.float32, device=values.device)
+        if grad_events is not None and ctx.valid:
+            g[:ctx.valid] = grad_events.to(torch.float32)
+        grad_values = torch.empty_like(values)
+        plan.backward_state(grid, values, ctx.x_cut, ints, offs, g, grad_values, ws)
+        return grad_values, None, None, None, None, None
+
+
 class _HistFunction(torch.autograd.Function):
     @staticmethod
     def forward(ctx, values, grid, x_cut, plan: BatchPlan, seed, sequence, bins, lo, hi):
@@ -290,9 +349,14 @@ class BatchedLOITS:
 
     ``config``: None (the plan's defaults: CTA size by occupancy), a
     ``loits_batch_config`` / dict, or ``"auto"``: the launch geometry is timed
-    on the first batch of each shape bucket (:mod:`quantom_loits_b200.tuning`)."""
+    on the first batch of each shape bucket (:mod:`quantom_loits_b200.tuning`).
 
-    def __init__(self, device="cuda", seed=None, config=None, device_sequence=False):
+    ``saved_state``: keep each kept row's interval and offset between forward
+    and backward (8 bytes per row) so that the backward reads them instead of
+    regenerating the uniforms and searching the intervals."""
+
+    def __init__(self, device="cuda", seed=None, config=None, device_sequence=False,
+                 saved_state=False):
         self.device = torch.device(device)
         N.require_device(self.device)
         self.seed = torch.initial_seed() if seed is None else int(seed)
@@ -303,6 +367,7 @@ class BatchedLOITS:
         # captured CUDA graph draws fresh uniforms on every replay
         self.sequence_dev = (torch.zeros(1, dtype=torch.int64, device=self.device)
                              if device_sequence else None)
+        self.saved_state = bool(saved_state)
         self._plans: dict = {}
 
     def plan_for(self, knot_offsets, event_counts, batch=None, hist=None) -> BatchPlan:
@@ -334,7 +399,8 @@ class BatchedLOITS:
         plan = self.plan_for(batch.knot_offsets, counts, batch)
         grid = batch.grid.detach().contiguous()
         x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
-        return _BatchFunction.apply(batch.values, grid, x_cut, plan, self.seed, sequence)
+        fn = _StateFunction if self.saved_state else _BatchFunction
+        return fn.apply(batch.values, grid, x_cut, plan, self.seed, sequence)
 
     __call__ = sample
 
@@ -374,7 +440,8 @@ class BatchStep:
     after each step (the kept-row count is ``row_offsets[-1]``, on the device).
     """
 
-    def __init__(self, plan: BatchPlan, seed: int, sequence: int = 0, with_cut=False):
+    def __init__(self, plan: BatchPlan, seed: int, sequence: int = 0, with_cut=False,
+                 saved_state=False):
         self.plan = plan
         dev = plan.device
         self.seed, self.sequence = int(seed), int(sequence)
@@ -387,15 +454,24 @@ class BatchStep:
         self.grad_events = torch.zeros(max(plan.capacity, 4), dtype=torch.float32, device=dev)
         self.grad_values = torch.empty(plan.total_knots, dtype=torch.float32, device=dev)
         self.workspace = plan.new_workspace()
+        self.state = plan.new_state() if saved_state else None
         self.graph = None
 
     def forward(self):
-        self.plan.forward(self.grid, self.values, self.x_cut, self.seed, self.sequence,
-                          self.events, self.row_offsets, self.workspace)
+        if self.state is not None:
+            self.plan.forward_state(self.grid, self.values, self.x_cut, self.seed, self.sequence,
+                                    self.events, self.row_offsets, *self.state, self.workspace)
+        else:
+            self.plan.forward(self.grid, self.values, self.x_cut, self.seed, self.sequence,
+                              self.events, self.row_offsets, self.workspace)
 
     def backward(self):
-        self.plan.backward(self.grid, self.values, self.x_cut, self.seed, self.sequence,
-                           self.grad_events, self.grad_values, self.workspace)
+        if self.state is not None:
+            self.plan.backward_state(self.grid, self.values, self.x_cut, *self.state,
+                                     self.grad_events, self.grad_values, self.workspace)
+        else:
+            self.plan.backward(self.grid, self.values, self.x_cut, self.seed, self.sequence,
+                               self.grad_events, self.grad_values, self.workspace)
 
     def step(self):
         if self.graph is not None:

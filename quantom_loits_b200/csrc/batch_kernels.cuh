@@ -102,9 +102,12 @@ struct BatchArgs {
   float* events;
   int64_t* row_offsets;
   int32_t* intervals;
+  float* offsets;              // saved state: u - c_j of each kept row (with intervals)
   // backward
   const float* grad;
   float* grad_values;
+  const int32_t* st_intervals; // saved state read instead of replaying the uniforms
+  const float* st_offsets;
   // histogram mode (events are binned instead of written; see hist_bin)
   float* hist;                 // forward: [B * hist_bins], accumulated
   unsigned long long* kept;    // forward: [B] kept events per density

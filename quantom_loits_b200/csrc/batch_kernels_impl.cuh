@@ -770,7 +770,8 @@ __device__ __forceinline__ void warp_store(const float* __restrict__ src, float*
   if (tail0 + lane < n) dst[tail0 + lane] = __ldcg(&src[tail0 + lane]);
 }
 
-// Optional per-row interval output (diagnostics): recomputed for kept rows.
+// Optional per-row interval (diagnostics, saved state) and offset u - c_j
+// (saved state) output of a general tile: recomputed for its kept rows.
 template <int TPB, int R, int kMode>
 __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGeom& tg,
                                                 const DensView& d, int64_t row0) {
@@ -781,6 +782,7 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
     const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
     const uint32_t range = d.skip ? 0u : block_range_mask(tg, blk);
     int js[4] = {0, 0, 0, 0};
+    float ts[4] = {0.f, 0.f, 0.f, 0.f};
     uint32_t keep = 0;
     if (range) {
       const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
@@ -788,13 +790,19 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
       const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
       keep = (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3)) & range;
       js[0] = e0.j; js[1] = e1.j; js[2] = e2.j; js[3] = e3.j;
+      ts[0] = e0.t; ts[1] = e1.t; ts[2] = e2.t; ts[3] = e3.t;
     }
     int total;
     const int excl = warp_exclusive_count(__popc(keep), total);
     int k = 0;
 #pragma unroll
-    for (int i = 0; i < 4; ++i)
-      if (keep & (1u << i)) a.intervals[row + excl + k++] = js[i];
+    for (int i = 0; i < 4; ++i) {
+      if (keep & (1u << i)) {
+        if (a.intervals) a.intervals[row + excl + k] = js[i];
+        if (a.offsets) a.offsets[row + excl + k] = ts[i];
+        ++k;
+      }
+    }
     row += total;
   }
 }
@@ -829,6 +837,7 @@ __device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, c
     }
     if (t == a.tiles_total - 1) {
       for (int dd = a.last_nonempty + 1; dd <= a.nd; ++dd) a.row_offsets[dd] = base + cnt;
+      a.tile_prefix[t + 1] = base + cnt;  // one past the last row
     }
   }
   return base;
@@ -924,6 +933,13 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
       if (keep & 4u) a.intervals[q++] = e2.j;
       if (keep & 8u) a.intervals[q] = e3.j;
     }
+    if (a.offsets) {
+      int64_t q = pos;
+      if (keep & 1u) a.offsets[q++] = e0.t;
+      if (keep & 2u) a.offsets[q++] = e1.t;
+      if (keep & 4u) a.offsets[q++] = e2.t;
+      if (keep & 8u) a.offsets[q] = e3.t;
+    }
     if (keep & 1u) __stcs(&a.events[pos++], e0.x);
     if (keep & 2u) __stcs(&a.events[pos++], e1.x);
     if (keep & 4u) __stcs(&a.events[pos++], e2.x);
@@ -966,6 +982,12 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, const TileGe
       if (range & 2u) a.intervals[row0 + 1] = e1.j;
       if (range & 4u) a.intervals[row0 + 2] = e2.j;
       if (range & 8u) a.intervals[row0 + 3] = e3.j;
+    }
+    if (a.offsets) {
+      if (range & 1u) a.offsets[row0] = e0.t;
+      if (range & 2u) a.offsets[row0 + 1] = e1.t;
+      if (range & 4u) a.offsets[row0 + 2] = e2.t;
+      if (range & 8u) a.offsets[row0 + 3] = e3.t;
     }
   }
 }
@@ -1019,7 +1041,7 @@ __device__ __forceinline__ void sample_tile_general(const BatchArgs& a, int32_t 
   __syncthreads();
   const int64_t row0 = sh.base + warp_excl;
   warp_store(sw, a.events + row0, acc);
-  if (a.intervals) write_intervals<TPB, R, kMode>(a, tg, d, row0);
+  if (a.intervals || a.offsets) write_intervals<TPB, R, kMode>(a, tg, d, row0);
 }
 
 // ------------------------------------------------------- histogram mode
@@ -1171,6 +1193,45 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
   }
 }
 
+// Backward chunk from a saved state: the chunk's kept rows [r0, r1) carry
+// their interval and offset u - c_j, so no uniform is regenerated and no
+// interval searched; each row scatters exactly what scatter_slot would for
+// the replayed slot.  Saved intervals are clamped to [0, G - 2], so reads
+// stay inside the density for any state contents.
+template <int TPB, int kMode>
+__device__ __forceinline__ void vjp_chunk_rows(const BatchArgs& a, const DensView& d, int64_t r0,
+                                               int64_t r1, float* gacc_s, float2* gc) {
+  constexpr int U = 4;  // rows per thread in flight
+  const int jmax = d.G - 2;
+  if (jmax < 0) return;
+#pragma unroll 1
+  for (int64_t base = r0; base < r1; base += static_cast<int64_t>(TPB) * U) {
+    Slot e[U];
+    float g[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int64_t r = base + i * TPB + threadIdx.x;
+      e[i].ok = r < r1;
+      e[i].j = 0;
+      e[i].t = 0.0f;
+      g[i] = 0.0f;
+      if (e[i].ok) {
+        e[i].j = min(max(__ldcs(&a.st_intervals[r]), 0), jmax);
+        e[i].t = __ldcs(&a.st_offsets[r]);
+        g[i] = __ldcs(&a.grad[r]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      if (!e[i].ok) continue;
+      const float* m = reinterpret_cast<const float*>(d.rec + e[i].j) + 3;
+      if constexpr (kMode == kShared) e[i].m = *m;
+      else e[i].m = __ldg(m);
+      scatter_slot<kMode>(e[i], g[i], d, gacc_s, gc);
+    }
+  }
+}
+
 // The tiles [t_first, t_end) of one backward chunk.  Every warp replays its
 // own slots of each tile; the forward recorded where its kept rows start
 // (tile_prefix + warp_off), so no scan across warps and no barrier is needed.
@@ -1181,6 +1242,13 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (d.skip) return;
+  if (a.st_intervals) {
+    // saved state: the chunk's rows run from its first tile's first row to
+    // the next tile's (tile_prefix has an entry past the last tile)
+    vjp_chunk_rows<TPB, kMode>(a, d, __ldcg(&a.tile_prefix[t_first]),
+                               __ldcg(&a.tile_prefix[t_end]), gacc_s, gc);
+    return;
+  }
   // kThreshold densities keep exactly the slots the forward kept by threshold
   const int kstar = d.threshold ? kept_threshold<kMode>(d) : 0;
   if (gh) {

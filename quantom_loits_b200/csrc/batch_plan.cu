@@ -558,7 +558,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   L.cagg = o; o = align_up(o + static_cast<size_t>(nc) * 8);
   L.cinc = o; o = align_up(o + static_cast<size_t>(nc) * 8);
   L.cmax = o; o = align_up(o + static_cast<size_t>(nc) * 8);
-  L.tile_prefix = o; o = align_up(o + static_cast<size_t>(nt) * 8);
+  L.tile_prefix = o; o = align_up(o + static_cast<size_t>(nt + 1) * 8);  // + one past the end
   L.warp_off = o; o = align_up(o + static_cast<size_t>(nt) * (p->tpb / 32) * 4);
   L.stage = o; o = align_up(o + static_cast<size_t>(p->fwd_grid) * tile_events * 4);
   L.partials = o; o = align_up(o + static_cast<size_t>(po) * 4);
@@ -759,6 +759,44 @@ extern "C" int loits_batch_backward(const loits_batch_plan* p, const float* grid
   BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
   a.grad = grad_events;
   a.grad_values = grad_values;
+  return launch_backward(p, a, workspace, p->bwd_smem, static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int loits_batch_forward_state(const loits_batch_plan* p, const float* grid,
+                                         const float* values, const float* x_cut, uint64_t seed,
+                                         uint64_t sequence, float* events, int64_t* row_offsets,
+                                         int32_t* intervals, float* offsets, void* workspace,
+                                         void* stream) {
+  if (p && p->capacity > 0 && (!intervals || !offsets)) return LOITS_ERR_INVALID;
+  if (!p || !grid || !values || !row_offsets || !workspace) return LOITS_ERR_INVALID;
+  if (p->capacity > 0 && (!events || !aligned16(events))) return LOITS_ERR_INVALID;
+  if (!aligned16(workspace)) return LOITS_ERR_INVALID;
+  if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  if (p->n_tiles == 0 &&
+      cudaMemsetAsync(row_offsets, 0, (p->nd + 1) * sizeof(int64_t), st) != cudaSuccess)
+    return LOITS_ERR_CUDA;
+  BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.events = events;
+  a.row_offsets = row_offsets;
+  a.intervals = intervals;
+  a.offsets = offsets;
+  return launch_forward(p, a, workspace, p->fwd_smem, st);
+}
+
+extern "C" int loits_batch_backward_state(const loits_batch_plan* p, const float* grid,
+                                          const float* values, const float* x_cut,
+                                          const int32_t* intervals, const float* offsets,
+                                          const float* grad_events, float* grad_values,
+                                          void* workspace, void* stream) {
+  if (!p || !grid || !values || !grad_values || !workspace) return LOITS_ERR_INVALID;
+  if (p->capacity > 0 && (!grad_events || !intervals || !offsets)) return LOITS_ERR_INVALID;
+  if (!aligned16(workspace)) return LOITS_ERR_INVALID;
+  BatchArgs a = step_args(p, workspace, grid, values, x_cut, 0, 0);
+  a.grad = grad_events;
+  a.grad_values = grad_values;
+  a.st_intervals = intervals;
+  a.st_offsets = offsets;
   return launch_backward(p, a, workspace, p->bwd_smem, static_cast<cudaStream_t>(stream));
 }
 
