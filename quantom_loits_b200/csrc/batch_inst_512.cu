@@ -4,20 +4,28 @@
 namespace loits_dev {
 
 template __global__ void batch_forward_kernel<512, 2, false>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 2, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 2, false, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 2, false, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 2, true>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 2, true>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 2, true, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 2, true, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 4, false>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 4, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 4, false, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 4, false, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 4, true>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 4, true>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 4, true, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 4, true, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 8, false>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 8, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 8, false, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 8, false, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 8, true>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 8, true>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 8, true, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 8, true, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 16, false>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 16, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 16, false, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 16, false, true>(BatchArgs, double*);
 template __global__ void batch_forward_kernel<512, 16, true>(BatchArgs);
-template __global__ void batch_backward_kernel<512, 16, true>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 16, true, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<512, 16, true, true>(BatchArgs, double*);
 
 }  // namespace loits_dev

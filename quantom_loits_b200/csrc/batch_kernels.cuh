@@ -58,6 +58,9 @@ struct BatchArgs {
   int32_t mcap;                // guide entries (M + 1) a sampling CTA holds
   int32_t gbits_cap;           // most guide bits this launch copies to shared memory
   int32_t lguide_bits;         // large densities: bits of the coarse guide in shared memory
+  int32_t win_n;               // backward: large densities' fixed-point window (intervals, 0: none)
+  int32_t bwd_guide_off;       // backward: uint32 words from the start of dynamic shared
+                               // memory to the guide
                                // (a larger guide is read every 2^s-th count)
   int32_t tiles_per_chunk;
   int64_t nmax;                // Philox slots per density (slot stride)

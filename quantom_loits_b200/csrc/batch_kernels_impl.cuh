@@ -553,9 +553,14 @@ struct DensView {
 
 struct SampleShared {
   int warp_cnt[32];
+  float red[32];
   int64_t base;
   uint32_t flags;
   float cut;
+  float fix_scale;   // backward chunk: fixed-point units per cotangent unit
+  int nonfinite;     // backward chunk: a non-finite contribution was seen
+  int win_b;         // density whose fixed-point window win_lo belongs to
+  int win_lo;
 };
 
 // Wait until density b's CDF is final (thread 0) and share its flags and cut.
@@ -1172,24 +1177,95 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
 
 // --------------------------------------------------------- backward phase
 
+// Where a backward chunk accumulates its grad-CDF.
+//  * small densities, fp32: gacc (shared memory), two fp32 atomics per kept
+//    slot;
+//  * small densities, fixed point (fix): per interval j the two sums
+//    A_j = sum g and B_j = sum g w, each a 64-bit two's-complement integer in
+//    units of 1/scale held as a low uint32 word and a high int32 word
+//    (alo/ahi/blo/bhi, planar so that consecutive intervals use consecutive
+//    banks).  Shared-memory fp32 atomicAdd is a compare-and-swap loop; uint32
+//    atomicAdd is one native instruction, and integer sums do not depend on
+//    their order.  The chunk's grad-CDF is formed from A and B when the chunk
+//    ends: gcdf_k = m_k (B_k - A_k) - m_{k-1} B_{k-1};
+//  * large densities: the same fixed-point sums for the intervals of a window
+//    [win_lo, win_lo + win_n) (the most probable ones), one float2 global
+//    atomic per kept slot for the others (gc).
+struct Acc {
+  float* gacc;
+  uint32_t *alo, *ahi, *blo, *bhi;
+  float2* gc;
+  float scale;
+  int win_lo, win_n;
+  int* nonfinite;
+};
+
+// Fixed-point value of f (already scaled): f rounded to an integer.
+__device__ __forceinline__ long long fix_round(float f) {
+  return fabsf(f) < 2.0e9f ? static_cast<long long>(__float2int_rn(f)) : __float2ll_rn(f);
+}
+
+// Adds v to the 64-bit sum (lo, hi): one uint32 atomic on the low word; the
+// high word takes the carry and v's high part when they do not cancel (for
+// |v| < 2^31: only when the low word wraps).
+__device__ __forceinline__ void fix_add(uint32_t* lo, uint32_t* hi, int i, long long v) {
+  const uint32_t vl = static_cast<uint32_t>(v);
+  const uint32_t vh = static_cast<uint32_t>(static_cast<unsigned long long>(v) >> 32);
+  const uint32_t old = atomicAdd(&lo[i], vl);
+  const uint32_t h = vh + (old + vl < old ? 1u : 0u);
+  if (h != 0u) atomicAdd(&hi[i], h);
+}
+
+__device__ __forceinline__ double fix_value(uint32_t lo, uint32_t hi, double inv_scale) {
+  return static_cast<double>(static_cast<long long>((static_cast<unsigned long long>(hi) << 32) |
+                                                    lo)) * inv_scale;
+}
+
+// One kept slot's (g, g w) into fixed-point slot i.  Values whose scaled
+// magnitude reaches 2^63 (non-finite cotangents among them) are not added;
+// they mark the chunk, whose gradient then becomes NaN, as any non-finite
+// cotangent makes the reference's (its normaliser VJP sums over every knot).
+__device__ __forceinline__ void fix_pair(const Acc& acc, int i, float g, float w) {
+  const float f0 = g * acc.scale, f1 = (g * w) * acc.scale;
+  if (!(fabsf(f0) < 9.0e18f) || !(fabsf(f1) < 9.0e18f)) {
+    *acc.nonfinite = 1;
+    return;
+  }
+  fix_add(acc.alo, acc.ahi, i, fix_round(f0));
+  fix_add(acc.blo, acc.bhi, i, fix_round(f1));
+}
+
+__device__ __forceinline__ void red_add_f32x2(float2* p, float x, float y) {
+  asm volatile("red.global.add.v2.f32 [%0], {%1, %2};" ::"l"(p), "f"(x), "f"(y) : "memory");
+}
+
 // Scatter of one kept slot's cotangent into the grad-CDF:
 // d x / d c_j = m (w - 1), d x / d c_{j+1} = -m w, w = (u - c_j) / d_j
-// (cpp/loits_core.cpp:293-300).  Small densities: fp32 shared-memory
-// atomics into the chunk's grad-CDF; large densities: one float2 global
-// atomic into interval j's pair (sum to knot j, sum to knot j + 1).
-template <int kMode>
+// (cpp/loits_core.cpp:293-300).
+// kFix (small densities): fixed-point sums instead of fp32 atomics.
+template <int kMode, bool kFix>
 __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensView& d,
-                                             float* gacc_s, float2* gc) {
+                                             const Acc& acc) {
   float inv;
   if constexpr (kMode == kShared) inv = d.invd[e.j];
   else inv = __ldg(&d.invd[e.j]);
   const float w = e.t * inv;
-  const float mg = e.m * g;
   if constexpr (kMode == kShared) {
-    atomicAdd(&gacc_s[e.j], mg * (w - 1.0f));
-    atomicAdd(&gacc_s[e.j + 1], -(mg * w));
+    if constexpr (kFix) {
+      fix_pair(acc, e.j, g, w);
+    } else {
+      const float mg = e.m * g;
+      atomicAdd(&acc.gacc[e.j], mg * (w - 1.0f));
+      atomicAdd(&acc.gacc[e.j + 1], -(mg * w));
+    }
   } else {
-    atomicAdd(&gc[e.j], make_float2(mg * (w - 1.0f), -(mg * w)));
+    const unsigned wj = static_cast<unsigned>(e.j - acc.win_lo);
+    if (wj < static_cast<unsigned>(acc.win_n)) {
+      fix_pair(acc, static_cast<int>(wj), g, w);
+    } else {
+      const float mg = e.m * g;
+      red_add_f32x2(&acc.gc[e.j], mg * (w - 1.0f), -(mg * w));
+    }
   }
 }
 
@@ -1198,9 +1274,9 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
 // interval searched; each row scatters exactly what scatter_slot would for
 // the replayed slot.  Saved intervals are clamped to [0, G - 2], so reads
 // stay inside the density for any state contents.
-template <int TPB, int kMode>
+template <int TPB, int kMode, bool kFix>
 __device__ __forceinline__ void vjp_chunk_rows(const BatchArgs& a, const DensView& d, int64_t r0,
-                                               int64_t r1, float* gacc_s, float2* gc) {
+                                               int64_t r1, const Acc& acc) {
   constexpr int U = 4;  // rows per thread in flight
   const int jmax = d.G - 2;
   if (jmax < 0) return;
@@ -1227,7 +1303,7 @@ __device__ __forceinline__ void vjp_chunk_rows(const BatchArgs& a, const DensVie
       const float* m = reinterpret_cast<const float*>(d.rec + e[i].j) + 3;
       if constexpr (kMode == kShared) e[i].m = *m;
       else e[i].m = __ldg(m);
-      scatter_slot<kMode>(e[i], g[i], d, gacc_s, gc);
+      scatter_slot<kMode, kFix>(e[i], g[i], d, acc);
     }
   }
 }
@@ -1235,18 +1311,18 @@ __device__ __forceinline__ void vjp_chunk_rows(const BatchArgs& a, const DensVie
 // The tiles [t_first, t_end) of one backward chunk.  Every warp replays its
 // own slots of each tile; the forward recorded where its kept rows start
 // (tile_prefix + warp_off), so no scan across warps and no barrier is needed.
-template <int TPB, int R, int kMode>
+template <int TPB, int R, int kMode, bool kFix>
 __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensView& d, TileGeom tg,
                                                 int32_t tb, int32_t t_first, int32_t t_end,
-                                                float* gacc_s, float2* gc, const float* gh) {
+                                                const Acc& acc, const float* gh) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   if (d.skip) return;
   if (a.st_intervals) {
     // saved state: the chunk's rows run from its first tile's first row to
     // the next tile's (tile_prefix has an entry past the last tile)
-    vjp_chunk_rows<TPB, kMode>(a, d, __ldcg(&a.tile_prefix[t_first]),
-                               __ldcg(&a.tile_prefix[t_end]), gacc_s, gc);
+    vjp_chunk_rows<TPB, kMode, kFix>(a, d, __ldcg(&a.tile_prefix[t_first]),
+                               __ldcg(&a.tile_prefix[t_end]), acc);
     return;
   }
   // kThreshold densities keep exactly the slots the forward kept by threshold
@@ -1268,10 +1344,10 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
         const uint32_t keep = (d.threshold ? threshold_keep(w, kstar)
                                            : (e0.ok | (e1.ok << 1) | (e2.ok << 2) | (e3.ok << 3))) &
                               range;
-        if (keep & 1u) scatter_slot<kMode>(e0, hist_cotangent(a, gh, e0.x), d, gacc_s, gc);
-        if (keep & 2u) scatter_slot<kMode>(e1, hist_cotangent(a, gh, e1.x), d, gacc_s, gc);
-        if (keep & 4u) scatter_slot<kMode>(e2, hist_cotangent(a, gh, e2.x), d, gacc_s, gc);
-        if (keep & 8u) scatter_slot<kMode>(e3, hist_cotangent(a, gh, e3.x), d, gacc_s, gc);
+        if (keep & 1u) scatter_slot<kMode, kFix>(e0, hist_cotangent(a, gh, e0.x), d, acc);
+        if (keep & 2u) scatter_slot<kMode, kFix>(e1, hist_cotangent(a, gh, e1.x), d, acc);
+        if (keep & 4u) scatter_slot<kMode, kFix>(e2, hist_cotangent(a, gh, e2.x), d, acc);
+        if (keep & 8u) scatter_slot<kMode, kFix>(e3, hist_cotangent(a, gh, e3.x), d, acc);
       }
     }
     return;
@@ -1305,10 +1381,10 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
         // grad-CDF atomics (which the compiler cannot prove disjoint)
         const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
         const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
-        if (range & 1u) scatter_slot<kMode>(e0, g4.x, d, gacc_s, gc);
-        if (range & 2u) scatter_slot<kMode>(e1, g4.y, d, gacc_s, gc);
-        if (range & 4u) scatter_slot<kMode>(e2, g4.z, d, gacc_s, gc);
-        if (range & 8u) scatter_slot<kMode>(e3, g4.w, d, gacc_s, gc);
+        if (range & 1u) scatter_slot<kMode, kFix>(e0, g4.x, d, acc);
+        if (range & 2u) scatter_slot<kMode, kFix>(e1, g4.y, d, acc);
+        if (range & 4u) scatter_slot<kMode, kFix>(e2, g4.z, d, acc);
+        if (range & 8u) scatter_slot<kMode, kFix>(e3, g4.w, d, acc);
       }
     }
     return;
@@ -1336,17 +1412,108 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
       }
       int total;
       int64_t my = row + warp_exclusive_count(__popc(keep), total);
-      if (keep & 1u) scatter_slot<kMode>(e0, __ldcs(&a.grad[my++]), d, gacc_s, gc);
-      if (keep & 2u) scatter_slot<kMode>(e1, __ldcs(&a.grad[my++]), d, gacc_s, gc);
-      if (keep & 4u) scatter_slot<kMode>(e2, __ldcs(&a.grad[my++]), d, gacc_s, gc);
-      if (keep & 8u) scatter_slot<kMode>(e3, __ldcs(&a.grad[my]), d, gacc_s, gc);
+      if (keep & 1u) scatter_slot<kMode, kFix>(e0, __ldcs(&a.grad[my++]), d, acc);
+      if (keep & 2u) scatter_slot<kMode, kFix>(e1, __ldcs(&a.grad[my++]), d, acc);
+      if (keep & 4u) scatter_slot<kMode, kFix>(e2, __ldcs(&a.grad[my++]), d, acc);
+      if (keep & 8u) scatter_slot<kMode, kFix>(e3, __ldcs(&a.grad[my]), d, acc);
       row += total;
     }
   }
 }
 
-// Backward chunk (density, run of sampling tiles).
-template <int TPB, int R, bool kLarge>
+// The fixed-point paths are compiled for CTAs of 512 and 1024 threads only
+// (64 registers; the 48 of a 256-thread CTA would spill), whose shared memory
+// has room for them.
+template <int TPB>
+constexpr bool kFixPaths = TPB >= 512;
+
+// Fixed-point scale of a backward chunk (into sh.fix_scale): a power of two
+// that puts the mean |cotangent| of up to TPB of the chunk's kept rows near
+// 2^20, so one unit is about 1e-6 of a typical contribution; larger values
+// take more bits (up to 2^63).  Histogram mode: the mean histogram-cotangent
+// step instead.  Ends with a barrier.
+template <int TPB>
+__device__ __forceinline__ void chunk_scale(const BatchArgs& a, const float* gh, int64_t r0,
+                                            int64_t r1, SampleShared& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  float v = 0.0f, c = 0.0f;
+  if (gh) {
+    const int nb = a.hist_bins;
+    for (int k = threadIdx.x; k <= nb; k += TPB) {
+      const float g1 = k < nb ? gh[k] : 0.0f, g0 = k > 0 ? gh[k - 1] : 0.0f;
+      const float q = fabsf(g1 - g0) * a.hist_inv_h;
+      if (q < 3.0e38f) { v += q; c += 1.0f; }
+    }
+  } else if (r0 + threadIdx.x < r1) {
+    const float q = fabsf(__ldcg(&a.grad[r0 + threadIdx.x]));
+    if (q < 3.0e38f) { v = q; c = 1.0f; }
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    v += __shfl_xor_sync(0xffffffffu, v, o);
+    c += __shfl_xor_sync(0xffffffffu, c, o);
+  }
+  if (lane == 0) { sh.red[warp] = v; sh.warp_cnt[warp] = static_cast<int>(c); }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    float sum = 0.0f;
+    int cnt = 0;
+    for (int w = 0; w < TPB / 32; ++w) { sum += sh.red[w]; cnt += sh.warp_cnt[w]; }
+    int e = 0;
+    if (cnt > 0 && sum > 0.0f) frexpf(sum / cnt, &e);
+    e = min(max(e, -100), 100);
+    sh.fix_scale = ldexpf(1.0f, 20 - e);
+    sh.nonfinite = 0;
+  }
+  __syncthreads();
+}
+
+// The window of a large density's fixed-point sums (into sh.win_lo): the run
+// of win_n intervals that holds the most probability, found on the coarse
+// guide in shared memory (bucket k0 .. k1 of the uniforms maps to intervals
+// L[k0] - 1 .. L[k1] - 1).  Ends with a barrier.
+template <int TPB>
+__device__ __forceinline__ void large_window(const BatchArgs& a, const DensView& d, int b,
+                                             SampleShared& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int M = 1 << (32 - d.shift);
+  const uint32_t* L = d.cguide;
+  const uint32_t room = static_cast<uint32_t>(a.win_n - 1);
+  int best_span = -1, best_k0 = 0;
+  for (int k0 = threadIdx.x * 4; k0 < M; k0 += TPB * 4) {
+    const uint32_t lim = L[k0] + room;
+    int lo = k0, hi = M;  // largest k1 in [k0, M] with L[k1] <= lim
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (L[mid] <= lim) lo = mid; else hi = mid - 1;
+    }
+    if (lo - k0 > best_span) { best_span = lo - k0; best_k0 = k0; }
+  }
+  const int wspan = __reduce_max_sync(0xffffffffu, best_span);
+  const int wk0 = __reduce_min_sync(0xffffffffu, best_span == wspan ? best_k0 : 0x7fffffff);
+  if (lane == 0) { sh.warp_cnt[warp] = wspan; sh.red[warp] = __int_as_float(wk0); }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int span = -1, k0 = 0;
+    for (int w = 0; w < TPB / 32; ++w) {
+      const int k = __float_as_int(sh.red[w]);
+      if (sh.warp_cnt[w] > span || (sh.warp_cnt[w] == span && k < k0)) {
+        span = sh.warp_cnt[w];
+        k0 = k;
+      }
+    }
+    const int n_int = d.G - 1;  // intervals of the density
+    int lo = static_cast<int>(L[k0]) - 1;
+    lo = min(lo, n_int - a.win_n);
+    sh.win_lo = max(lo, 0);
+    sh.win_b = b;
+  }
+  __syncthreads();
+}
+
+// Backward chunk (density, run of sampling tiles).  kFix: the plan has small
+// densities that sum in fixed point (compiled separately: the fp32 path
+// alone needs fewer registers).
+template <int TPB, int R, bool kLarge, bool kFix>
 __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
                                                uint32_t* guide_s, float* invd_s, float* gacc_s,
                                                SampleShared& sh, int& guide_key) {
@@ -1365,35 +1532,118 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
     const float* src = a.grad_hist + static_cast<int64_t>(b) * a.hist_bins;
     for (int k = threadIdx.x; k < a.hist_bins; k += TPB) gh[k] = __ldg(&src[k]);
   }
+  // the chunk's kept rows (event modes): [tile_prefix[t_first], tile_prefix[t_end])
+  const int64_t r0 = gh ? 0 : __ldcg(&a.tile_prefix[t_first]);
+  const int64_t r1 = gh ? 0 : __ldcg(&a.tile_prefix[t_end]);
+  Acc acc{};
+  acc.nonfinite = &sh.nonfinite;
   if (kLarge && tg.G > a.gcap) {
     const DensView d = load_density(a, b, tg.k0, tg.G, true, nullptr, guide_s, nullptr, false,
                                     sh, guide_key);
-    vjp_chunk_tiles<TPB, R, kRO>(a, d, tg, tb, t_first, t_end, nullptr,
-                                 a.gcdf + __ldg(&a.gc_off[b]), gh);
+    acc.gc = a.gcdf + __ldg(&a.gc_off[b]);
+    const bool win = kFixPaths<TPB> && a.win_n > 0 && d.coarse && !d.skip && G - 1 > a.win_n;
+    if (win) {
+      // the window's sums live where small densities keep their records
+      if (sh.win_b != b) large_window<TPB>(a, d, b, sh);
+      uint32_t* base = reinterpret_cast<uint32_t*>(rec_s);
+      for (int i = threadIdx.x; i < 4 * a.win_n; i += TPB) base[i] = 0u;
+      chunk_scale<TPB>(a, gh, r0, r1, sh);
+      acc.alo = base;
+      acc.ahi = base + a.win_n;
+      acc.blo = base + 2 * a.win_n;
+      acc.bhi = base + 3 * a.win_n;
+      acc.scale = sh.fix_scale;
+      acc.win_lo = sh.win_lo;
+      acc.win_n = a.win_n;
+    }
+    vjp_chunk_tiles<TPB, R, kRO, false>(a, d, tg, tb, t_first, t_end, acc, gh);
+    if (win) {
+      __syncthreads();
+      const double inv_scale = 1.0 / static_cast<double>(acc.scale);
+      if (sh.nonfinite) {
+        if (threadIdx.x == 0) red_add_f32x2(&acc.gc[acc.win_lo], __int_as_float(0x7fc00000), 0.0f);
+      } else {
+        for (int i = threadIdx.x; i < a.win_n; i += TPB) {
+          if ((acc.alo[i] | acc.ahi[i] | acc.blo[i] | acc.bhi[i]) == 0u) continue;
+          const int j = acc.win_lo + i;
+          const double A = fix_value(acc.alo[i], acc.ahi[i], inv_scale);
+          const double Bs = fix_value(acc.blo[i], acc.bhi[i], inv_scale);
+          const double m = static_cast<double>(__ldg(reinterpret_cast<const float*>(d.rec + j) + 3));
+          red_add_f32x2(&acc.gc[j], static_cast<float>(m * (Bs - A)), static_cast<float>(-m * Bs));
+        }
+      }
+    }
     // the density's grad-CDF atomics are performed before the chunk counts
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
     return;
   }
-  // The chunk's grad-CDF is replicated `rep` times in the shared slot sized
-  // for the largest density (copy c at c * (G + 1): copies of one knot fall
-  // in different banks); lane l adds into copy l % rep, so lanes whose events
-  // share an interval (small, peaked densities) rarely collide.
+  float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;
+  // fp32 sums, replicated `rep` times in the shared slot sized for the
+  // largest density (copy c at c * (G + 1): copies of one knot fall in
+  // different banks); lane l adds into copy l % rep, so lanes whose events
+  // share an interval (small, peaked densities) rarely collide
   int rep = 1;
   while (rep < 32 && 2 * rep * (G + 1) <= a.gcap) rep *= 2;
-  const int stride = rep > 1 ? G + 1 : G;  // rep * stride <= gcap
-  for (int i = threadIdx.x; i < rep * stride; i += TPB) gacc_s[i] = 0.0f;
-  const DensView d = load_density(a, b, tg.k0, tg.G, false, rec_s, guide_s, invd_s, false, sh,
-                                  guide_key);
-  float* gacc_lane = gacc_s + ((threadIdx.x & 31) & (rep - 1)) * stride;
-  vjp_chunk_tiles<TPB, R, kShared>(a, d, tg, tb, t_first, t_end, gacc_lane, nullptr, gh);
-  __syncthreads();
-  float* part = a.partials + __ldg(&a.part_off[b]) + static_cast<int64_t>(ki) * G;
-  for (int i = threadIdx.x; i < G; i += TPB) {
-    float v = gacc_s[i];
-    for (int c = 1; c < rep; ++c) v += gacc_s[c * stride + i];
-    __stcg(&part[i], v);
+  // Fixed-point sums instead where one fp32 copy would be shared by every
+  // lane, the density has at most 4096 knots (larger ones measured slower in
+  // fixed point) and its records, weights and sums (36 bytes per knot) fit
+  // the slot before the guide: records at 0, weights at 16 G, sums A, B at
+  // 20 G bytes.
+  if (kFix && kFixPaths<TPB> && rep == 1 && G <= 4096 && 36ll * G <= 4ll * a.bwd_guide_off) {
+    float4* rec_f = rec_s;
+    float* invd_f = reinterpret_cast<float*>(rec_s + G);
+    uint32_t* base = reinterpret_cast<uint32_t*>(invd_f + G);
+    const DensView d = load_density(a, b, tg.k0, tg.G, false, rec_f, guide_s, invd_f, false, sh,
+                                    guide_key);
+    if (d.count_all) {
+      // count semantics: intervals and offsets are not bounded, fp32 sums
+      float* gacc = reinterpret_cast<float*>(base);
+      for (int i = threadIdx.x; i < G; i += TPB) gacc[i] = 0.0f;
+      __syncthreads();
+      acc.gacc = gacc;
+      vjp_chunk_tiles<TPB, R, kShared, false>(a, d, tg, tb, t_first, t_end, acc, gh);
+      __syncthreads();
+      for (int i = threadIdx.x; i < G; i += TPB) __stcg(&part[i], gacc[i]);
+    } else {
+      for (int i = threadIdx.x; i < 4 * G; i += TPB) base[i] = 0u;
+      chunk_scale<TPB>(a, gh, r0, r1, sh);
+      acc.alo = base;
+      acc.ahi = base + G;
+      acc.blo = base + 2 * G;
+      acc.bhi = base + 3 * G;
+      acc.scale = sh.fix_scale;
+      vjp_chunk_tiles<TPB, R, kShared, true>(a, d, tg, tb, t_first, t_end, acc, gh);
+      __syncthreads();
+      const double inv_scale = 1.0 / static_cast<double>(acc.scale);
+      const bool bad = sh.nonfinite != 0;
+      for (int i = threadIdx.x; i < G; i += TPB) {
+        // gcdf_i = m_i (B_i - A_i) - m_{i-1} B_{i-1} (no interval starts at knot G-1)
+        double v = 0.0;
+        if (i + 1 < G)
+          v = static_cast<double>(rec_f[i].w) * (fix_value(acc.blo[i], acc.bhi[i], inv_scale) -
+                                                  fix_value(acc.alo[i], acc.ahi[i], inv_scale));
+        if (i > 0)
+          v -= static_cast<double>(rec_f[i - 1].w) *
+               fix_value(acc.blo[i - 1], acc.bhi[i - 1], inv_scale);
+        __stcg(&part[i], bad ? __int_as_float(0x7fc00000) : static_cast<float>(v));
+      }
+    }
+  } else {
+    const DensView d = load_density(a, b, tg.k0, tg.G, false, rec_s, guide_s, invd_s, false, sh,
+                                    guide_key);
+    const int stride = rep > 1 ? G + 1 : G;  // rep * stride <= gcap
+    for (int i = threadIdx.x; i < rep * stride; i += TPB) gacc_s[i] = 0.0f;
+    __syncthreads();
+    acc.gacc = gacc_s + ((threadIdx.x & 31) & (rep - 1)) * stride;
+    vjp_chunk_tiles<TPB, R, kShared, false>(a, d, tg, tb, t_first, t_end, acc, gh);
+    __syncthreads();
+    for (int i = threadIdx.x; i < G; i += TPB) {
+      float v = gacc_s[i];
+      for (int c = 1; c < rep; ++c) v += gacc_s[c * stride + i];
+      __stcg(&part[i], v);
+    }
   }
   __threadfence();
   __syncthreads();
@@ -1652,20 +1902,23 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
   }
 }
 
-template <int TPB, int R, bool kLarge>
+template <int TPB, int R, bool kLarge, bool kFix>
 __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchArgs a, double* grho) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
   float* invd_s = reinterpret_cast<float*>(rec_s + a.gcap);
   float* gacc_s = invd_s + a.gcap;
-  uint32_t* guide_s = reinterpret_cast<uint32_t*>(gacc_s + a.gcap);
+  uint32_t* guide_s = reinterpret_cast<uint32_t*>(smem_raw) + a.bwd_guide_off;
   __shared__ union {
     FinShared<TPB> fin;
     SampleShared smp;
   } sh;
   __shared__ uint32_t s_item;
   __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
-  if (threadIdx.x == 0) s_guide_key = -1;
+  if (threadIdx.x == 0) {
+    s_guide_key = -1;
+    sh.smp.win_b = -1;  // no fixed-point window chosen yet
+  }
   const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo, nL = a.l_hi - a.l_lo;
   const uint32_t n_items = static_cast<uint32_t>(nK + nD + 2 * nL);
   while (true) {
@@ -1675,7 +1928,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     __syncthreads();
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nK)) {
-      vjp_chunk_item<TPB, R, kLarge>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s,
+      vjp_chunk_item<TPB, R, kLarge, kFix>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s,
                                      invd_s, gacc_s, sh.smp, s_guide_key);
     } else if (item < static_cast<uint32_t>(nK + nD)) {
       vjp_finalize_item<TPB>(a, a.d_lo + static_cast<int32_t>(item) - nK, grho, sh.fin);

@@ -15,7 +15,7 @@
 namespace loits_dev {
 template <int TPB, int R, bool kLarge>
 __global__ void batch_forward_kernel(BatchArgs a);
-template <int TPB, int R, bool kLarge>
+template <int TPB, int R, bool kLarge, bool kFix>
 __global__ void batch_backward_kernel(BatchArgs a, double* grho);
 __global__ void batch_cdf_export_kernel(const float4* rec, int64_t n, double* cdf);
 __global__ void batch_quantile_kernel(const float4* rec, const uint32_t* guide, int m, int G,
@@ -51,6 +51,9 @@ struct loits_batch_plan {
   int32_t n_tiles = 0, n_cdf = 0, n_fin = 0, n_chunks = 0, last_nonempty = -1;
   int32_t gcap = 0, mcap = 0, tiles_per_chunk = 1, n_lfin = 0, m_cap_b = 2;
   int32_t lbits_f = 0, lbits_b = 0;  // coarse large-density guide bits in shared memory
+  bool fix_small = false;             // backward slot sized for fixed-point sums of gcap knots
+  bool fix_used = false;              // backward variant with the fixed-point small path
+  int32_t win_n = 0, bwd_guide_off = 0;  // backward: large-density window, guide offset
   bool has_large = false;  // densities above the shared-memory limit
   int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
@@ -77,38 +80,42 @@ using FwdKernel = void (*)(BatchArgs);
 using BwdKernel = void (*)(BatchArgs, double*);
 
 template <int TPB, int R>
-void pick(bool large, FwdKernel& f, BwdKernel& b) {
+void pick(bool large, bool fix, FwdKernel& f, BwdKernel& b) {
+  constexpr bool kFixOK = TPB >= 512;  // fixed-point paths: 512- and 1024-thread CTAs
   if (large) {
     f = batch_forward_kernel<TPB, R, true>;
-    b = batch_backward_kernel<TPB, R, true>;
+    b = batch_backward_kernel<TPB, R, true, false>;
+    if constexpr (kFixOK) if (fix) b = batch_backward_kernel<TPB, R, true, true>;
   } else {
     f = batch_forward_kernel<TPB, R, false>;
-    b = batch_backward_kernel<TPB, R, false>;
+    b = batch_backward_kernel<TPB, R, false, false>;
+    if constexpr (kFixOK) if (fix) b = batch_backward_kernel<TPB, R, false, true>;
   }
 }
 
 // Kernels of a launch geometry; `large`: the plan has densities above the
-// shared-memory limit.
-bool kernels_for(int tpb, int r, bool large, FwdKernel& f, BwdKernel& b) {
+// shared-memory limit; `fix`: small densities that sum in fixed point (the
+// backward variant with that path; 512- and 1024-thread CTAs).
+bool kernels_for(int tpb, int r, bool large, FwdKernel& f, BwdKernel& b, bool fix = false) {
   if (tpb == 256) {
     switch (r) {
-      case 2: pick<256, 2>(large, f, b); return true;
-      case 4: pick<256, 4>(large, f, b); return true;
-      case 8: pick<256, 8>(large, f, b); return true;
-      case 16: pick<256, 16>(large, f, b); return true;
+      case 2: pick<256, 2>(large, fix, f, b); return true;
+      case 4: pick<256, 4>(large, fix, f, b); return true;
+      case 8: pick<256, 8>(large, fix, f, b); return true;
+      case 16: pick<256, 16>(large, fix, f, b); return true;
     }
   } else if (tpb == 512) {
     switch (r) {
-      case 2: pick<512, 2>(large, f, b); return true;
-      case 4: pick<512, 4>(large, f, b); return true;
-      case 8: pick<512, 8>(large, f, b); return true;
-      case 16: pick<512, 16>(large, f, b); return true;
+      case 2: pick<512, 2>(large, fix, f, b); return true;
+      case 4: pick<512, 4>(large, fix, f, b); return true;
+      case 8: pick<512, 8>(large, fix, f, b); return true;
+      case 16: pick<512, 16>(large, fix, f, b); return true;
     }
   } else if (tpb == 1024) {
     switch (r) {
-      case 2: pick<1024, 2>(large, f, b); return true;
-      case 4: pick<1024, 4>(large, f, b); return true;
-      case 8: pick<1024, 8>(large, f, b); return true;
+      case 2: pick<1024, 2>(large, fix, f, b); return true;
+      case 4: pick<1024, 4>(large, fix, f, b); return true;
+      case 8: pick<1024, 8>(large, fix, f, b); return true;
     }
   }
   return false;
@@ -167,6 +174,9 @@ struct SmemGeometry {
   int m_cap_b = 2;  // backward: the same beside records, weights and gradients
   int lbits_f = 0;  // large densities: log2 of the coarse guide a forward CTA holds
   int lbits_b = 0;  // ... and a backward CTA
+  bool fix_small = false;   // backward slot sized for fixed-point sums of gcap knots
+  int32_t win_n = 0;        // backward: large densities' fixed-point window (intervals)
+  int32_t bwd_guide_off = 0;  // backward: uint32 words before the guide
   int32_t mcap = 0;
   size_t static_smem = 0, fwd = 0, bwd = 0;
 };
@@ -217,36 +227,70 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
   const int32_t mcap_b = std::min<int32_t>(g.mcap, int32_t(1) << g.m_cap_b);
   // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
   // kept events are staged in global memory, not here
-  size_t guide_f = static_cast<size_t>((g.mcap + 7) & ~7) * sizeof(uint32_t);
-  size_t guide_b = static_cast<size_t>((mcap_b + 7) & ~7) * sizeof(uint32_t);
+  auto gbytes = [](int32_t entries) { return static_cast<size_t>((entries + 7) & ~7) * sizeof(uint32_t); };
+  const size_t guide_f = gbytes(g.mcap);
+  size_t guide_b = gbytes(mcap_b);
+  // CTAs per SM that `bytes` of dynamic shared memory allow (at most the
+  // register cap's 1280 / tpb)
+  auto resident = [&](size_t bytes) {
+    size_t c = static_cast<size_t>(std::max(1, 1280 / tpb));
+    while (c > 1 && c * (bytes + g.static_smem + kSmemPerCtaReserved) > kSmemPerSM) --c;
+    return c;
+  };
+  // Backward small-density slot: records, weights and either fp32 grad-CDF
+  // sums (4 bytes per knot) or the fixed-point sums A, B (16 bytes per
+  // knot).  Fixed point is used when it costs neither residency nor guide
+  // resolution (a coarser backward guide measured slower than the fp32 sums).
+  size_t small_b = bwd_knots;
+  {
+    const size_t fix_knots = static_cast<size_t>(gcap) * (sizeof(float4) + 5 * sizeof(float));
+    if (tpb >= 512 && fix_knots + guide_b + g.static_smem + 16 * 1024 <= kSmemLimit &&
+        resident(fix_knots + guide_b) >= resident(bwd_knots + guide_b)) {
+      g.fix_small = true;
+      small_b = fix_knots;
+    }
+  }
+  size_t before_guide = small_b;
   if (large) {
     // backward CTAs of large densities (records in global memory) read a
     // coarse copy of the guide (every 2^s-th count, 2^lbits + 1 uint32) from
-    // shared memory, sized not to lower the residency the register cap
-    // allows and to leave room for a histogram-mode cotangent (16 KB); the
-    // forward reads the full guide through L2 (lbits_f = 0), which measured
-    // faster than the coarser buckets' longer searches
+    // shared memory and sum the most probable run of intervals (the window)
+    // in fixed point where small densities keep their records; both sized
+    // not to lower the residency the register cap allows and to leave room
+    // for a histogram-mode cotangent (16 KB).  The forward reads the full
+    // guide through L2 (lbits_f = 0), which measured faster than the coarser
+    // buckets' longer searches.
     auto bytes = [](int b) { return ((size_t(1) << b) + 1 + 7) / 8 * 8 * sizeof(uint32_t); };
-    size_t ctas = static_cast<size_t>(std::max(1, 1280 / tpb));
-    while (ctas > 1 && ctas * (bwd_knots + g.static_smem + bytes(6) + kSmemPerCtaReserved) > kSmemPerSM)
-      --ctas;
-    const size_t per_cta = kSmemPerSM / ctas - kSmemPerCtaReserved;
+    const size_t ctas = resident(small_b + bytes(6));
+    const size_t per_cta = std::min(kSmemPerSM / ctas - kSmemPerCtaReserved, kSmemLimit);
+    const size_t avail = per_cta > g.static_smem + 16 * 1024 ? per_cta - g.static_smem - 16 * 1024 : 0;
+    size_t win_bytes = std::min<size_t>(8192 * 16, avail / 2) / 4096 * 4096;
+    if (win_bytes < 1024 * 16 || tpb < 512) win_bytes = 0;  // the kernels' fixed-point paths
+    const size_t region = std::max(small_b, win_bytes);
     int lb = kMaxLargeGuideBits;
-    while (lb > 6 && (bwd_knots + bytes(lb) + g.static_smem > per_cta ||
-                      bwd_knots + bytes(lb) + g.static_smem + 16 * 1024 > kSmemLimit))
-      --lb;
+    while (lb > 6 && region + bytes(lb) > avail) --lb;
     g.lbits_f = 0;
     // a copy more than 16 times coarser than the largest guide costs more
     // search steps than it saves: the full guide is read in place instead
+    // (and the window, found on the coarse copy, is not used)
     g.lbits_b = lb >= guide_bits(large_g, kMaxLargeGuideBits) - 4 ? lb : 0;
-    if (g.lbits_b > 0) guide_b = std::max(guide_b, bytes(lb));
+    if (g.lbits_b > 0) {
+      guide_b = std::max(guide_b, bytes(lb));
+      g.win_n = static_cast<int32_t>(win_bytes / 16);
+      before_guide = region;
+    }
   }
+  g.bwd_guide_off = static_cast<int32_t>((before_guide / sizeof(uint32_t) + 3) & ~size_t(3));
   g.fwd = fwd_knots + guide_f;
-  g.bwd = bwd_knots + guide_b;
+  g.bwd = static_cast<size_t>(g.bwd_guide_off) * sizeof(uint32_t) + guide_b;
   if (g.fwd + g.static_smem > kSmemLimit || g.bwd + g.static_smem > kSmemLimit)
     return LOITS_ERR_UNSUPPORTED;
+  FwdKernel fk2;
+  BwdKernel bk_fix;
+  kernels_for(tpb, r, large, fk2, bk_fix, true);
   if (!allow_dynamic_smem(reinterpret_cast<const void*>(fk), g.fwd) ||
-      !allow_dynamic_smem(reinterpret_cast<const void*>(bk), g.bwd))
+      !allow_dynamic_smem(reinterpret_cast<const void*>(bk), g.bwd) ||
+      !allow_dynamic_smem(reinterpret_cast<const void*>(bk_fix), g.bwd))
     return LOITS_ERR_CUDA;
   return LOITS_OK;
 }
@@ -484,6 +528,19 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->m_cap_b = sg.m_cap_b;
   p->lbits_f = sg.lbits_f;
   p->lbits_b = sg.lbits_b;
+  p->fix_small = sg.fix_small;
+  p->win_n = sg.win_n;
+  p->bwd_guide_off = sg.bwd_guide_off;
+  // the backward variant with fixed-point sums, when some small density
+  // takes that path (one fp32 copy of its sums per CTA, at most 4096 knots,
+  // its 36 bytes per knot within the slot; see vjp_chunk_item)
+  if (p->tpb >= 512) {
+    for (int64_t b = 0; b < n_densities && !p->fix_used; ++b) {
+      const int64_t g = p->koff[b + 1] - p->koff[b];
+      p->fix_used = g <= p->gcap && 2 * (g + 1) > p->gcap && g <= 4096 &&
+                    36 * g <= 4 * static_cast<int64_t>(p->bwd_guide_off);
+    }
+  }
   p->fwd_smem = sg.fwd;
   p->fwd_smem_allowed = sg.fwd;
   p->bwd_smem_allowed = sg.bwd;
@@ -681,10 +738,12 @@ int launch_backward(const loits_batch_plan* p, BatchArgs& a, void* workspace, si
     return LOITS_ERR_CUDA;
   a.gbits_cap = p->m_cap_b;
   a.lguide_bits = p->lbits_b;
+  a.win_n = p->win_n;
+  a.bwd_guide_off = p->bwd_guide_off;
   double* grho = carve<double>(workspace, L.grho);
   FwdKernel fk;
   BwdKernel bk;
-  kernels_for(p->tpb, p->r, p->has_large, fk, bk);
+  kernels_for(p->tpb, p->r, p->has_large, fk, bk, p->fix_used);
   if (smem > p->bwd_smem_allowed) {
     if (!allow_dynamic_smem(reinterpret_cast<const void*>(bk), smem)) return LOITS_ERR_CUDA;
     p->bwd_smem_allowed = smem;
