@@ -123,9 +123,10 @@ def test_cdf_matches_fp64_oracle(B, golden, oracle_lib):
         np.testing.assert_allclose(norm.cpu().numpy(), onorm, rtol=1e-12)
 
 
-# The backward accumulates each chunk's grad-CDF with fp32 shared-memory
-# atomics, whose order varies from run to run: gradients are reproducible to
-# fp32 accumulation rounding, events and row offsets bit for bit.
+# The backward accumulates each chunk's grad-CDF with fp32 atomics, whose
+# order varies from run to run, or with order-independent fixed-point sums:
+# gradients are reproducible to fp32 accumulation rounding, events and row
+# offsets bit for bit.
 GRAD_REPRO = 1e-6
 
 
@@ -535,3 +536,66 @@ def test_precision_workload_shape_matches_oracle(B, oracle_lib):
         xo, jo = oracle_lib.d_quantile(b, spec.knot_offsets, spec.grid, ref["cdf"],
                                        p.astype(np.float64))
         np.testing.assert_allclose(x.cpu().numpy(), xo, rtol=EVENT_RTOL)
+
+
+def _fixed_point_case(n_dens=6, knots=1024, events=60_000):
+    """Densities whose backward sums run in fixed point on 512/1024-thread
+    CTAs (one fp32 copy of the sums would fill the slot: G = gcap <= 4096)."""
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.uniform(scale=events / 1e6, n_densities=n_dens, knots=knots)
+    return dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, scalars=np.array([spec.seed, 2]))
+
+
+@pytest.mark.parametrize("threads", [512, 1024])
+def test_fixed_point_backward_is_bit_reproducible(B, oracle_lib, threads):
+    """Integer sums do not depend on the order of the atomics: two backward
+    runs give bit-identical gradients, within 1e-4 of the oracle's."""
+    case = _fixed_point_case()
+    koff, counts = case["knot_offsets"], case["event_counts"]
+    eoff = np.concatenate([[0], np.cumsum(counts)])
+    seed, seq = int(case["scalars"][0]), int(case["scalars"][1])
+    ref = oracle_lib.d_forward(koff, eoff, case["grid"], case["values"], None, seed, seq)
+    case["cotangent"] = np.random.default_rng(3).standard_normal(len(ref["events"])).astype(np.float32)
+    out = run_batch(B, case, B.make_config(threads=threads), with_intervals=False)
+    plan, ws = out["plan"], out["ws"]
+    g = torch.zeros(max(plan.capacity, 4), dtype=torch.float32, device=DEV)
+    g[:out["valid"]] = torch.from_numpy(case["cotangent"]).to(DEV)
+    again = torch.empty_like(out["values"])
+    plan.backward(out["grid"], out["values"], None, out["seed"], out["seq"], g, again, ws)
+    plan.check_status(ws)
+    assert np.array_equal(again.cpu().numpy(), out["grad_values"])
+    gref = oracle_lib.d_backward(koff, eoff, case["grid"], case["values"], None, seed, seq,
+                                 case["cotangent"], fwd=ref)
+    for b in range(len(counts)):
+        o, e = koff[b], koff[b + 1]
+        scale = np.abs(gref[o:e]).max()
+        assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b
+
+
+@pytest.mark.parametrize("threads", [256, 512])
+def test_non_finite_cotangent_poisons_only_its_density(B, threads):
+    """A NaN cotangent makes its density's gradient non-finite (the
+    normaliser VJP sums over every knot, as in the reference); the other
+    densities' gradients are unchanged."""
+    case = _fixed_point_case(n_dens=4, events=20_000)
+    out = run_batch(B, case, B.make_config(threads=threads), with_intervals=False)
+    plan, ws = out["plan"], out["ws"]
+    rows = out["rows"]
+    g = torch.zeros(max(plan.capacity, 4), dtype=torch.float32, device=DEV)
+    g[:out["valid"]] = torch.randn(out["valid"], generator=torch.Generator(device=DEV).manual_seed(9),
+                                   device=DEV)
+    clean = torch.empty_like(out["values"])
+    plan.backward(out["grid"], out["values"], None, out["seed"], out["seq"], g, clean, ws)
+    g[int(rows[1]) + 17] = float("nan")
+    dirty = torch.empty_like(out["values"])
+    plan.backward(out["grid"], out["values"], None, out["seed"], out["seq"], g, dirty, ws)
+    plan.check_status(ws)
+    koff = case["knot_offsets"]
+    c, d = clean.cpu().numpy(), dirty.cpu().numpy()
+    assert not np.isfinite(d[koff[1]:koff[2]]).any()
+    for b in (0, 2, 3):
+        o, e = koff[b], koff[b + 1]
+        assert np.isfinite(d[o:e]).all()
+        np.testing.assert_allclose(d[o:e], c[o:e], rtol=1e-5, atol=1e-6 * np.abs(c[o:e]).max())
