@@ -59,6 +59,9 @@ struct BatchArgs {
   int32_t gbits_cap;           // most guide bits this launch copies to shared memory
   int32_t lguide_bits;         // large densities: bits of the coarse guide in shared memory
   int32_t win_n;               // backward: large densities' fixed-point window (intervals, 0: none)
+  int32_t fwin_n;              // forward: large densities' window of records in shared memory
+  int32_t fwd_guide_off;       // forward: uint32 words from the start of dynamic shared
+                               // memory to the guide
   int32_t bwd_guide_off;       // backward: uint32 words from the start of dynamic shared
                                // memory to the guide
                                // (a larger guide is read every 2^s-th count)

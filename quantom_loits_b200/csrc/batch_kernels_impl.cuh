@@ -547,7 +547,11 @@ struct DensView {
   bool accept_all;
   bool threshold;         // kept = uniforms above one threshold (kThreshold)
   bool skip;              // large density whose CDF is not non-decreasing: not sampled
-  bool coarse;            // large: search from cguide (shift covers its bits)
+  bool coarse;            // large: cguide in shared memory (shift covers its bits)
+  bool fresh;             // large: the coarse guide was copied for this view
+  int shift_full;         // large: 32 - bits of the full guide
+  const float4* wrec;     // forward, large: records [wk0, wk1) in shared memory
+  int wk0, wk1;
   float cut;
 };
 
@@ -561,6 +565,7 @@ struct SampleShared {
   int nonfinite;     // backward chunk: a non-finite contribution was seen
   int win_b;         // density whose fixed-point window win_lo belongs to
   int win_lo;
+  int run_k0;        // most_probable_run's result
 };
 
 // Wait until density b's CDF is final (thread 0) and share its flags and cut.
@@ -581,9 +586,9 @@ __device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool la
 
 // The density's sampling view: small densities copy their records, packed
 // guide and (backward) weights into shared memory; large densities keep
-// records and weights in global memory and read their guide in place
-// (forward: lguide_bits == 0) or copy a coarse guide (backward).  Ends with
-// a barrier.  guide_key (shared) names the density whose coarse guide
+// records and weights in global memory and copy a coarse guide when
+// lguide_bits > 0 (the forward adds a window of records: sample_item).  Ends
+// with a barrier.  guide_key (shared) names the density whose coarse guide
 // guide_s holds, so a CTA's consecutive items on one large density copy it
 // once.
 __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int64_t k0, int64_t G,
@@ -599,7 +604,8 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
     v.rec = a.rec + k0;
     v.invd = a.invd + k0;
     const uint32_t* L = a.gl + __ldg(&a.goff[b]);
-    if (coarse && !nonmono && guide_key != b) {
+    v.fresh = coarse && !nonmono && guide_key != b;
+    if (v.fresh) {
       // every 2^s-th count of the guide (the guide with 2^s-times wider
       // buckets), 2^m + 1 uint32
       const int sft = m_full - m;
@@ -627,12 +633,16 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
     v.guide = guide_s;
     v.cguide = guide_s;
     v.invd = invd_s;
+    v.fresh = false;
   }
   __syncthreads();
   // every thread has read guide_key above; the next read follows the item
   // loop's barriers
   if (threadIdx.x == 0) guide_key = large ? (nonmono || !coarse ? guide_key : b) : -1;
   v.shift = 32 - m;
+  v.shift_full = 32 - m_full;
+  v.wrec = nullptr;
+  v.wk0 = v.wk1 = 0;
   v.G = static_cast<int>(G);
   v.count_all = nonmono && !large;
   v.accept_all = (sh.flags & kAcceptAll) != 0;
@@ -660,6 +670,34 @@ struct Slot {
   bool ok;
 };
 
+// Interval of u whose count #{t : u >= c_t} lies in [lo, hi] (a guide
+// bucket; c_0 = 0, so lo >= 1): both candidate records are loaded at once --
+// interval lo-1 (count == lo) and knot/interval lo (count > lo) -- and one
+// exact compare selects, without a branch.  Only a bucket holding several
+// knots needs a search.  Reads record indices lo-1 .. hi only.
+template <int kMode>
+__device__ __forceinline__ void pick_interval(const float4* rec, int G, float u, int lo, int hi,
+                                              int& j, float4& r) {
+  const int ja = max(min(lo - 1, G - 2), 0);
+  const float4 ra = rec_at<kMode>(rec, ja);
+  const float4 rb = rec_at<kMode>(rec, ja + 1);
+  const bool step = (lo < hi) & (u >= rb.x);
+  // count == lo + 1 moves to interval lo, unless lo - 1 is the last one
+  const bool adv = step & (lo <= G - 2);
+  j = ja + (adv ? 1 : 0);
+  r = adv ? rb : ra;
+  if (step & (hi - lo >= 2)) {
+    // count in [lo + 1, hi]: first key above u
+    int l = lo + 1, h = hi;
+    while (l < h) {
+      const int mid = (l + h) >> 1;
+      if (u >= key_at<kMode>(rec, mid)) l = mid + 1; else h = mid;
+    }
+    j = min(l - 1, G - 2);
+    r = rec_at<kMode>(rec, j);
+  }
+}
+
 template <int kMode>
 __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
   const float u = uniform_from_bits(bits);
@@ -668,48 +706,44 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
   if (kMode == kShared && d.count_all) {
     j = interval_count_all(d.rec, u, d.G);
     r = d.rec[j];
+  } else if constexpr (kMode == kShared) {
+    const uint32_t pk = d.guide[bits >> d.shift];
+    pick_interval<kShared>(d.rec, d.G, u, static_cast<int>(pk & 0xffffu),
+                           static_cast<int>(pk >> 16), j, r);
+  } else if constexpr (kMode == kL2) {
+    // forward, large density: when the coarse bucket's knots all lie in the
+    // shared window [wk0, wk1), search there; otherwise the full guide and
+    // records through L2 (written earlier in this launch)
+    bool hot = false;
+    if (d.coarse) {
+      const uint32_t kc = bits >> d.shift;
+      const int lo = static_cast<int>(d.cguide[kc]), hi = static_cast<int>(d.cguide[kc + 1]);
+      hot = lo > d.wk0 && hi < d.wk1;
+      if (hot) {
+        // window coordinates (knot index - wk0): the clamps to [0, G-2] do
+        // not bind inside the window, so the pick is the same
+        pick_interval<kShared>(d.wrec, d.G - d.wk0, u, lo - d.wk0, hi - d.wk0, j, r);
+        j += d.wk0;
+      }
+    }
+    if (!hot) {
+      const uint32_t k = bits >> d.shift_full;
+      pick_interval<kL2>(d.rec, d.G, u, static_cast<int>(__ldcg(d.guide + k)),
+                         static_cast<int>(__ldcg(d.guide + k + 1)), j, r);
+    }
   } else {
-    // count = #{t : u >= c_t} lies in [lo, hi] (guide bucket of u); c_0 = 0,
-    // so lo >= 1.  Both candidate records are loaded at once: interval lo-1
-    // (count == lo) and knot/interval lo (count > lo); one exact compare
-    // selects, without a branch.  Only a bucket holding several knots needs
-    // a search.
+    // backward, large density: the coarse guide in shared memory, or the
+    // full guide through the read-only cache
     const uint32_t k = bits >> d.shift;
     int lo, hi;
-    if constexpr (kMode == kShared) {
-      const uint32_t pk = d.guide[k];
-      lo = static_cast<int>(pk & 0xffffu);
-      hi = static_cast<int>(pk >> 16);
-    } else if constexpr (kMode == kL2) {
-      // the full guide in global memory (written earlier in this launch)
-      lo = static_cast<int>(__ldcg(d.guide + k));
-      hi = static_cast<int>(__ldcg(d.guide + k + 1));
-    } else if (d.coarse) {
-      // the coarse guide in shared memory
+    if (d.coarse) {
       lo = static_cast<int>(d.cguide[k]);
       hi = static_cast<int>(d.cguide[k + 1]);
     } else {
       lo = static_cast<int>(__ldg(d.guide + k));
       hi = static_cast<int>(__ldg(d.guide + k + 1));
     }
-    const int ja = max(min(lo - 1, d.G - 2), 0);
-    const float4 ra = rec_at<kMode>(d.rec, ja);
-    const float4 rb = rec_at<kMode>(d.rec, ja + 1);
-    const bool step = (lo < hi) & (u >= rb.x);
-    // count == lo + 1 moves to interval lo, unless lo - 1 is the last one
-    const bool adv = step & (lo <= d.G - 2);
-    j = ja + (adv ? 1 : 0);
-    r = adv ? rb : ra;
-    if (step & (hi - lo >= 2)) {
-      // count in [lo + 1, hi]: first key above u
-      int l = lo + 1, h = hi;
-      while (l < h) {
-        const int mid = (l + h) >> 1;
-        if (u >= key_at<kMode>(d.rec, mid)) l = mid + 1; else h = mid;
-      }
-      j = min(l - 1, d.G - 2);
-      r = rec_at<kMode>(d.rec, j);
-    }
+    pick_interval<kRO>(d.rec, d.G, u, lo, hi, j, r);
   }
   Slot o;
   o.x = interval_value(r, u, o.t);
@@ -1129,20 +1163,87 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   __syncthreads();
 }
 
+// The first bucket k0 of the run of coarse-guide buckets [k0, k1] that holds
+// the most uniforms while L[k1] - L[k0] <= room, i.e. whose knots fit a window
+// of room + 1 counts: the density's most probable stretch.  Each thread tries
+// every 4th bucket start (binary search for k1); ties go to the smallest k0.
+// Returns the same k0 on every thread; ends with a barrier.
+template <int TPB>
+__device__ __forceinline__ int most_probable_run(const uint32_t* L, int M, uint32_t room,
+                                                 SampleShared& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  int best_span = -1, best_k0 = 0;
+  for (int k0 = threadIdx.x * 4; k0 < M; k0 += TPB * 4) {
+    const uint32_t lim = L[k0] + room;
+    int lo = k0, hi = M;  // largest k1 in [k0, M] with L[k1] <= lim
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if (L[mid] <= lim) lo = mid; else hi = mid - 1;
+    }
+    if (lo - k0 > best_span) { best_span = lo - k0; best_k0 = k0; }
+  }
+  const int wspan = __reduce_max_sync(0xffffffffu, best_span);
+  const int wk0 = __reduce_min_sync(0xffffffffu, best_span == wspan ? best_k0 : 0x7fffffff);
+  if (lane == 0) { sh.warp_cnt[warp] = wspan; sh.red[warp] = __int_as_float(wk0); }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    int span = -1, k0 = 0;
+    for (int w = 0; w < TPB / 32; ++w) {
+      const int k = __float_as_int(sh.red[w]);
+      if (sh.warp_cnt[w] > span || (sh.warp_cnt[w] == span && k < k0)) {
+        span = sh.warp_cnt[w];
+        k0 = k;
+      }
+    }
+    sh.run_k0 = k0;
+  }
+  __syncthreads();
+  return sh.run_k0;
+}
+
+// Forward, large density with a coarse guide: the window of fwin_n records
+// [wk0, wk1) around its most probable stretch, copied to shared memory (rec_s)
+// when the view is fresh (its coarse guide was just copied: a small density
+// or another large one used the slot since).  Slots whose coarse bucket lies
+// inside the window are searched there (sample_slot).  Ends with a barrier.
+template <int TPB>
+__device__ __forceinline__ void forward_window(const BatchArgs& a, DensView& d, int64_t k0,
+                                               float4* rec_s, int2& win, SampleShared& sh) {
+  if (d.skip) {  // not sampled
+    d.wk0 = d.wk1 = 0;
+    return;
+  }
+  if (d.fresh) {
+    const int W = min(a.fwin_n, d.G);
+    const int M = 1 << (32 - d.shift);
+    // buckets [k0, k1] with L[k1] <= L[k0] + W - 2 hold counts the window
+    // [L[k0] - 1, L[k0] - 1 + W) answers (see sample_slot)
+    const int kb = most_probable_run<TPB>(d.cguide, M, static_cast<uint32_t>(W - 2), sh);
+    const int w0 = max(min(static_cast<int>(d.cguide[kb]) - 1, d.G - W), 0);
+    for (int i = threadIdx.x; i < W; i += TPB) rec_s[i] = __ldcg(&a.rec[k0 + w0 + i]);
+    if (threadIdx.x == 0) win = make_int2(w0, w0 + W);
+    __syncthreads();
+  }
+  d.wrec = rec_s;
+  d.wk0 = win.x;
+  d.wk1 = win.y;
+}
+
 // kLarge: the plan has densities above the shared-memory limit (compiled
 // separately so that plans without them carry none of the global-memory path).
 template <int TPB, int R, bool kLarge>
 __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
                                             uint32_t* guide_s, float* stage, SampleShared& sh,
-                                            int& guide_key) {
+                                            int& guide_key, int2& win) {
   const TileGeom tg = tile_geom<TPB, R>(a, t);
   const bool large = kLarge && tg.G > a.gcap;
   density_flags(a, tg.b, large, true, sh);
   if (a.hist) {
     float* hs = reinterpret_cast<float*>(rec_s) + a.hist_smem_off;
     if (large) {
-      const DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
-                                     guide_key);
+      DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
+                                guide_key);
+      if (d.coarse) forward_window<TPB>(a, d, tg.k0, rec_s, win, sh);
       sample_tile_hist<TPB, R, kL2>(a, tg, d, hs);
     } else {
       const DensView d = density_view(a, tg.b, tg.k0, tg.G, false, rec_s, guide_s, nullptr, sh,
@@ -1161,8 +1262,9 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
   }
   // one view per branch: each sees constant `large` (shared or global loads)
   if (large) {
-    const DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
-                                   guide_key);
+    DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
+                              guide_key);
+    if (d.coarse) forward_window<TPB>(a, d, tg.k0, rec_s, win, sh);
     if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, tg, d, sh.base);
     else if (d.threshold) sample_tile_threshold<TPB, R, kL2>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kL2>(a, t, tg, d, stage, sh);
@@ -1468,42 +1570,17 @@ __device__ __forceinline__ void chunk_scale(const BatchArgs& a, const float* gh,
 }
 
 // The window of a large density's fixed-point sums (into sh.win_lo): the run
-// of win_n intervals that holds the most probability, found on the coarse
-// guide in shared memory (bucket k0 .. k1 of the uniforms maps to intervals
-// L[k0] - 1 .. L[k1] - 1).  Ends with a barrier.
+// of win_n intervals that holds the most probability (buckets k0 .. k1 of
+// the coarse guide map to intervals L[k0] - 1 .. L[k1] - 1).  Ends with a
+// barrier.
 template <int TPB>
 __device__ __forceinline__ void large_window(const BatchArgs& a, const DensView& d, int b,
                                              SampleShared& sh) {
-  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int M = 1 << (32 - d.shift);
-  const uint32_t* L = d.cguide;
-  const uint32_t room = static_cast<uint32_t>(a.win_n - 1);
-  int best_span = -1, best_k0 = 0;
-  for (int k0 = threadIdx.x * 4; k0 < M; k0 += TPB * 4) {
-    const uint32_t lim = L[k0] + room;
-    int lo = k0, hi = M;  // largest k1 in [k0, M] with L[k1] <= lim
-    while (lo < hi) {
-      const int mid = (lo + hi + 1) >> 1;
-      if (L[mid] <= lim) lo = mid; else hi = mid - 1;
-    }
-    if (lo - k0 > best_span) { best_span = lo - k0; best_k0 = k0; }
-  }
-  const int wspan = __reduce_max_sync(0xffffffffu, best_span);
-  const int wk0 = __reduce_min_sync(0xffffffffu, best_span == wspan ? best_k0 : 0x7fffffff);
-  if (lane == 0) { sh.warp_cnt[warp] = wspan; sh.red[warp] = __int_as_float(wk0); }
-  __syncthreads();
+  const int k0 = most_probable_run<TPB>(d.cguide, M, static_cast<uint32_t>(a.win_n - 1), sh);
   if (threadIdx.x == 0) {
-    int span = -1, k0 = 0;
-    for (int w = 0; w < TPB / 32; ++w) {
-      const int k = __float_as_int(sh.red[w]);
-      if (sh.warp_cnt[w] > span || (sh.warp_cnt[w] == span && k < k0)) {
-        span = sh.warp_cnt[w];
-        k0 = k;
-      }
-    }
     const int n_int = d.G - 1;  // intervals of the density
-    int lo = static_cast<int>(L[k0]) - 1;
-    lo = min(lo, n_int - a.win_n);
+    const int lo = min(static_cast<int>(d.cguide[k0]) - 1, n_int - a.win_n);
     sh.win_lo = max(lo, 0);
     sh.win_b = b;
   }
@@ -1872,7 +1949,7 @@ template <int TPB, int R, bool kLarge>
 __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArgs a) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
-  uint32_t* guide_s = reinterpret_cast<uint32_t*>(rec_s + a.gcap);
+  uint32_t* guide_s = reinterpret_cast<uint32_t*>(smem_raw) + a.fwd_guide_off;
   // this CTA's staging run in global memory (TPB * R * 4 floats): kept
   // events wait there for their tile's row base; they stay in L2
   float* stage = a.stage_g + static_cast<int64_t>(blockIdx.x) * (TPB * R * 4);
@@ -1882,6 +1959,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
   } sh;
   __shared__ uint32_t s_item;
   __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
+  __shared__ int2 s_win;       // ... and its window of records in rec_s
   if (threadIdx.x == 0) s_guide_key = -1;
   const int32_t nC = a.c_hi - a.c_lo, nF = a.f_hi - a.f_lo, nT = a.t_hi - a.t_lo;
   const uint32_t n_items = static_cast<uint32_t>(nC + nF + nT);
@@ -1897,7 +1975,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
       cdf_finalize_item<TPB>(a, a.f_lo + static_cast<int32_t>(item) - nC, sh.cdf);
     } else {
       sample_item<TPB, R, kLarge>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s,
-                                  guide_s, stage, sh.smp, s_guide_key);
+                                  guide_s, stage, sh.smp, s_guide_key, s_win);
     }
   }
 }

@@ -54,6 +54,7 @@ struct loits_batch_plan {
   bool fix_small = false;             // backward slot sized for fixed-point sums of gcap knots
   bool fix_used = false;              // backward variant with the fixed-point small path
   int32_t win_n = 0, bwd_guide_off = 0;  // backward: large-density window, guide offset
+  int32_t fwin_n = 0, fwd_guide_off = 0;  // forward: large-density window, guide offset
   bool has_large = false;  // densities above the shared-memory limit
   int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
@@ -177,6 +178,8 @@ struct SmemGeometry {
   bool fix_small = false;   // backward slot sized for fixed-point sums of gcap knots
   int32_t win_n = 0;        // backward: large densities' fixed-point window (intervals)
   int32_t bwd_guide_off = 0;  // backward: uint32 words before the guide
+  int32_t fwin_n = 0;       // forward: large densities' window of records
+  int32_t fwd_guide_off = 0;  // forward: uint32 words before the guide
   int32_t mcap = 0;
   size_t static_smem = 0, fwd = 0, bwd = 0;
 };
@@ -281,7 +284,31 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
     }
   }
   g.bwd_guide_off = static_cast<int32_t>((before_guide / sizeof(uint32_t) + 3) & ~size_t(3));
-  g.fwd = fwd_knots + guide_f;
+  // Forward CTAs of large densities (512/1024 threads): a coarse guide (at
+  // most 2^14 buckets) and a window of up to 8192 records around the
+  // density's most probable stretch in shared memory, where the slots that
+  // fall in it are searched; the rest use the full guide through L2.  Sized
+  // not to lower the residency the register cap allows, with room for a
+  // histogram-mode tile (16 KB).
+  size_t fwd_region = fwd_knots, guide_fl = guide_f;
+  if (large && tpb >= 512) {
+    auto bytes = [](int b) { return ((size_t(1) << b) + 1 + 7) / 8 * 8 * sizeof(uint32_t); };
+    const size_t ctas = resident(fwd_knots + guide_f);
+    const size_t per_cta = std::min(kSmemPerSM / ctas - kSmemPerCtaReserved, kSmemLimit);
+    const size_t avail = per_cta > g.static_smem + 16 * 1024 ? per_cta - g.static_smem - 16 * 1024 : 0;
+    int lb = 14;
+    while (lb > 6 && bytes(lb) * 3 > avail) --lb;
+    const size_t rest = avail > bytes(lb) ? avail - bytes(lb) : 0;
+    const size_t w = std::min<size_t>(8192, rest / sizeof(float4) / 256 * 256);
+    if (w >= 1024) {
+      g.lbits_f = lb;
+      g.fwin_n = static_cast<int32_t>(w);
+      fwd_region = std::max(fwd_knots, w * sizeof(float4));
+      guide_fl = std::max(guide_f, bytes(lb));
+    }
+  }
+  g.fwd_guide_off = static_cast<int32_t>((fwd_region / sizeof(uint32_t) + 3) & ~size_t(3));
+  g.fwd = static_cast<size_t>(g.fwd_guide_off) * sizeof(uint32_t) + guide_fl;
   g.bwd = static_cast<size_t>(g.bwd_guide_off) * sizeof(uint32_t) + guide_b;
   if (g.fwd + g.static_smem > kSmemLimit || g.bwd + g.static_smem > kSmemLimit)
     return LOITS_ERR_UNSUPPORTED;
@@ -354,6 +381,8 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.mcap = p->mcap;
   a.gbits_cap = 30;  // forward: full guides (the backward lowers this)
   a.lguide_bits = p->lbits_f;
+  a.fwin_n = p->fwin_n;
+  a.fwd_guide_off = p->fwd_guide_off;
   a.nd = static_cast<int32_t>(p->nd);
   a.last_nonempty = p->last_nonempty;
   a.tiles_total = p->n_tiles;
@@ -531,6 +560,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->fix_small = sg.fix_small;
   p->win_n = sg.win_n;
   p->bwd_guide_off = sg.bwd_guide_off;
+  p->fwin_n = sg.fwin_n;
+  p->fwd_guide_off = sg.fwd_guide_off;
   // the backward variant with fixed-point sums, when some small density
   // takes that path (one fp32 copy of its sums per CTA, at most 4096 knots,
   // its 36 bytes per knot within the slot; see vjp_chunk_item)
