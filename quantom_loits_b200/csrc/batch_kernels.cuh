@@ -121,6 +121,7 @@ struct BatchArgs {
   int32_t hist_bins;
   int32_t hist_rep;            // shared copies of a tile's histogram (lane % rep), power of 2
   int32_t hist_smem_off;       // floats from the start of dynamic shared memory
+  int32_t hist_shift;          // forward: fixed-point bits of a unit weight
   float hist_lo, hist_inv_h;
 };
 

@@ -1102,12 +1102,18 @@ __device__ __forceinline__ void hist_bin(const BatchArgs& a, float x, int& k, fl
   f = sc - fk;
 }
 
-__device__ __forceinline__ void hist_add(const BatchArgs& a, float* h, float x) {
+// Bins a kept event into a tile's shared copy of the histogram in fixed
+// point: weights 2^S - w and w = f 2^S rounded (S = hist_shift, so that a
+// copy's bins cannot overflow within a tile), one native uint32 atomic each
+// (fp32 shared-memory atomicAdd is a compare-and-swap loop).
+__device__ __forceinline__ void hist_add(const BatchArgs& a, uint32_t* h, float x) {
   int k;
   float f;
   hist_bin(a, x, k, f);
-  if (k >= 0 && k < a.hist_bins) atomicAdd(&h[k], 1.0f - f);
-  if (k + 1 >= 0 && k + 1 < a.hist_bins) atomicAdd(&h[k + 1], f);
+  const uint32_t one = 1u << a.hist_shift;
+  const uint32_t w1 = __float2uint_rn(ldexpf(f, a.hist_shift));
+  if (k >= 0 && k < a.hist_bins) atomicAdd(&h[k], one - w1);
+  if (k + 1 >= 0 && k + 1 < a.hist_bins) atomicAdd(&h[k + 1], w1);
 }
 
 __device__ __forceinline__ float hist_cotangent(const BatchArgs& a, const float* gh, float x) {
@@ -1128,9 +1134,10 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nb = a.hist_bins, stride = nb + 1;
   const int rep = a.hist_rep;
-  for (int i = threadIdx.x; i < rep * stride; i += TPB) hs[i] = 0.0f;
+  uint32_t* hu = reinterpret_cast<uint32_t*>(hs);
+  for (int i = threadIdx.x; i < rep * stride; i += TPB) hu[i] = 0u;
   __syncthreads();
-  float* mine = hs + (lane & (rep - 1)) * stride;
+  uint32_t* mine = hu + (lane & (rep - 1)) * stride;
   const bool full = tile_full<TPB, R>(tg);
   const int kstar = d.threshold ? kept_threshold<kMode>(d) : 0;
   int kept = 0;
@@ -1156,9 +1163,9 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   __syncthreads();
   float* out = a.hist + static_cast<int64_t>(tg.b) * nb;
   for (int k = threadIdx.x; k < nb; k += TPB) {
-    float v = hs[k];
-    for (int c = 1; c < rep; ++c) v += hs[c * stride + k];
-    if (v != 0.0f) atomicAdd(&out[k], v);
+    unsigned long long v = hu[k];
+    for (int c = 1; c < rep; ++c) v += hu[c * stride + k];
+    if (v != 0ull) atomicAdd(&out[k], ldexpf(static_cast<float>(v), -a.hist_shift));
   }
   __syncthreads();
 }

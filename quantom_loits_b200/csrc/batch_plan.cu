@@ -914,6 +914,12 @@ extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* 
   while (rep < 32 && 2 * rep * (bins + 1) * sizeof(float) <= static_cast<size_t>(kHistSmemBytes))
     rep *= 2;
   a.hist_rep = rep;
+  // a copy takes at most tpb / rep lanes x r blocks x 4 slots of a tile, each
+  // adding at most 2^shift to one bin: keep that below 2^32
+  const int64_t per_copy = static_cast<int64_t>(p->tpb) * p->r * 4 / rep;
+  int shift = 31;
+  while (shift > 8 && (per_copy << shift) >= (int64_t(1) << 32)) --shift;
+  a.hist_shift = shift;
   const size_t smem = p->fwd_smem + static_cast<size_t>(rep) * (bins + 1) * sizeof(float);
   return launch_forward(p, a, workspace, smem, st);
 }
