@@ -104,3 +104,39 @@ def global_rows(local_rows: int, group=None) -> tuple[int, int]:
     c = [int(x.item()) for x in counts]
     r = dist.get_rank(group)
     return sum(c[:r]), sum(c)
+
+
+def gather_batch(events, row_offsets, group=None):
+    """The unsplit batch on every rank, for a consumer that needs all of it:
+    (events, row_offsets) of the whole batch from each rank's kept rows and
+    its densities' row offsets (ranks hold contiguous density ranges in rank
+    order).  One all_gather of the row counts, one of the events (padded to
+    the largest rank's count) and one of the row offsets (padded to the most
+    densities); over NCCL on GPU tensors, gloo on host tensors."""
+    import torch
+    import torch.distributed as dist
+
+    world = dist.get_world_size(group)
+    dev = _collective_device()
+    ev = events.to(dev).contiguous()
+    ro = row_offsets.to(device=dev, dtype=torch.int64).contiguous()
+    sizes = torch.tensor([ev.numel(), ro.numel()], dtype=torch.int64, device=dev)
+    all_sizes = [torch.zeros(2, dtype=torch.int64, device=dev) for _ in range(world)]
+    dist.all_gather(all_sizes, sizes, group=group)
+    n_ev = [int(s[0].item()) for s in all_sizes]
+    n_ro = [int(s[1].item()) for s in all_sizes]
+    pad_ev = torch.zeros(max(max(n_ev), 1), dtype=ev.dtype, device=dev)
+    pad_ev[:ev.numel()] = ev
+    pad_ro = torch.zeros(max(n_ro), dtype=torch.int64, device=dev)
+    pad_ro[:ro.numel()] = ro
+    evs = [torch.empty_like(pad_ev) for _ in range(world)]
+    ros = [torch.empty_like(pad_ro) for _ in range(world)]
+    dist.all_gather(evs, pad_ev, group=group)
+    dist.all_gather(ros, pad_ro, group=group)
+    out_ev = torch.cat([evs[r][:n_ev[r]] for r in range(world)])
+    offs, base = [torch.zeros(1, dtype=torch.int64, device=dev)], 0
+    for r in range(world):
+        if n_ro[r] > 1:
+            offs.append(ros[r][1:n_ro[r]] + base)
+        base += n_ev[r]
+    return out_ev, torch.cat(offs)

@@ -7,7 +7,8 @@ unsplit batch's Philox counters.  Here each rank runs the CPU oracle on its
 shard (standing in for its GPU), the ranks exchange one kept-row count each
 (``sharding.global_rows``) to place their rows, and rank 0 checks that the
 gathered events, row offsets and gradients equal the unsplit batch's.  Step
-times are reduced with ``sharding.max_over_ranks``.
+times are reduced with ``sharding.max_over_ranks``; ``sharding.gather_batch``
+gives every rank the unsplit batch's events and row offsets.
 """
 from __future__ import annotations
 
@@ -58,9 +59,15 @@ def _rank_main(rank: int, world: int, port: int, out):
         parts = [None] * world
         dist.all_gather_object(parts, dict(lo=lo, hi=hi, first=first, events=fwd["events"],
                                            rows=fwd["row_offsets"], grad=grad))
+        # the whole batch on every rank (a consumer that needs all of it)
+        import torch
+
+        ev_all, rows_all = sharding.gather_batch(torch.from_numpy(fwd["events"]),
+                                                 torch.from_numpy(fwd["row_offsets"]))
         step_ms = sharding.max_over_ranks(1.5 + rank)
         if rank == 0:
-            out.put(dict(parts=parts, total=total, step_ms=step_ms, seed=seed, seq=seq))
+            out.put(dict(parts=parts, total=total, step_ms=step_ms, seed=seed, seq=seq,
+                         ev_all=ev_all.numpy(), rows_all=rows_all.numpy()))
     finally:
         dist.destroy_process_group()
 
@@ -102,3 +109,6 @@ def test_two_gloo_ranks_reproduce_the_unsplit_batch(oracle_lib, golden):
     np.testing.assert_allclose(np.concatenate([p["grad"] for p in parts]), gref,
                                rtol=1e-12, atol=1e-15)
     assert res["step_ms"] == 2.5  # max over the ranks' 1.5 and 2.5
+    # gather_batch: every rank can hold the unsplit batch's events and rows
+    assert np.array_equal(res["ev_all"], ref["events"])
+    assert np.array_equal(res["rows_all"], ref["row_offsets"])
