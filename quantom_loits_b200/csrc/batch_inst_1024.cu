@@ -22,4 +22,11 @@ template __global__ void batch_forward_kernel<1024, 8, true>(BatchArgs);
 template __global__ void batch_backward_kernel<1024, 8, true, false>(BatchArgs, double*);
 template __global__ void batch_backward_kernel<1024, 8, true, true>(BatchArgs, double*);
 
+template __global__ void batch_forward_kernel<1024, 16, false>(BatchArgs);
+template __global__ void batch_backward_kernel<1024, 16, false, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<1024, 16, false, true>(BatchArgs, double*);
+template __global__ void batch_forward_kernel<1024, 16, true>(BatchArgs);
+template __global__ void batch_backward_kernel<1024, 16, true, false>(BatchArgs, double*);
+template __global__ void batch_backward_kernel<1024, 16, true, true>(BatchArgs, double*);
+
 }  // namespace loits_dev

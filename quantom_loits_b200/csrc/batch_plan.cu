@@ -117,6 +117,7 @@ bool kernels_for(int tpb, int r, bool large, FwdKernel& f, BwdKernel& b, bool fi
       case 2: pick<1024, 2>(large, fix, f, b); return true;
       case 4: pick<1024, 4>(large, fix, f, b); return true;
       case 8: pick<1024, 8>(large, fix, f, b); return true;
+      case 16: pick<1024, 16>(large, fix, f, b); return true;
     }
   }
   return false;
@@ -145,7 +146,6 @@ int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
   if (out.blocks_per_item != 0 && out.blocks_per_item != 2 && out.blocks_per_item != 4 &&
       out.blocks_per_item != 8 && out.blocks_per_item != 16)
     return LOITS_ERR_INVALID;
-  if (out.threads == 1024 && out.blocks_per_item == 16) return LOITS_ERR_INVALID;
   if (out.scan_knots < 1 || out.scan_knots > 64) return LOITS_ERR_INVALID;
   if (out.ctas_per_sm < 0 || out.ctas_per_sm > 32) return LOITS_ERR_INVALID;
   if (out.plain != 0 && out.plain != 1) return LOITS_ERR_INVALID;
@@ -338,7 +338,6 @@ int choose_threads(int r_req, int64_t large_g, int32_t gcap, int64_t max_g, int&
   int best = -1, best_tpb = 0, last_rc = LOITS_ERR_UNSUPPORTED;
   for (int tpb : {256, 512, 1024}) {
     const int r = r_req ? r_req : default_blocks(tpb);
-    if (tpb == 1024 && r == 16) continue;
     SmemGeometry g;
     const int rc = smem_geometry(tpb, r, large_g, gcap, max_g, g);
     if (rc != LOITS_OK) {

@@ -2,7 +2,7 @@
 
 The batched kernels take three launch parameters (``loits_batch_config``):
 threads per CTA (256, 512, 1024), Philox blocks per thread per sampling tile
-(2, 4, 8, 16; at most 8 with 1024 threads) and knots per thread in the CDF
+(2, 4, 8, 16) and knots per thread in the CDF
 scan.  Which is fastest depends on the batch: the largest density decides
 how much shared memory a CTA holds (hence how many CTAs fit on an SM), the
 event counts decide how many tiles there are to balance, and the cut decides
@@ -35,7 +35,7 @@ from . import _native as N
 CANDIDATES = (
     (256, 16, 8), (256, 8, 8), (256, 4, 8),
     (512, 16, 8), (512, 8, 8),
-    (1024, 8, 8), (1024, 4, 8), (1024, 8, 16),
+    (1024, 16, 8), (1024, 8, 8), (1024, 4, 8), (1024, 8, 16),
 )
 
 

@@ -142,7 +142,7 @@ def test_plain_and_persistent_forms_agree(B, golden):
 
 @pytest.mark.parametrize("threads,blocks,scan", [(256, 2, 1), (256, 2, 3), (512, 4, 8),
                                                  (512, 8, 16), (256, 16, 64), (1024, 2, 1),
-                                                 (1024, 8, 4)])
+                                                 (1024, 8, 4), (1024, 16, 8)])
 def test_launch_geometries_agree(B, golden, threads, blocks, scan):
     c = golden_case(golden, "ragged_small")
     a = run_batch(B, c)

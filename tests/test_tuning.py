@@ -17,7 +17,7 @@ def test_shape_key_buckets_by_powers_of_two():
 def test_candidates_are_valid_geometries():
     for threads, blocks, scan in tuning.CANDIDATES:
         assert threads in (256, 512, 1024)
-        assert blocks in (2, 4, 8, 16) and not (threads == 1024 and blocks == 16)
+        assert blocks in (2, 4, 8, 16)
         assert 1 <= scan <= 64
 
 
