@@ -832,7 +832,15 @@ def run_gan_b200(args, rank, world, dist) -> dict:
 
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
-    tr = BatchedGANTrainer(dev, seed=rank)
+    # the sampler's launch geometry: tuned on the batch (config="auto") unless
+    # --threads / --blocks name one
+    if args.threads or args.blocks:
+        from quantom_loits_b200.batched import make_config
+
+        config = make_config(threads=args.threads, blocks_per_item=args.blocks)
+    else:
+        config = "auto"
+    tr = BatchedGANTrainer(dev, seed=rank, config=config)
     tr.capture()  # the whole step as one CUDA graph
     stream = torch.cuda.current_stream(dev)
     for _ in range(args.warmup):
@@ -896,7 +904,8 @@ def run_gan_b200(args, rank, world, dist) -> dict:
         "data": "synthetic",
         "config": {**describe_gan(tr), "events_per_step": ev_step,
                    "parallelism": f"replicas x{world}", "form": "whole step in one CUDA graph",
-                   "launch": None},
+                   "launch": next(iter(tr.sampler._plans.values())).config
+                   if tr.sampler._plans else None},
         "gan": {"steps_per_s": 1e3 / ms, "sampler_ms_per_step": s_ms,
                 "sampler_share": s_ms / ms, "d_loss": float(d_loss), "g_loss": float(g_loss)},
         "e2e": {"value": ev_step * world / (e_ms * 1e-3), "unit": "events/s", "ms_per_step": e_ms,
