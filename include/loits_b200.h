@@ -145,7 +145,8 @@ typedef struct loits_batch_plan loits_batch_plan; /* opaque, host object */
 
 /* Launch geometry of the batched kernels.  Zero fields take defaults. */
 typedef struct loits_batch_config {
-  int32_t threads;         /* threads per CTA of the sampling kernels: 256 (default), 512 or 1024 */
+  int32_t threads;         /* threads per CTA of the sampling kernels: 256, 512 or 1024;
+                              0 = the size with the most resident threads per SM */
   int32_t blocks_per_item; /* Philox blocks (4 slots each) per thread per tile: 2,4,8,16;
                               default 16 (8 with 1024 threads) */
   int32_t scan_knots;      /* knots per thread in the CDF scan: 1..64, default 8 */
