@@ -121,28 +121,52 @@ struct CdfShared {
 
 // Double-float prefix step for knot t of density (g, f): adds the area of
 // interval [t-1, t] (t >= 1).  Returns false if that area is negative/NaN.
-__device__ __forceinline__ bool add_area(const float* __restrict__ g, const float* __restrict__ f,
-                                         int64_t t, float& ph, float& pl) {
+// A density's knots as the CDF passes read them: knot t's position and value
+// at g[t - off], f[t - off] -- the density in global memory (off = 0), or a
+// CDF tile's knots staged in shared memory (kS: plain loads; __ldg is for
+// global memory only).
+struct Knots {
+  const float* g;
+  const float* f;
+  int64_t off;
+};
+
+template <bool kS>
+__device__ __forceinline__ float knot_g(const Knots& kn, int64_t t) {
+  if constexpr (kS) return kn.g[t - kn.off];
+  else return __ldg(&kn.g[t - kn.off]);
+}
+
+template <bool kS>
+__device__ __forceinline__ float knot_f(const Knots& kn, int64_t t) {
+  if constexpr (kS) return kn.f[t - kn.off];
+  else return __ldg(&kn.f[t - kn.off]);
+}
+
+template <bool kS>
+__device__ __forceinline__ bool add_area(const Knots& kn, int64_t t, float& ph, float& pl) {
   if (t < 1) return true;
   float ah, al;
-  trapezoid_df(__ldg(&g[t - 1]), __ldg(&g[t]), __ldg(&f[t - 1]), __ldg(&f[t]), ah, al);
+  trapezoid_df(knot_g<kS>(kn, t - 1), knot_g<kS>(kn, t), knot_f<kS>(kn, t - 1), knot_f<kS>(kn, t),
+               ah, al);
   df_add(ph, pl, ah, al);
   return ah >= 0.0f;
 }
 
 // Pass 1 over this thread's knots [my_lo, my_hi): local total and max prefix.
 // bad_grid: a knot position is not finite or below its predecessor.
-__device__ __forceinline__ void cdf_pass1(const float* g, const float* f, int64_t my_lo,
-                                          int64_t my_hi, double& total, double& maxp, bool& neg,
+template <bool kS>
+__device__ __forceinline__ void cdf_pass1(const Knots& kn, int64_t my_lo, int64_t my_hi,
+                                          double& total, double& maxp, bool& neg,
                                           bool& bad_grid) {
   float ph = 0.0f, pl = 0.0f;
   maxp = kNegInf;
   neg = false;
   bad_grid = false;
   for (int64_t t = my_lo; t < my_hi; ++t) {
-    const float gt = __ldg(&g[t]);
-    bad_grid |= !isfinite(gt) || (t >= 1 && !(gt >= __ldg(&g[t - 1])));
-    neg |= !add_area(g, f, t, ph, pl);
+    const float gt = knot_g<kS>(kn, t);
+    bad_grid |= !isfinite(gt) || (t >= 1 && !(gt >= knot_g<kS>(kn, t - 1)));
+    neg |= !add_area<kS>(kn, t, ph, pl);
     const double p = static_cast<double>(ph) + static_cast<double>(pl);
     maxp = p > maxp ? p : maxp;
   }
@@ -163,16 +187,18 @@ __device__ __forceinline__ int32_t bucket_start(float key, int m) {
 // Record: {key, key - c, g_t, m_t}; key = the smallest fp32 >= c_t, so that
 // for every fp32 u, (u >= c_t) == (u >= key) exactly.
 // gd: guide of the density (nullptr when the CDF is not non-decreasing).
-__device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, int64_t t, double c,
-                                            bool has_next, double c_next, uint32_t* gd, int m) {
+template <bool kS>
+__device__ __forceinline__ void emit_record(const BatchArgs& a, int64_t k0, const Knots& kn,
+                                            int64_t t, double c, bool has_next, double c_next,
+                                            uint32_t* gd, int m) {
   const float key = __double2float_ru(c);
   const float dk = __double2float_rn(static_cast<double>(key) - c);
-  const float gt = __ldg(&a.grid[k0 + t]);
+  const float gt = knot_g<kS>(kn, t);
   float m_slope = 0.0f, inv = 0.0f, key_next = 0.0f;
   if (has_next) {
     key_next = __double2float_ru(c_next);
     const double inv_d = 1.0 / (c_next - c + kEps);
-    const double md = (static_cast<double>(__ldg(&a.grid[k0 + t + 1])) - static_cast<double>(gt)) * inv_d;
+    const double md = (static_cast<double>(knot_g<kS>(kn, t + 1)) - static_cast<double>(gt)) * inv_d;
     m_slope = __double2float_rn(md);
     inv = __double2float_rn(inv_d);
   }
@@ -242,17 +268,15 @@ __device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
 // base = tile_excl + thread exclusive sum; run0 = max of the prefix before
 // this thread (the clamp); tile_next_c is c at knot `hi` when hi < G;
 // gd / m: the density's guide table (nullptr for count semantics).
-template <int TPB>
-__device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_t G, int64_t hi, int64_t my_lo,
+template <int TPB, bool kS>
+__device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, const Knots& kn, int64_t G, int64_t hi, int64_t my_lo,
                           int64_t my_hi, double base, double run0, double norm, bool nonmono,
                           double tile_next_c, uint32_t* gd, int m, CdfShared<TPB>& sh) {
-  const float* g = a.grid + k0;
-  const float* f = a.values + k0;
   // first knot of each thread goes to shared memory for its left neighbour
   double c_first = 0.0;
   if (my_lo < my_hi) {
     float ph = 0.0f, pl = 0.0f;
-    add_area(g, f, my_lo, ph, pl);
+    add_area<kS>(kn, my_lo, ph, pl);
     double s = base + (static_cast<double>(ph) + static_cast<double>(pl));
     if (!nonmono) s = s > run0 ? s : run0;
     c_first = s / norm;
@@ -263,21 +287,21 @@ __device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, int64_
     float ph = 0.0f, pl = 0.0f;
     double run = run0, c_prev = 0.0;
     for (int64_t t = my_lo; t < my_hi; ++t) {
-      add_area(g, f, t, ph, pl);
+      add_area<kS>(kn, t, ph, pl);
       double s = base + (static_cast<double>(ph) + static_cast<double>(pl));
       if (!nonmono) {
         run = s > run ? s : run;
         s = run;
       }
       const double c = s / norm;
-      if (t > my_lo) emit_record(a, k0, t - 1, c_prev, true, c, gd, m);
+      if (t > my_lo) emit_record<kS>(a, k0, kn, t - 1, c_prev, true, c, gd, m);
       c_prev = c;
     }
     // last knot of this thread: end of density, next thread, or next tile
     const int64_t t = my_hi - 1;
-    if (t == G - 1) emit_record(a, k0, t, c_prev, false, 0.0, gd, m);
-    else if (t + 1 < hi) emit_record(a, k0, t, c_prev, true, sh.cfirst[threadIdx.x + 1], gd, m);
-    else emit_record(a, k0, t, c_prev, true, tile_next_c, gd, m);
+    if (t == G - 1) emit_record<kS>(a, k0, kn, t, c_prev, false, 0.0, gd, m);
+    else if (t + 1 < hi) emit_record<kS>(a, k0, kn, t, c_prev, true, sh.cfirst[threadIdx.x + 1], gd, m);
+    else emit_record<kS>(a, k0, kn, t, c_prev, true, tile_next_c, gd, m);
   }
   // every thread publishes its records before thread 0 signals readiness
   __threadfence();
@@ -340,8 +364,48 @@ __device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first
   return chained_lookback(a.cflag, a.cagg, a.cinc, a.status, first, ct, agg);
 }
 
+// Whether CDF item `it` (owner table first[]: scan or finalize items) can
+// stage its knots, 2 floats per knot of [lo - 1, hi + 1), in the dynamic
+// shared memory before the guide.
+__device__ __forceinline__ bool cdf_tile_fits(const BatchArgs& a, const int32_t* first, int32_t it,
+                                              int tpb) {
+  const int b = find_owner(first, a.d_lo, a.d_hi, it);
+  const int64_t G = __ldg(&a.knot_off[b + 1]) - __ldg(&a.knot_off[b]);
+  const int64_t KT = static_cast<int64_t>(tpb) * a.scan_knots;
+  const int64_t n = (G < KT ? G : KT) + 2;
+  return 8 * n <= 4ll * a.fwd_guide_off;
+}
+
+// Knots [s0, s1) of the density at k0 into shared memory (sg, sf): coalesced
+// loads, all in flight at once, instead of each thread's strided chain of
+// dependent loads.  The caller synchronises.
 template <int TPB>
-__device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared<TPB>& sh) {
+__device__ __forceinline__ void stage_knots(const BatchArgs& a, int64_t k0, int64_t s0,
+                                            int64_t s1, float* sg, float* sf) {
+  const int64_t n = s1 - s0;
+#pragma unroll 4
+  for (int64_t i = threadIdx.x; i < n; i += TPB) {
+    sg[i] = __ldg(&a.grid[k0 + s0 + i]);
+    sf[i] = __ldg(&a.values[k0 + s0 + i]);
+  }
+}
+
+// The knots a CDF tile [lo, hi) reads: [lo - 1, hi + 1) within the density.
+// kS: staged in shared memory (stage_s, which holds 2 (s1 - s0) floats).
+template <bool kS>
+__device__ __forceinline__ Knots tile_knots(const BatchArgs& a, int64_t k0, int64_t G,
+                                            int64_t lo, int64_t hi, float* stage_s) {
+  if constexpr (kS) {
+    const int64_t s0 = lo > 0 ? lo - 1 : 0, s1 = hi + 1 < G ? hi + 1 : G;
+    return Knots{stage_s, stage_s + (s1 - s0), s0};
+  } else {
+    return Knots{a.grid + k0, a.values + k0, 0};
+  }
+}
+
+template <int TPB, bool kS>
+__device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared<TPB>& sh,
+                                              float* stage_s) {
   const int b = find_owner(a.cdf_first, a.d_lo, a.d_hi, ct);
   const int32_t first = __ldg(&a.cdf_first[b]);
   const int32_t ci = ct - first, nci = __ldg(&a.cdf_first[b + 1]) - first;
@@ -349,13 +413,19 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
   const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
+  const Knots kn = tile_knots<kS>(a, k0, G, lo, hi, stage_s);
+  if constexpr (kS) {
+    stage_knots<TPB>(a, k0, kn.off, kn.off + (kn.f - kn.g), const_cast<float*>(kn.g),
+                     const_cast<float*>(kn.f));
+    __syncthreads();
+  }
   const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * a.scan_knots;
   const int64_t my_lo = my_lo_raw < hi ? my_lo_raw : hi;
   const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
   double tot, maxp;
   bool neg;
   bool bad_grid;
-  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg, bad_grid);
+  cdf_pass1<kS>(kn, my_lo, my_hi, tot, maxp, neg, bad_grid);
   double tile_tot;
   const double excl = block_exclusive_sum<double, TPB>(tot, tile_tot, sh.dscan);
   const double thr_max = my_lo < my_hi ? excl + maxp : kNegInf;
@@ -366,8 +436,8 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   if (nci == 1) {
     // whole density in one tile: finalise now
     uint32_t* gd = any_neg ? nullptr : a.gl + __ldg(&a.goff[b]);
-    cdf_pass2<TPB>(a, k0, G, hi, my_lo, my_hi, excl, run0, tile_tot, any_neg, 0.0, gd,
-                   __ldg(&a.gbits[b]), sh);
+    cdf_pass2<TPB, kS>(a, k0, kn, G, hi, my_lo, my_hi, excl, run0, tile_tot, any_neg, 0.0, gd,
+                       __ldg(&a.gbits[b]), sh);
     if (!any_neg) pack_guide<TPB>(a, b);
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -406,8 +476,9 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   __syncthreads();
 }
 
-template <int TPB>
-__device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi, CdfShared<TPB>& sh) {
+template <int TPB, bool kS>
+__device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi, CdfShared<TPB>& sh,
+                                                  float* stage_s) {
   const int b = find_owner(a.fin_first, a.d_lo, a.d_hi, fi);
   const int32_t ci = fi - __ldg(&a.fin_first[b]);
   const int32_t first = __ldg(&a.cdf_first[b]);
@@ -417,6 +488,10 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
   const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
+  const Knots kn = tile_knots<kS>(a, k0, G, lo, hi, stage_s);
+  if constexpr (kS)  // made visible by the barrier after the lane-0 work below
+    stage_knots<TPB>(a, k0, kn.off, kn.off + (kn.f - kn.g), const_cast<float*>(kn.g),
+                     const_cast<float*>(kn.f));
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
     if (lane == 0 && !wait_counter(&a.cdf_scanned[b], static_cast<uint32_t>(nci), a.status))
@@ -442,7 +517,7 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
       if (hi < G) {
         // first knot of the next tile, exactly as that tile's own pass 2 forms it
         float ph = 0.0f, pl = 0.0f;
-        add_area(a.grid + k0, a.values + k0, hi, ph, pl);
+        add_area<false>(Knots{a.grid + k0, a.values + k0, 0}, hi, ph, pl);
         double s = (__ldcg(&a.cinc[ct]) + 0.0) + (static_cast<double>(ph) + static_cast<double>(pl));
         if (!sh.nonmono) {
           const double m_own = __ldcg(&a.cmax[ct]);
@@ -461,7 +536,7 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
   double tot, maxp;
   bool neg, bad_grid;
-  cdf_pass1(a.grid + k0, a.values + k0, my_lo, my_hi, tot, maxp, neg, bad_grid);
+  cdf_pass1<kS>(kn, my_lo, my_hi, tot, maxp, neg, bad_grid);
   double tile_tot;
   const double excl = block_exclusive_sum<double, TPB>(tot, tile_tot, sh.dscan);
   const double thr_max = my_lo < my_hi ? (tile_excl + excl) + maxp : kNegInf;
@@ -470,8 +545,8 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   run0 = run0 > mprev ? run0 : mprev;
   (void)has_next;
   uint32_t* gd = nonmono ? nullptr : a.gl + __ldg(&a.goff[b]);
-  cdf_pass2<TPB>(a, k0, G, hi, my_lo, my_hi, tile_excl + excl, run0, norm, nonmono, cnext, gd,
-                 __ldg(&a.gbits[b]), sh);
+  cdf_pass2<TPB, kS>(a, k0, kn, G, hi, my_lo, my_hi, tile_excl + excl, run0, norm, nonmono,
+                     cnext, gd, __ldg(&a.gbits[b]), sh);
   // the last finalize item of the density packs its guide and publishes it
   if (threadIdx.x == 0) sh.has_next = atomicAdd(&a.fin_done[b], 1u) == static_cast<uint32_t>(nci - 1);
   __syncthreads();
@@ -1957,6 +2032,9 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
   extern __shared__ __align__(16) unsigned char smem_raw[];
   float4* rec_s = reinterpret_cast<float4*>(smem_raw);
   uint32_t* guide_s = reinterpret_cast<uint32_t*>(smem_raw) + a.fwd_guide_off;
+  // CDF items stage their tile's knots where sampling items later keep
+  // records (a CTA takes every CDF ticket it gets before any sampling ticket)
+  float* stage_s = reinterpret_cast<float*>(smem_raw);
   // this CTA's staging run in global memory (TPB * R * 4 floats): kept
   // events wait there for their tile's row base; they stay in L2
   float* stage = a.stage_g + static_cast<int64_t>(blockIdx.x) * (TPB * R * 4);
@@ -1977,9 +2055,13 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
     __syncthreads();
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nC)) {
-      cdf_scan_item<TPB>(a, a.c_lo + static_cast<int32_t>(item), sh.cdf);
+      const int32_t ct = a.c_lo + static_cast<int32_t>(item);
+      if (cdf_tile_fits(a, a.cdf_first, ct, TPB)) cdf_scan_item<TPB, true>(a, ct, sh.cdf, stage_s);
+      else cdf_scan_item<TPB, false>(a, ct, sh.cdf, stage_s);
     } else if (item < static_cast<uint32_t>(nC + nF)) {
-      cdf_finalize_item<TPB>(a, a.f_lo + static_cast<int32_t>(item) - nC, sh.cdf);
+      const int32_t fi = a.f_lo + static_cast<int32_t>(item) - nC;
+      if (cdf_tile_fits(a, a.fin_first, fi, TPB)) cdf_finalize_item<TPB, true>(a, fi, sh.cdf, stage_s);
+      else cdf_finalize_item<TPB, false>(a, fi, sh.cdf, stage_s);
     } else {
       sample_item<TPB, R, kLarge>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s,
                                   guide_s, stage, sh.smp, s_guide_key, s_win);
