@@ -23,11 +23,12 @@ namespace loits_dev {
 //
 // Densities of at most `gcap` knots are sampled from shared memory (records
 // and packed guide copied per tile); larger ones ("large densities", more
-// than 8192 knots) are sampled straight from the records and the uint32
-// guide in global memory (L2-resident where the events concentrate), their
-// backward accumulates per interval the pair of grad-CDF sums it sends to its
-// two knots with one float2 global atomic per event, and finalizes with a
-// multi-tile reverse scan.
+// than 8192 knots) keep records and the uint32 guide in global memory: the
+// forward searches a window of records around the most probable stretch in
+// shared memory (coarse guide beside it) and the rest through L2; the
+// backward sums the window's intervals in fixed point in shared memory,
+// sends every other event's pair of grad-CDF sums to its two knots with one
+// float2 global reduction, and finalizes with a multi-tile reverse scan.
 struct BatchArgs {
   // plan tables (device)
   const int64_t* knot_off;     // [B+1]

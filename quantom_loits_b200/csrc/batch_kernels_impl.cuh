@@ -30,7 +30,8 @@
 //   1. Chunks (density, run of sampling tiles): recompute uniforms, intervals
 //      and the compaction ranks of the forward, read the cotangents of the
 //      kept rows, scatter the interpolation VJP (cpp/loits_core.cpp:293-300)
-//      into a shared-memory grad-CDF, write it as the chunk's partial.
+//      into shared-memory grad-CDF sums (fixed point or replicated fp32),
+//      write them as the chunk's partial.
 //   2. Density finalize: sum the partials in chunk order (fp64,
 //      deterministic), reverse suffix scan (cdf_vjp, :340-368) and the
 //      normaliser VJP (density_vjp, :400-435), fp32 output.
