@@ -107,6 +107,11 @@ def test_entry_points_reject_bad_arguments_on_host(native):
         native.LOITS_ERR_UNSUPPORTED
     assert lib.loits_batch_forward(None, None, None, None, 0, 0, None, None, None, None, None) == \
         native.LOITS_ERR_INVALID
+    # saved-state entry points: a missing plan or buffer is rejected before any launch
+    assert lib.loits_batch_forward_state(None, None, None, None, 0, 0, None, None, None, None,
+                                         None, None) == native.LOITS_ERR_INVALID
+    assert lib.loits_batch_backward_state(None, None, None, None, None, None, None, None, None,
+                                          None) == native.LOITS_ERR_INVALID
     assert lib.loits_tuple_sample_workspace(0) >= 16
 
 
