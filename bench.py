@@ -1,38 +1,48 @@
 """Benchmark: fwd+VJP events/s of the batched LOITS sampler on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
-                    [--workload uniform|single|ragged|precision|tuple|gan] [--events E]
+                    [--workload ragged|uniform|single|precision|tuple|gan] [--events E]
 
 One step = forward (normalise, CDF, Philox, inverse-CDF search +
 interpolation, stable compaction) + VJP of the whole density batch.  The
-default workload is 64 densities on a 1024-knot uniform grid over [1e-3, 1]
-with 1e6 events each (6.4e7 events per step), seeded synthetic densities
-(sums of 1-3 x^a (1-x)^b components); no dataset is involved.
+default workload is the ragged batch: 512 densities with knot counts
+log-uniform in [64, 8192] and event counts log-uniform in [1e4, 1e6] (about
+1.0e8 events per step), a per-density acceptance cut x > x_cut; seeded
+synthetic densities (sums of 1-3 x^a (1-x)^b components), no dataset.
 
 Arms:
-  --impl b200       (default) the persistent, CUDA-graph-captured form; the
-                    plain one-launch-per-density form is measured beside it.
+  --impl b200       (default) the persistent form captured in one CUDA graph
+                    (``value``); beside it the plain form -- one forward and
+                    one backward launch per density, no graph -- with its own
+                    tuned launch geometry, the saved-state form, and ``e2e``:
+                    LOITS(backend="cuda")(DensityBatch, event_counts) +
+                    autograd backward with host buffers.
   --impl reference  the reference's own openmp core (oracle/_ref, compiled
                     from the reference sources) on the host cores, on the exact
                     embedding of the same workload, a bounded sample per step.
 
 Before timing, the launch geometry (threads per CTA, Philox blocks per thread,
-CDF scan width) is tuned on the workload itself by timing each candidate
-(quantom_loits_b200.tuning; untimed, reported as config.tuning_ms_per_step);
---no-tune keeps the plan's default (CTA size by occupancy).
+CDF scan width) of each form is tuned on the workload itself by timing each
+of its candidates (quantom_loits_b200.tuning; untimed, reported as
+tuning_ms_per_step); --no-tune keeps the plan's default (CTA size by
+occupancy); --threads/--blocks and --plain-threads/--plain-blocks fix them.
 
---workload gan runs config 4: batched GAN steps (generator MLP -> power-law
-theory on 2048 knots -> 256 x 2e5 events binned into 64-bin histograms in the
-sampler's kernels -> discriminator), the sampler's share of the step reported.
+--workload uniform (64 x 1024 knots, 1e6 events each), single (1 x 256 knots,
+1e5 events) and precision (16 x 2^20 knots, 1e7 events each) run the other
+batch shapes; --workload gan runs batched GAN steps (generator MLP ->
+power-law theory on 2048 knots -> 256 x 2e5 events binned into 64-bin
+histograms in the sampler's kernels -> discriminator), the sampler's share of
+the step reported; --workload tuple runs the reference's own 2-D theory tuple
+at the scale of its GPU benchmark (99 x 99 cells, K = 10, 1e7 events; fp64,
+bit-exact with the reference) through LOITS(backend="cuda"); its reference
+arm is the reference's openmp core on the identical tuple.
 
---workload tuple runs the reference's own 2-D theory tuple at the scale of its
-GPU benchmark (99 x 99 cells, K = 10, 1e7 events; fp64, bit-exact with the
-reference) through LOITS(backend="cuda"); its reference arm is the reference's
-openmp core on the identical tuple.
+--eager-steps K only runs K eager forward + backward launches of a batched
+workload at a given geometry (the launches a profiler attaches to).
 
-Under torchrun each rank (one GPU) samples its own 64 densities of a global
-batch (density_base = rank * 64, same Philox slot stride): weak scaling, no
-collective on the data path; the step time is the max over ranks.
+Under torchrun each rank (one GPU) samples its own copy-shaped share of a
+global batch (density_base = rank * B, same Philox slot stride): weak
+scaling, no collective on the data path; the step time is the max over ranks.
 """
 from __future__ import annotations
 
@@ -267,34 +277,86 @@ def run_reference(args, spec) -> dict:
 
 # ------------------------------------------------------------------- b200
 
+def tune(spec, dev, args, plain: bool):
+    """Launch geometry of the persistent form (plain=False) or of the
+    one-launch-per-density form (plain=True), each timed on this rank's batch
+    on its own candidates (untimed by the bench).  Returns (config dict,
+    {candidate: ms})."""
+    from quantom_loits_b200 import batched as B
+    from quantom_loits_b200.tuning import CANDIDATES, PLAIN_CANDIDATES, Autotuner
+
+    threads, blocks = (args.plain_threads, args.plain_blocks) if plain else (args.threads,
+                                                                              args.blocks)
+    base = {"guide_ratio": args.guide_ratio}
+    if plain:
+        base["plain"] = 1
+    if threads or blocks or args.no_tune:
+        return dict(base, threads=threads, blocks_per_item=blocks, scan_knots=0), None
+    tbatch = B.DensityBatch.from_spec(spec, dev)
+    tuner = Autotuner(dev, candidates=PLAIN_CANDIDATES if plain else CANDIDATES, base=base)
+    best, times = tuner.tune(tbatch, spec.event_counts, spec.seed, 0)
+    return best, times
+
+
+def make_step(spec, dev, geom, rank, saved_state=False):
+    from quantom_loits_b200 import batched as B
+
+    nmax = int(spec.event_counts.max())
+    cfg = B.make_config(**geom, density_base=rank * spec.n_densities, slot_stride=nmax)
+    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev)
+    step = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None,
+                       saved_state=saved_state)
+    step.grid.copy_(torch_from(spec.grid))
+    step.values.copy_(torch_from(spec.values))
+    if spec.x_cut is not None:
+        step.x_cut.copy_(torch_from(spec.x_cut))
+    return plan, step
+
+
+def torch_from(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a))
+
+
+def time_steps(step, steps, barrier, stream) -> float:
+    """ms per step of `steps` back-to-back steps (graph replays when
+    captured), device-timed with CUDA events between barriers."""
+    import torch
+
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    barrier()
+    t0.record(stream)
+    for _ in range(steps):
+        step.step()
+    t1.record(stream)
+    barrier()
+    return t0.elapsed_time(t1) / steps
+
+
+def time_kernels(step, steps, stream) -> tuple[float, float]:
+    """Mean device time of the forward launch and of the backward launch."""
+    import torch
+
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    fwd, bwd = [], []
+    for _ in range(steps):
+        ev[0].record(stream)
+        step.forward()
+        ev[1].record(stream)
+        step.backward()
+        ev[2].record(stream)
+        ev[2].synchronize()
+        fwd.append(ev[0].elapsed_time(ev[1]))
+        bwd.append(ev[1].elapsed_time(ev[2]))
+    return float(np.mean(fwd)), float(np.mean(bwd))
+
+
 def run_b200(args, spec, rank, world, dist) -> dict:
     import torch
 
-    from quantom_loits_b200 import batched as B
-
     dev = torch.device("cuda", int(os.environ.get("LOCAL_RANK", "0")))
     torch.cuda.set_device(dev)
-    nmax = int(spec.event_counts.max())
-    # launch geometry: tuned on this rank's batch (untimed), unless given
-    geom = dict(threads=args.threads, blocks_per_item=args.blocks, scan_knots=0)
-    tune_ms = None
-    if not args.no_tune and args.threads == 0 and args.blocks == 0:
-        from quantom_loits_b200.tuning import Autotuner
-
-        tbatch = B.DensityBatch.from_spec(spec, dev)
-        best, tune_ms = Autotuner(dev).tune(tbatch, spec.event_counts, spec.seed, 0)
-        geom.update(best)
-        del tbatch
-    args.geom = geom
-    cfg = B.make_config(**geom, density_base=rank * spec.n_densities, slot_stride=nmax)
-    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev)
-    step = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None)
-    step.grid.copy_(torch.from_numpy(spec.grid))
-    step.values.copy_(torch.from_numpy(spec.values))
-    if spec.x_cut is not None:
-        step.x_cut.copy_(torch.from_numpy(spec.x_cut))
-    gen = torch.Generator(device=dev).manual_seed(1000 + rank)
-    step.grad_events.normal_(generator=gen)
     stream = torch.cuda.current_stream(dev)
 
     def barrier():
@@ -302,110 +364,70 @@ def run_b200(args, spec, rank, world, dist) -> dict:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
+    # ---- launch geometries: each form tuned on its own candidates
+    geom, tune_ms = tune(spec, dev, args, plain=False)
+    pgeom, ptune_ms = tune(spec, dev, args, plain=True)
+    args.geom = geom
+    plan, step = make_step(spec, dev, geom, rank)
+    gen = torch.Generator(device=dev).manual_seed(1000 + rank)
+    step.grad_events.normal_(generator=gen)
+
     # ---- per-kernel durations (forward and backward launches, eager)
     for _ in range(max(args.warmup, 3)):
         step.forward()
         step.backward()
     torch.cuda.synchronize(dev)
     step.check_status()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
-    fwd_ms, bwd_ms = [], []
-    for _ in range(args.steps):
-        ev[0].record(stream)
-        step.forward()
-        ev[1].record(stream)
-        step.backward()
-        ev[2].record(stream)
-        ev[2].synchronize()
-        fwd_ms.append(ev[0].elapsed_time(ev[1]))
-        bwd_ms.append(ev[1].elapsed_time(ev[2]))
+    f_ms, b_ms = time_kernels(step, args.steps, stream)
 
-    # ---- batched form: persistent kernels, fwd+bwd captured in one graph
+    # ---- batched form: persistent kernels, forward + backward in one graph
     step.capture()
     for _ in range(args.warmup):
         step.step()
-    barrier()
-    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev.index) as clocks:
-        barrier()
-        t0.record(stream)
-        for _ in range(args.steps):
-            step.step()
-        t1.record(stream)
-        barrier()
+        ms = time_steps(step, args.steps, barrier, stream)
     step.check_status()
-    ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
         ms = max_over_ranks(ms)
     events_step = spec.total_events * world
     value = events_step / (ms * 1e-3)
     valid = int(step.row_offsets[-1].item())
 
-    # ---- plain form: one launch per density for forward and for backward
-    plain_cfg = B.make_config(**geom, plain=1, density_base=rank * spec.n_densities,
-                              slot_stride=nmax)
-    pplan = B.BatchPlan(spec.knot_offsets, spec.event_counts, plain_cfg, dev)
-    pstep = B.BatchStep(pplan, seed=spec.seed, with_cut=spec.x_cut is not None)
-    pstep.grid.copy_(step.grid); pstep.values.copy_(step.values)
-    if spec.x_cut is not None:
-        pstep.x_cut.copy_(step.x_cut)
+    # ---- plain form: one forward and one backward launch per density, its
+    # own tuned geometry, no graph
+    pplan, pstep = make_step(spec, dev, pgeom, rank)
     pstep.grad_events.copy_(step.grad_events)
     for _ in range(args.warmup):
         pstep.step()
-    barrier()
-    t0.record(stream)
-    for _ in range(args.steps):
-        pstep.step()
-    t1.record(stream)
-    barrier()
+    plain_ms = time_steps(pstep, args.steps, barrier, stream)
     pstep.check_status()
-    plain_ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
         plain_ms = max_over_ranks(plain_ms)
-    plain_value = events_step / (plain_ms * 1e-3)
     same = torch.equal(pstep.events[:valid], step.events[:valid])
+    plain_rows_same = torch.equal(pstep.row_offsets, step.row_offsets)
+    plain_launch = pplan.config
     del pstep, pplan
 
     # ---- saved-state form: the forward also writes (interval, offset) per
     # kept row, the backward reads them instead of replaying the uniforms
-    sstep = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None, saved_state=True)
-    sstep.grid.copy_(step.grid); sstep.values.copy_(step.values)
-    if spec.x_cut is not None:
-        sstep.x_cut.copy_(step.x_cut)
+    splan, sstep = make_step(spec, dev, geom, rank, saved_state=True)
     sstep.grad_events.copy_(step.grad_events)
     for _ in range(max(args.warmup, 3)):
-        sstep.forward()
-        sstep.backward()
+        sstep.step()
     torch.cuda.synchronize(dev)
     sstep.check_status()
-    s_fwd, s_bwd = [], []
-    for _ in range(args.steps):
-        ev[0].record(stream)
-        sstep.forward()
-        ev[1].record(stream)
-        sstep.backward()
-        ev[2].record(stream)
-        ev[2].synchronize()
-        s_fwd.append(ev[0].elapsed_time(ev[1]))
-        s_bwd.append(ev[1].elapsed_time(ev[2]))
+    s_fwd, s_bwd = time_kernels(sstep, args.steps, stream)
     sstep.capture()
     for _ in range(args.warmup):
         sstep.step()
-    barrier()
-    t0.record(stream)
-    for _ in range(args.steps):
-        sstep.step()
-    t1.record(stream)
-    barrier()
+    state_ms = time_steps(sstep, args.steps, barrier, stream)
     sstep.check_status()
-    state_ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
         state_ms = max_over_ranks(state_ms)
     gscale = float(step.grad_values.abs().max().item()) or 1.0
     saved_state = {
         "value": events_step / (state_ms * 1e-3), "ms_per_step": state_ms,
-        "kernels_ms": {"batch_forward_kernel": float(np.mean(s_fwd)),
-                       "batch_backward_kernel": float(np.mean(s_bwd))},
+        "kernels_ms": {"batch_forward_kernel": s_fwd, "batch_backward_kernel": s_bwd},
         "form": "forward writes interval (int32) + offset u - c_j (fp32) per kept row; "
                 "backward reads them, one CUDA graph",
         "state_bytes": 8 * valid,
@@ -414,13 +436,12 @@ def run_b200(args, spec, rank, world, dist) -> dict:
                                           .item()) / gscale,
     }
     sstep.graph = None
-    del sstep
+    del sstep, splan
 
-    # ---- end to end through the public autograd API, host buffers
+    # ---- end to end through LOITS(backend="cuda") with host buffers
     e2e = run_e2e(args, spec, dev, rank, world, dist)
 
     # ---- roofline of the dominant kernel
-    f_ms, b_ms = float(np.mean(fwd_ms)), float(np.mean(bwd_ms))
     knots = spec.total_knots
     fwd_bytes = FWD_B_PER_EVENT * valid + FWD_B_PER_KNOT * knots
     bwd_bytes = BWD_B_PER_EVENT * valid + BWD_B_PER_KNOT * knots
@@ -438,6 +459,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     except Exception:
         pass
     precision = precision_report(plan, step, spec) if rank == 0 else None
+    step.graph = None
 
     out = {
         "metric": METRIC, "value": value, "unit": "events/s", "n_gpus": world,
@@ -452,9 +474,11 @@ def run_b200(args, spec, rank, world, dist) -> dict:
                          "inputs smaller than L2: not a valid roofline case",
                    "launch": plan.config, "accepted_events_per_step": valid * world,
                    "tuning_ms_per_step": tune_ms},
-        "plain": {"value": plain_value, "ms_per_step": plain_ms,
+        "plain": {"value": events_step / (plain_ms * 1e-3), "ms_per_step": plain_ms,
                   "form": "one forward + one backward launch per density, no graph",
-                  "batched_over_plain": value / plain_value, "events_identical": bool(same)},
+                  "launch": plain_launch, "tuning_ms_per_step": ptune_ms,
+                  "batched_over_plain": plain_ms / ms, "events_identical": bool(same),
+                  "row_offsets_identical": bool(plain_rows_same)},
         "kernels_ms": {"batch_forward_kernel": f_ms, "batch_backward_kernel": b_ms},
         "saved_state": saved_state,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
@@ -469,6 +493,28 @@ def run_b200(args, spec, rank, world, dist) -> dict:
         "clocks": clocks.summary(),
     }
     return out
+
+
+def run_eager(args, spec) -> dict:
+    """--eager-steps K: K eager forward + backward launches of the persistent
+    form on one GPU at a given geometry, untimed -- the launches a profiler
+    attaches to.  Prints the kept-row count and the resolved launch."""
+    import torch
+
+    dev = torch.device("cuda", 0)
+    torch.cuda.set_device(dev)
+    geom = dict(threads=args.threads, blocks_per_item=args.blocks, scan_knots=args.scan_knots,
+                guide_ratio=args.guide_ratio, plain=1 if args.plain else 0)
+    plan, step = make_step(spec, dev, geom, 0, saved_state=args.saved_state)
+    step.grad_events.normal_(generator=torch.Generator(device=dev).manual_seed(0))
+    for _ in range(args.eager_steps):
+        step.forward()
+        step.backward()
+    torch.cuda.synchronize(dev)
+    step.check_status()
+    return {"workload": spec.name, "eager_steps": args.eager_steps,
+            "events": spec.total_events, "knots": spec.total_knots,
+            "kept": int(step.row_offsets[-1].item()), "launch": plan.config}
 
 
 def precision_report(plan, step, spec, n_check: int = 2) -> dict:
@@ -525,23 +571,23 @@ def precision_report(plan, step, spec, n_check: int = 2) -> dict:
 
 def run_e2e(args, spec, dev, rank, world, dist) -> dict:
     """The user-facing call with host data: pinned host -> device copies of the
-    step's inputs (density values, grid, cotangent), BatchedLOITS.sample +
-    autograd backward, device -> host copies of the events and the gradient.
-    The cotangent's copy in and the events' copy out run on their own streams
-    (opposite PCIe directions) beside the forward; the backward waits for the
-    cotangent and the step ends when events and gradient are on the host."""
+    step's inputs (density values, grid, cut, cotangent),
+    ``LOITS(backend="cuda")(DensityBatch, event_counts)`` + autograd backward,
+    device -> host copies of the events and the gradient.  The cotangent's copy
+    in and the events' copy out run on their own streams (opposite PCIe
+    directions) beside the forward; the backward waits for the cotangent and
+    the step ends when events and gradient are on the host."""
     import torch
 
     from quantom_loits_b200 import batched as B
+    from quantom_loits_b200.loits import LOITS
 
     nmax = int(spec.event_counts.max())
-    sampler = B.BatchedLOITS(dev, seed=spec.seed,
-                             config=B.make_config(**args.geom,
-                                                  density_base=rank * spec.n_densities,
-                                                  slot_stride=nmax))
-    h_vals = torch.from_numpy(spec.values).pin_memory()
-    h_grid = torch.from_numpy(spec.grid).pin_memory()
-    h_cut = None if spec.x_cut is None else torch.from_numpy(spec.x_cut).pin_memory()
+    cfg = B.make_config(**args.geom, density_base=rank * spec.n_densities, slot_stride=nmax)
+    sampler = LOITS(backend="cuda", device=dev, batch_config=cfg)
+    h_vals = torch_from(spec.values).pin_memory()
+    h_grid = torch_from(spec.grid).pin_memory()
+    h_cut = None if spec.x_cut is None else torch_from(spec.x_cut).pin_memory()
     h_cot = torch.randn(spec.total_events, generator=torch.Generator().manual_seed(5)).pin_memory()
     h_events = torch.empty(spec.total_events, dtype=torch.float32).pin_memory()
     h_grad = torch.empty(spec.total_knots, dtype=torch.float32).pin_memory()
@@ -557,7 +603,7 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
         grid = h_grid.to(dev, non_blocking=True)
         cut = None if h_cut is None else h_cut.to(dev, non_blocking=True)
         batch = B.DensityBatch(grid, values, spec.knot_offsets, spec.event_counts, cut)
-        events, rows = sampler.sample(batch, sequence=0)
+        events, rows = sampler(batch, spec.event_counts)
         n = events.shape[0]
         s_out.wait_stream(stream)
         with torch.cuda.stream(s_out):
@@ -589,7 +635,7 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
     d2h = 4 * (n + spec.total_knots)
     return {"value": spec.total_events * world / (ms * 1e-3), "unit": "events/s",
             "ms_per_step": ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
-            "api": "BatchedLOITS.sample + autograd backward"}
+            "api": "LOITS(backend='cuda')(DensityBatch, event_counts) + autograd backward"}
 
 
 def tuple_cpu_baseline(args, spec) -> dict:
@@ -931,12 +977,25 @@ def main(argv=None) -> int:
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
     ap.add_argument("--workload",
-                    choices=["uniform", "single", "ragged", "precision", "tuple", "gan"],
-                    default="uniform")
+                    choices=["ragged", "uniform", "single", "precision", "tuple", "gan"],
+                    default="ragged")
     ap.add_argument("--events", type=int, default=0,
                     help="events per step of the tuple workload (default 1e7)")
-    ap.add_argument("--threads", type=int, default=0)
-    ap.add_argument("--blocks", type=int, default=0)
+    ap.add_argument("--threads", type=int, default=0,
+                    help="threads per CTA of the persistent form (0: tuned)")
+    ap.add_argument("--blocks", type=int, default=0,
+                    help="Philox blocks per thread per tile of the persistent form (0: tuned)")
+    ap.add_argument("--plain-threads", type=int, default=0,
+                    help="threads per CTA of the one-launch-per-density form (0: tuned)")
+    ap.add_argument("--plain-blocks", type=int, default=0,
+                    help="Philox blocks per thread per tile of that form (0: tuned)")
+    ap.add_argument("--scan-knots", type=int, default=0)
+    ap.add_argument("--guide-ratio", type=int, default=0,
+                    help="log2 guide buckets per knot of small densities (0: default)")
+    ap.add_argument("--eager-steps", type=int, default=0,
+                    help="only run this many eager forward + backward launches (for a profiler)")
+    ap.add_argument("--plain", action="store_true", help="--eager-steps: the plain form")
+    ap.add_argument("--saved-state", action="store_true", help="--eager-steps: saved-state form")
     ap.add_argument("--ref-seconds", type=float, default=3.0,
                     help="CPU seconds per reference step (bounded sample)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -948,6 +1007,11 @@ def main(argv=None) -> int:
     world, rank, local = dist_env()
     is_tuple, is_gan = args.workload == "tuple", args.workload == "gan"
     spec = None if is_gan else workload_spec(args.workload, args.events)
+    if args.eager_steps:
+        if is_tuple or is_gan:
+            ap.error("--eager-steps runs the batched workloads")
+        print(json.dumps(run_eager(args, spec)), flush=True)
+        return 0
 
     if args.impl == "reference":
         if rank != 0:

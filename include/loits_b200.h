@@ -105,12 +105,15 @@ int loits_tuple_sample(const loits_shape* shape, const double* x_bins, const dou
  * reference.  For callers that cannot allocate device memory where they
  * sample (a framework that owns the whole GPU through its own memory pool,
  * or a loop that must not allocate after start-up): the look-back scratch is
- * a fixed 512 KiB array inside the library (16 B + 8 B per 1024-slot tile),
- * so `active` may be at most LOITS_TUPLE_NOALLOC_MAX_ACTIVE (67,108,864);
- * more returns LOITS_ERR_CAPACITY without launching.  The first call on a
- * device looks up that array's device address (cudaGetSymbolAddress), so make
- * it before any stream capture.  Every call on a device shares the one array
- * and leaves its contents behind: calls that may overlap on the GPU
+ * a fixed array of 524,304 bytes inside the library (16 B of ticket + 8 B per
+ * 1024-slot tile, 65,536 tiles), so `active` may be at most
+ * LOITS_TUPLE_NOALLOC_MAX_ACTIVE (67,108,864); more returns
+ * LOITS_ERR_CAPACITY without launching.  The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress) and keeps it for the
+ * life of the process's context on that device, so make that call before any
+ * stream capture, and do not call this entry point again on a device whose
+ * context was destroyed (cudaDeviceReset).  Every call on a device shares the
+ * one array and leaves its contents behind: calls that may overlap on the GPU
  * (different streams without ordering between them) race. */
 #define LOITS_TUPLE_NOALLOC_MAX_ACTIVE 67108864
 int loits_tuple_sample_noalloc(const loits_shape* shape, const double* x_bins,
@@ -152,6 +155,9 @@ typedef struct loits_batch_config {
   int32_t scan_knots;      /* knots per thread in the CDF scan: 1..64, default 8 */
   int32_t ctas_per_sm;     /* persistent CTAs per SM (0 = as many as fit) */
   int32_t plain;           /* 1 = one launch per density (no persistent queue) */
+  int32_t guide_ratio;     /* log2 of guide buckets per knot of a small density, 1..6;
+                              0 = 4 (16 buckets per knot), lowered where the guide
+                              would cost resident CTAs */
   int64_t density_base;    /* global index of density 0 of this plan (sharding) */
   int64_t slot_stride;     /* Philox slots per density, >= max n_b (0 = max n_b) */
 } loits_batch_config;

@@ -81,13 +81,15 @@ class DensityBatch:
 
 
 def default_config() -> N.BatchConfig:
-    return N.BatchConfig(0, 0, 0, 0, 0, 0, 0)
+    return N.BatchConfig()
 
 
 def make_config(threads=0, blocks_per_item=0, scan_knots=0, ctas_per_sm=0, plain=0,
-                density_base=0, slot_stride=0) -> N.BatchConfig:
-    return N.BatchConfig(int(threads), int(blocks_per_item), int(scan_knots), int(ctas_per_sm),
-                         int(plain), int(density_base), int(slot_stride))
+                density_base=0, slot_stride=0, guide_ratio=0) -> N.BatchConfig:
+    return N.BatchConfig(threads=int(threads), blocks_per_item=int(blocks_per_item),
+                         scan_knots=int(scan_knots), ctas_per_sm=int(ctas_per_sm),
+                         plain=int(plain), guide_ratio=int(guide_ratio),
+                         density_base=int(density_base), slot_stride=int(slot_stride))
 
 
 class BatchPlan:

@@ -17,9 +17,11 @@ namespace loits_dev {
 //             (c_{k+1} - c_k + 1e-5) (0 on the last knot);
 //   invd[k] = 1 / (c_{k+1} - c_k + 1e-5), the backward's weight of interval k;
 //   guide   = per density with a non-decreasing CDF, M = 2^m buckets of
-//             u: L[k] = number of knots with c_t <= k / M (M < 2G when
-//             shared memory or the large-density cap limits it), so the interval of
-//             u in [k/M, (k+1)/M) is found among knots [L[k], L[k+1]].
+//             u: L[k] = number of knots with c_t <= k / M (M >= 16 G where
+//             shared memory allows; fewer when it or the large-density cap
+//             limits it), so the interval of u in [k/M, (k+1)/M) is found
+//             among knots [L[k], L[k+1]]; small densities also keep it
+//             packed (pack_entry) for sampling from shared memory.
 //
 // Densities of at most `gcap` knots are sampled from shared memory (records
 // and packed guide copied per tile); larger ones ("large densities", more
@@ -80,7 +82,8 @@ struct BatchArgs {
   float4* rec;
   float* invd;
   uint32_t* gl;                // per density: L[k] = #{t : c_t <= k / M}, k = 0..M
-  uint32_t* gpk;               // per small density: L[k] | L[k+1] << 16, k = 0..M-1
+  uint32_t* gpk;               // per small density: packed entries (first interval of
+                               // bucket k | movable knots << 16), k = 0..M-1
   double* norm;
   uint32_t* dflags;            // bit 0: CDF not non-decreasing (count semantics)
   uint32_t* cdf_ready;         // 1 once a density's records and packed guide are final

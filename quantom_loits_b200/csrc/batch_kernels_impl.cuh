@@ -248,19 +248,32 @@ __device__ __forceinline__ uint32_t threshold_flag(const BatchArgs& a, int b, in
   return kThreshold;
 }
 
-// Pack small density b's guide for sampling from shared memory: gpk[k] =
-// L[k] | L[k+1] << 16 (counts of a small density fit 16 bits).  Every L entry
-// was written (and fenced) before this runs.  Large densities are sampled
-// from L itself.
+// Packed guide entry of a small density (G <= 8192 knots) for the bucket
+// whose counts are [lo, hi] (lo = L[k] >= 1, hi = L[k+1]): the interval the
+// bucket starts in, ja = lo - 1, and the number of knots inside the bucket
+// that can still move the interval, span = min(hi, G - 1) - lo (a count past
+// G - 1 only moves past the last interval, which the interval clamp undoes).
+// Interval of u in the bucket: ja + #{t in [lo, lo + span) : key_t <= u}.
+// Clamps make every entry safe (ja + span <= G - 2) whatever L holds.
+__device__ __forceinline__ uint32_t pack_entry(uint32_t lo, uint32_t hi, int G) {
+  const int l = static_cast<int>(lo), h = min(static_cast<int>(hi), G - 1);
+  const int ja = max(min(l - 1, G - 2), 0);
+  const int span = max(h - (ja + 1), 0);
+  return static_cast<uint32_t>(ja) | (static_cast<uint32_t>(span) << 16);
+}
+
+// Pack small density b's guide for sampling from shared memory:
+// gpk[k] = pack_entry(L[k], L[k+1]).  Every L entry was written (and fenced)
+// before this runs.  Large densities are sampled from L itself.
 template <int TPB>
 __device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
   const int64_t po = __ldg(&a.pkoff[b]);
   if (po < 0) return;
   const int M = 1 << __ldg(&a.gbits[b]);
+  const int G = static_cast<int>(__ldg(&a.knot_off[b + 1]) - __ldg(&a.knot_off[b]));
   const uint32_t* L = a.gl + __ldg(&a.goff[b]);
   uint32_t* P = a.gpk + po;
-  for (int k = threadIdx.x; k < M; k += TPB)
-    P[k] = __ldcg(&L[k]) | (__ldcg(&L[k + 1]) << 16);
+  for (int k = threadIdx.x; k < M; k += TPB) P[k] = pack_entry(__ldcg(&L[k]), __ldcg(&L[k + 1]), G);
   __threadfence();
 }
 
@@ -638,7 +651,7 @@ struct SampleShared {
   uint32_t flags;
   float cut;
   float fix_scale;   // backward chunk: fixed-point units per cotangent unit
-  int nonfinite;     // backward chunk: a non-finite contribution was seen
+  float fix_cap;     // backward chunk: largest scaled term a fixed-point sum takes
   int win_b;         // density whose fixed-point window win_lo belongs to
   int win_lo;
   int run_k0;        // most_probable_run's result
@@ -702,8 +715,9 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
       // every 2^s-th count: the guide with 2^s-times wider buckets
       const int sft = m_full - m;
       const uint32_t* L = a.gl + __ldg(&a.goff[b]);
+      const int Gi = static_cast<int>(G);
       for (int k = threadIdx.x; k < (1 << m); k += blockDim.x)
-        guide_s[k] = __ldcg(&L[k << sft]) | (__ldcg(&L[(k + 1) << sft]) << 16);
+        guide_s[k] = pack_entry(__ldcg(&L[k << sft]), __ldcg(&L[(k + 1) << sft]), Gi);
     }
     v.rec = rec_s;
     v.guide = guide_s;
@@ -774,6 +788,30 @@ __device__ __forceinline__ void pick_interval(const float4* rec, int G, float u,
   }
 }
 
+// Interval of u from a small density's packed guide entry (pack_entry), the
+// records in shared memory: one key load and compare move u from the
+// bucket's first interval to the next (always in bounds: ja + 1 <= G - 1);
+// only a bucket with two or more movable knots -- rare with M >= 16 G
+// buckets -- finishes with a binary search.  The record itself is loaded
+// once, after the interval is known.
+__device__ __forceinline__ int pick_packed(const float4* rec, uint32_t pk, float u) {
+  const float* keys = reinterpret_cast<const float*>(rec);
+  const int ja = static_cast<int>(pk & 0xffffu);
+  const int span = static_cast<int>(pk >> 16);
+  const bool step = (span > 0) & (u >= keys[4 * (ja + 1)]);
+  int j = ja + (step ? 1 : 0);
+  if (step & (span >= 2)) {
+    // first key above u among knots [ja + 2, ja + 1 + span)
+    int l = ja + 2, h = ja + 1 + span;
+    while (l < h) {
+      const int mid = (l + h) >> 1;
+      if (u >= keys[4 * mid]) l = mid + 1; else h = mid;
+    }
+    j = l - 1;
+  }
+  return j;
+}
+
 template <int kMode>
 __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
   const float u = uniform_from_bits(bits);
@@ -783,9 +821,8 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
     j = interval_count_all(d.rec, u, d.G);
     r = d.rec[j];
   } else if constexpr (kMode == kShared) {
-    const uint32_t pk = d.guide[bits >> d.shift];
-    pick_interval<kShared>(d.rec, d.G, u, static_cast<int>(pk & 0xffffu),
-                           static_cast<int>(pk >> 16), j, r);
+    j = pick_packed(d.rec, d.guide[bits >> d.shift], u);
+    r = d.rec[j];
   } else if constexpr (kMode == kL2) {
     // forward, large density: when the coarse bucket's knots all lie in the
     // shared window [wk0, wk1), search there; otherwise the full guide and
@@ -1376,13 +1413,20 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
 //  * large densities: the same fixed-point sums for the intervals of a window
 //    [win_lo, win_lo + win_n) (the most probable ones), one float2 global
 //    atomic per kept slot for the others (gc).
+// A fixed-point term is added only while its scaled magnitude stays below
+// cap = 2^63 / (the chunk's kept rows), so that no sum of the chunk can wrap
+// its 64 bits; a larger (or non-finite) cotangent's terms take the fp32 path
+// instead, as global fp32 reductions: into the chunk's partial (`spill`,
+// zeroed when the chunk starts and added to the fixed-point sums when it
+// ends) for small densities, into gc for large ones.  Non-finite values
+// therefore reach the gradient as they would through fp32 sums.
 struct Acc {
   float* gacc;
   uint32_t *alo, *ahi, *blo, *bhi;
   float2* gc;
-  float scale;
+  float* spill;
+  float scale, cap;
   int win_lo, win_n;
-  int* nonfinite;
 };
 
 // Fixed-point value of f (already scaled): f rounded to an integer.
@@ -1406,18 +1450,15 @@ __device__ __forceinline__ double fix_value(uint32_t lo, uint32_t hi, double inv
                                                     lo)) * inv_scale;
 }
 
-// One kept slot's (g, g w) into fixed-point slot i.  Values whose scaled
-// magnitude reaches 2^63 (non-finite cotangents among them) are not added;
-// they mark the chunk, whose gradient then becomes NaN, as any non-finite
-// cotangent makes the reference's (its normaliser VJP sums over every knot).
-__device__ __forceinline__ void fix_pair(const Acc& acc, int i, float g, float w) {
+// One kept slot's (g, g w) into fixed-point slot i, when both scaled terms
+// are below the chunk's cap (false: nothing added, the caller takes the fp32
+// path).
+__device__ __forceinline__ bool fix_pair(const Acc& acc, int i, float g, float w) {
   const float f0 = g * acc.scale, f1 = (g * w) * acc.scale;
-  if (!(fabsf(f0) < 9.0e18f) || !(fabsf(f1) < 9.0e18f)) {
-    *acc.nonfinite = 1;
-    return;
-  }
+  if (!(fabsf(f0) < acc.cap) || !(fabsf(f1) < acc.cap)) return false;
   fix_add(acc.alo, acc.ahi, i, fix_round(f0));
   fix_add(acc.blo, acc.bhi, i, fix_round(f1));
+  return true;
 }
 
 __device__ __forceinline__ void red_add_f32x2(float2* p, float x, float y) {
@@ -1437,7 +1478,11 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
   const float w = e.t * inv;
   if constexpr (kMode == kShared) {
     if constexpr (kFix) {
-      fix_pair(acc, e.j, g, w);
+      if (!fix_pair(acc, e.j, g, w)) {
+        const float mg = e.m * g;
+        atomicAdd(&acc.spill[e.j], mg * (w - 1.0f));  // no return value: a reduction
+        atomicAdd(&acc.spill[e.j + 1], -(mg * w));
+      }
     } else {
       const float mg = e.m * g;
       atomicAdd(&acc.gacc[e.j], mg * (w - 1.0f));
@@ -1445,9 +1490,7 @@ __device__ __forceinline__ void scatter_slot(const Slot& e, float g, const DensV
     }
   } else {
     const unsigned wj = static_cast<unsigned>(e.j - acc.win_lo);
-    if (wj < static_cast<unsigned>(acc.win_n)) {
-      fix_pair(acc, static_cast<int>(wj), g, w);
-    } else {
+    if (!(wj < static_cast<unsigned>(acc.win_n) && fix_pair(acc, static_cast<int>(wj), g, w))) {
       const float mg = e.m * g;
       red_add_f32x2(&acc.gc[e.j], mg * (w - 1.0f), -(mg * w));
     }
@@ -1615,11 +1658,13 @@ constexpr bool kFixPaths = TPB >= 512;
 // Fixed-point scale of a backward chunk (into sh.fix_scale): a power of two
 // that puts the mean |cotangent| of up to TPB of the chunk's kept rows near
 // 2^20, so one unit is about 1e-6 of a typical contribution; larger values
-// take more bits (up to 2^63).  Histogram mode: the mean histogram-cotangent
-// step instead.  Ends with a barrier.
+// take more bits.  Histogram mode: the mean histogram-cotangent step
+// instead.  sh.fix_cap = 2^62 / rows (rounded down to a power of two): `rows`
+// terms below it cannot wrap a 64-bit sum (rows: the chunk's kept rows, or
+// in histogram mode its slots).  Ends with a barrier.
 template <int TPB>
 __device__ __forceinline__ void chunk_scale(const BatchArgs& a, const float* gh, int64_t r0,
-                                            int64_t r1, SampleShared& sh) {
+                                            int64_t r1, int64_t rows, SampleShared& sh) {
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   float v = 0.0f, c = 0.0f;
   if (gh) {
@@ -1647,7 +1692,8 @@ __device__ __forceinline__ void chunk_scale(const BatchArgs& a, const float* gh,
     if (cnt > 0 && sum > 0.0f) frexpf(sum / cnt, &e);
     e = min(max(e, -100), 100);
     sh.fix_scale = ldexpf(1.0f, 20 - e);
-    sh.nonfinite = 0;
+    const int lg = rows > 1 ? 64 - __clzll(static_cast<unsigned long long>(rows - 1)) : 0;
+    sh.fix_cap = ldexpf(1.0f, 62 - lg);
   }
   __syncthreads();
 }
@@ -1695,8 +1741,10 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   // the chunk's kept rows (event modes): [tile_prefix[t_first], tile_prefix[t_end])
   const int64_t r0 = gh ? 0 : __ldcg(&a.tile_prefix[t_first]);
   const int64_t r1 = gh ? 0 : __ldcg(&a.tile_prefix[t_end]);
+  // an upper bound on the chunk's kept rows (histogram mode: its slots)
+  const int64_t chunk_rows =
+      gh ? static_cast<int64_t>(t_end - t_first) * TPB * R * 4 : r1 - r0;
   Acc acc{};
-  acc.nonfinite = &sh.nonfinite;
   if (kLarge && tg.G > a.gcap) {
     const DensView d = load_density(a, b, tg.k0, tg.G, true, nullptr, guide_s, nullptr, false,
                                     sh, guide_key);
@@ -1707,12 +1755,13 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       if (sh.win_b != b) large_window<TPB>(a, d, b, sh);
       uint32_t* base = reinterpret_cast<uint32_t*>(rec_s);
       for (int i = threadIdx.x; i < 4 * a.win_n; i += TPB) base[i] = 0u;
-      chunk_scale<TPB>(a, gh, r0, r1, sh);
+      chunk_scale<TPB>(a, gh, r0, r1, chunk_rows, sh);
       acc.alo = base;
       acc.ahi = base + a.win_n;
       acc.blo = base + 2 * a.win_n;
       acc.bhi = base + 3 * a.win_n;
       acc.scale = sh.fix_scale;
+      acc.cap = sh.fix_cap;
       acc.win_lo = sh.win_lo;
       acc.win_n = a.win_n;
     }
@@ -1720,17 +1769,13 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
     if (win) {
       __syncthreads();
       const double inv_scale = 1.0 / static_cast<double>(acc.scale);
-      if (sh.nonfinite) {
-        if (threadIdx.x == 0) red_add_f32x2(&acc.gc[acc.win_lo], __int_as_float(0x7fc00000), 0.0f);
-      } else {
-        for (int i = threadIdx.x; i < a.win_n; i += TPB) {
-          if ((acc.alo[i] | acc.ahi[i] | acc.blo[i] | acc.bhi[i]) == 0u) continue;
-          const int j = acc.win_lo + i;
-          const double A = fix_value(acc.alo[i], acc.ahi[i], inv_scale);
-          const double Bs = fix_value(acc.blo[i], acc.bhi[i], inv_scale);
-          const double m = static_cast<double>(__ldg(reinterpret_cast<const float*>(d.rec + j) + 3));
-          red_add_f32x2(&acc.gc[j], static_cast<float>(m * (Bs - A)), static_cast<float>(-m * Bs));
-        }
+      for (int i = threadIdx.x; i < a.win_n; i += TPB) {
+        if ((acc.alo[i] | acc.ahi[i] | acc.blo[i] | acc.bhi[i]) == 0u) continue;
+        const int j = acc.win_lo + i;
+        const double A = fix_value(acc.alo[i], acc.ahi[i], inv_scale);
+        const double Bs = fix_value(acc.blo[i], acc.bhi[i], inv_scale);
+        const double m = static_cast<double>(__ldg(reinterpret_cast<const float*>(d.rec + j) + 3));
+        red_add_f32x2(&acc.gc[j], static_cast<float>(m * (Bs - A)), static_cast<float>(-m * Bs));
       }
     }
     // the density's grad-CDF atomics are performed before the chunk counts
@@ -1767,17 +1812,21 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       __syncthreads();
       for (int i = threadIdx.x; i < G; i += TPB) __stcg(&part[i], gacc[i]);
     } else {
+      // the chunk's partial takes the fp32 reductions of terms above the cap
       for (int i = threadIdx.x; i < 4 * G; i += TPB) base[i] = 0u;
-      chunk_scale<TPB>(a, gh, r0, r1, sh);
+      for (int i = threadIdx.x; i < G; i += TPB) __stcg(&part[i], 0.0f);
+      chunk_scale<TPB>(a, gh, r0, r1, chunk_rows, sh);
       acc.alo = base;
       acc.ahi = base + G;
       acc.blo = base + 2 * G;
       acc.bhi = base + 3 * G;
       acc.scale = sh.fix_scale;
+      acc.cap = sh.fix_cap;
+      acc.spill = part;
       vjp_chunk_tiles<TPB, R, kShared, true>(a, d, tg, tb, t_first, t_end, acc, gh);
+      __threadfence();
       __syncthreads();
       const double inv_scale = 1.0 / static_cast<double>(acc.scale);
-      const bool bad = sh.nonfinite != 0;
       for (int i = threadIdx.x; i < G; i += TPB) {
         // gcdf_i = m_i (B_i - A_i) - m_{i-1} B_{i-1} (no interval starts at knot G-1)
         double v = 0.0;
@@ -1787,7 +1836,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
         if (i > 0)
           v -= static_cast<double>(rec_f[i - 1].w) *
                fix_value(acc.blo[i - 1], acc.bhi[i - 1], inv_scale);
-        __stcg(&part[i], bad ? __int_as_float(0x7fc00000) : static_cast<float>(v));
+        __stcg(&part[i], static_cast<float>(v + static_cast<double>(__ldcg(&part[i]))));
       }
     }
   } else {

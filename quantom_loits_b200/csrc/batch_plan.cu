@@ -136,6 +136,16 @@ constexpr size_t kSmemLimit = 227 * 1024;
 
 int default_blocks(int threads) { return threads == 1024 ? 8 : 16; }
 
+// Guide buckets per knot of a small density, as log2: M >= 2^ratio G buckets
+// where shared memory allows without lowering the CTAs an SM holds.  Finer
+// buckets hold fewer knots, so fewer slots need more than one key compare:
+// with 16 G buckets about 0.2 % of the benchmark densities' slots search,
+// against 3 % with 2 G (and a warp waits for its slowest lane).
+constexpr int kDefaultGuideRatio = 4;
+constexpr int kMaxGuideRatio = 6;
+// Most guide bits a small density's packed guide takes in shared memory.
+constexpr int kMaxSmallGuideBits = 15;
+
 // Validates a configuration; threads == 0 (choose by occupancy) and
 // blocks_per_item == 0 (default for the thread count) stay unresolved.
 int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
@@ -149,6 +159,8 @@ int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
   if (out.scan_knots < 1 || out.scan_knots > 64) return LOITS_ERR_INVALID;
   if (out.ctas_per_sm < 0 || out.ctas_per_sm > 32) return LOITS_ERR_INVALID;
   if (out.plain != 0 && out.plain != 1) return LOITS_ERR_INVALID;
+  if (out.guide_ratio < 0 || out.guide_ratio > kMaxGuideRatio) return LOITS_ERR_INVALID;
+  if (out.guide_ratio == 0) out.guide_ratio = kDefaultGuideRatio;
   if (out.density_base < 0 || out.slot_stride < 0) return LOITS_ERR_INVALID;
   return LOITS_OK;
 }
@@ -188,15 +200,17 @@ struct SmemGeometry {
 constexpr size_t kSmemPerSM = 228 * 1024;
 constexpr size_t kSmemPerCtaReserved = 1024;
 
-// Guide bits of a density of g knots: M = 2^m buckets, 2g <= M, at most 2^cap.
-int guide_bits(int64_t g, int cap) {
+// Guide bits of a density of g knots: M = 2^m buckets, 2^ratio g <= M, at
+// most 2^cap.
+int guide_bits(int64_t g, int cap, int ratio) {
   int m = 2;
-  while ((int64_t(1) << m) < 2 * g && m < cap) ++m;
+  while ((int64_t(1) << m) < (g << ratio) && m < cap) ++m;
   return m;
 }
 
 // large_g: knots of the largest density above the shared-memory limit (0: none).
-int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, SmemGeometry& g) {
+int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, int ratio,
+                  SmemGeometry& g) {
   const bool large = large_g > 0;
   FwdKernel fk;
   BwdKernel bk;
@@ -222,17 +236,11 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
       --mc;
     return mc;
   };
-  g.m_cap = cap_for(fwd_knots, 14);
+  g.m_cap = cap_for(fwd_knots, kMaxSmallGuideBits);
   g.m_cap_b = cap_for(bwd_knots, g.m_cap);
-  int m = 2;
-  while ((int64_t(1) << m) < 2 * max_g && m < g.m_cap) ++m;
-  g.mcap = static_cast<int32_t>(int64_t(1) << m);
-  const int32_t mcap_b = std::min<int32_t>(g.mcap, int32_t(1) << g.m_cap_b);
-  // sampling CTAs hold the guide as packed (L[k], L[k+1]) pairs: M uint32;
+  // sampling CTAs hold the guide as packed entries (pack_entry): M uint32;
   // kept events are staged in global memory, not here
   auto gbytes = [](int32_t entries) { return static_cast<size_t>((entries + 7) & ~7) * sizeof(uint32_t); };
-  const size_t guide_f = gbytes(g.mcap);
-  size_t guide_b = gbytes(mcap_b);
   // CTAs per SM that `bytes` of dynamic shared memory allow (at most the
   // register cap's 1280 / tpb)
   auto resident = [&](size_t bytes) {
@@ -240,6 +248,24 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
     while (c > 1 && c * (bytes + g.static_smem + kSmemPerCtaReserved) > kSmemPerSM) --c;
     return c;
   };
+  // the largest small density's guide: 2^ratio buckets per knot, unless that
+  // holds fewer CTAs per SM than 2 buckets per knot would (in the forward
+  // with records beside it; in the backward with records, weights and sums)
+  const int m1 = guide_bits(max_g, g.m_cap, 1);
+  int m = guide_bits(max_g, g.m_cap, ratio);
+  while (m > m1 && resident(fwd_knots + gbytes(1 << m)) < resident(fwd_knots + gbytes(1 << m1))) --m;
+  g.m_cap = m;  // every small density's guide takes at most this many bits
+  g.mcap = static_cast<int32_t>(int64_t(1) << m);
+  const int mb1 = std::min(g.m_cap_b, m1);
+  int mb = std::min(g.m_cap_b, m);
+  const size_t bwd_fix = static_cast<size_t>(gcap) * (sizeof(float4) + 5 * sizeof(float));
+  while (mb > mb1 && resident(std::max(bwd_knots, tpb >= 512 ? bwd_fix : 0) + gbytes(1 << mb)) <
+                         resident(std::max(bwd_knots, tpb >= 512 ? bwd_fix : 0) + gbytes(1 << mb1)))
+    --mb;
+  g.m_cap_b = mb;
+  const int32_t mcap_b = std::min<int32_t>(g.mcap, int32_t(1) << g.m_cap_b);
+  const size_t guide_f = gbytes(g.mcap);
+  size_t guide_b = gbytes(mcap_b);
   // Backward small-density slot: records, weights and either fp32 grad-CDF
   // sums (4 bytes per knot) or the fixed-point sums A, B (16 bytes per
   // knot).  Fixed point is used when it costs neither residency nor guide
@@ -276,7 +302,7 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
     // a copy more than 16 times coarser than the largest guide costs more
     // search steps than it saves: the full guide is read in place instead
     // (and the window, found on the coarse copy, is not used)
-    g.lbits_b = lb >= guide_bits(large_g, kMaxLargeGuideBits) - 4 ? lb : 0;
+    g.lbits_b = lb >= guide_bits(large_g, kMaxLargeGuideBits, 1) - 4 ? lb : 0;
     if (g.lbits_b > 0) {
       guide_b = std::max(guide_b, bytes(lb));
       g.win_n = static_cast<int32_t>(win_bytes / 16);
@@ -334,12 +360,13 @@ void occupancy(int tpb, int r, bool large, const SmemGeometry& g, int& occ_f, in
 
 // CTA size with the most resident threads per SM for both kernels (the
 // smaller CTA on a tie: fewer threads wait at each tile barrier).
-int choose_threads(int r_req, int64_t large_g, int32_t gcap, int64_t max_g, int& tpb_out) {
+int choose_threads(int r_req, int64_t large_g, int32_t gcap, int64_t max_g, int ratio,
+                   int& tpb_out) {
   int best = -1, best_tpb = 0, last_rc = LOITS_ERR_UNSUPPORTED;
   for (int tpb : {256, 512, 1024}) {
     const int r = r_req ? r_req : default_blocks(tpb);
     SmemGeometry g;
-    const int rc = smem_geometry(tpb, r, large_g, gcap, max_g, g);
+    const int rc = smem_geometry(tpb, r, large_g, gcap, max_g, ratio, g);
     if (rc != LOITS_OK) {
       last_rc = rc;
       continue;
@@ -470,7 +497,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   // ---- launch geometry: the CTA size (by occupancy unless given)
   if (c.threads == 0) {
     int tpb = 0;
-    rc = choose_threads(c.blocks_per_item, large_g, p->gcap, p->small_max_g, tpb);
+    rc = choose_threads(c.blocks_per_item, large_g, p->gcap, p->small_max_g, c.guide_ratio,
+                        tpb);
     if (rc != LOITS_OK) { delete p; return rc; }
     c.threads = tpb;
   }
@@ -479,7 +507,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->tpb = c.threads;
   p->r = c.blocks_per_item;
   SmemGeometry sg;
-  rc = smem_geometry(p->tpb, p->r, large_g, p->gcap, p->small_max_g, sg);
+  rc = smem_geometry(p->tpb, p->r, large_g, p->gcap, p->small_max_g, c.guide_ratio, sg);
   if (rc != LOITS_OK) { delete p; return rc; }
   // ---- work items
   const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;
@@ -530,7 +558,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   for (int64_t b = 0; b < n_densities; ++b) {
     const int64_t g = p->koff[b + 1] - p->koff[b];
     const bool large = g > p->gcap;
-    const int m = guide_bits(g, large ? kMaxLargeGuideBits : sg.m_cap);
+    const int m = large ? guide_bits(g, kMaxLargeGuideBits, 1) : guide_bits(g, sg.m_cap, c.guide_ratio);
     p->gbits[b] = m;
     p->goff[b] = go;
     go += ((int64_t(1) << m) + 1 + 7) & ~int64_t(7);

@@ -561,7 +561,9 @@ extern "C" int loits_tuple_prepare(const loits_shape* shape, const double* x_bin
 }
 
 extern "C" size_t loits_tuple_sample_workspace(int64_t active) {
-  const int64_t tiles = (active + kSampleTile - 1) / kSampleTile;
+  if (active <= 0) return 16;
+  // whole tiles, formed without overflow for any positive active
+  const int64_t tiles = active / kSampleTile + (active % kSampleTile != 0 ? 1 : 0);
   return 16 + static_cast<size_t>(tiles) * sizeof(unsigned long long);
 }
 
@@ -759,7 +761,10 @@ void* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
 // Device address of the scratch array on the current device.  In host code
 // the array's name is a host-side stand-in, not a device address, so the
-// address is looked up once per device (with that device current) and kept.
+// address is looked up once per device (with that device current) and kept
+// for the life of the process's context on that device: a process that
+// destroys that context (cudaDeviceReset) must not call this entry point on
+// the device again, since the kept address would be stale.
 int noalloc_scratch(void** out) {
   int dev = -1;
   if (cudaGetDevice(&dev) != cudaSuccess) return LOITS_ERR_CUDA;
@@ -785,7 +790,9 @@ extern "C" int loits_tuple_sample_noalloc(const loits_shape* shape, const double
                                           int16_t* interval_x, int16_t* interval_q,
                                           int64_t* valid, int32_t* status, void* stream) {
   if (active < 0) return LOITS_ERR_INVALID;
-  if (loits_tuple_sample_workspace(active) > kNoAllocScratchBytes) return LOITS_ERR_CAPACITY;
+  if (active > LOITS_TUPLE_NOALLOC_MAX_ACTIVE ||
+      loits_tuple_sample_workspace(active) > kNoAllocScratchBytes)
+    return LOITS_ERR_CAPACITY;
   void* scratch = nullptr;
   const int rc = noalloc_scratch(&scratch);
   if (rc != LOITS_OK) return rc;

@@ -110,7 +110,9 @@ def gather_batch(events, row_offsets, group=None):
     """The unsplit batch on every rank, for a consumer that needs all of it:
     (events, row_offsets) of the whole batch from each rank's kept rows and
     its densities' row offsets (ranks hold contiguous density ranges in rank
-    order).  One all_gather of the row counts, one of the events (padded to
+    order).  ``events`` may be longer than the rank's kept rows (the plan's
+    capacity-sized buffer): its first ``row_offsets[-1]`` entries are the
+    rows.  One all_gather of the row counts, one of the events (padded to
     the largest rank's count) and one of the row offsets (padded to the most
     densities); over NCCL on GPU tensors, gloo on host tensors."""
     import torch
@@ -118,8 +120,11 @@ def gather_batch(events, row_offsets, group=None):
 
     world = dist.get_world_size(group)
     dev = _collective_device()
-    ev = events.to(dev).contiguous()
     ro = row_offsets.to(device=dev, dtype=torch.int64).contiguous()
+    kept = int(ro[-1].item()) if ro.numel() else 0
+    if kept > events.numel():
+        raise ValueError(f"row_offsets end at row {kept} but events holds {events.numel()} rows")
+    ev = events.reshape(-1)[:kept].to(dev).contiguous()
     sizes = torch.tensor([ev.numel(), ro.numel()], dtype=torch.int64, device=dev)
     all_sizes = [torch.zeros(2, dtype=torch.int64, device=dev) for _ in range(world)]
     dist.all_gather(all_sizes, sizes, group=group)

@@ -2,8 +2,9 @@
 
 The batched kernels take three launch parameters (``loits_batch_config``):
 threads per CTA (256, 512, 1024), Philox blocks per thread per sampling tile
-(2, 4, 8, 16) and knots per thread in the CDF
-scan.  Which is fastest depends on the batch: the largest density decides
+(2, 4, 8, 16) and knots per thread in the CDF scan.  ``base`` fixes other
+fields for every candidate (``plain=1`` tunes the one-launch-per-density
+form, with ``PLAIN_CANDIDATES``).  Which is fastest depends on the batch: the largest density decides
 how much shared memory a CTA holds (hence how many CTAs fit on an SM), the
 event counts decide how many tiles there are to balance, and the cut decides
 whether the identity compaction applies.  Without tuning, the plan picks the
@@ -31,11 +32,19 @@ import torch
 
 from . import _native as N
 
-# (threads, blocks_per_item, scan_knots)
+# (threads, blocks_per_item, scan_knots) of the persistent form
 CANDIDATES = (
     (256, 16, 8), (256, 8, 8), (256, 4, 8),
-    (512, 16, 8), (512, 8, 8),
-    (1024, 16, 8), (1024, 8, 8), (1024, 4, 8), (1024, 8, 16),
+    (512, 16, 8), (512, 8, 8), (512, 16, 16), (512, 4, 8),
+    (1024, 16, 8), (1024, 8, 8), (1024, 4, 8), (1024, 16, 16), (1024, 8, 16), (1024, 16, 4),
+)
+
+# The one-launch-per-density form runs each density on its own: smaller tiles
+# give a density of 1e4 - 1e6 events more CTAs to fill the GPU with.
+PLAIN_CANDIDATES = (
+    (256, 2, 8), (256, 4, 8), (256, 8, 8), (256, 16, 8),
+    (512, 2, 8), (512, 4, 8), (512, 8, 8),
+    (1024, 2, 8), (1024, 4, 8), (1024, 8, 8), (1024, 16, 8),
 )
 
 
@@ -55,9 +64,11 @@ class Autotuner:
     timing forward + backward on the batch being sampled."""
 
     def __init__(self, device="cuda", candidates=CANDIDATES, reps: int = 3,
-                 cache_path: str | os.PathLike | None = None):
+                 cache_path: str | os.PathLike | None = None, base: dict | None = None):
         self.device = torch.device(device)
         self.candidates = tuple(candidates)
+        # fields every candidate shares (e.g. plain=1, guide_ratio)
+        self.base = dict(base or {})
         self.reps = max(1, int(reps))
         path = cache_path if cache_path is not None else os.environ.get("LOITS_TUNE_CACHE")
         self.cache_path = Path(path) if path else None
@@ -77,6 +88,8 @@ class Autotuner:
         (bins, lo, hi) to time the histogram mode instead of event writing."""
         counts = batch.event_counts if event_counts is None else np.asarray(event_counts, np.int64)
         key = shape_key(batch.knot_offsets, counts, batch.x_cut is not None)
+        for k in sorted(self.base):
+            key += f"-{k}{self.base[k]}"
         if hist is not None:
             key += f"-hist{int(hist[0])}"
         with self._lock:
@@ -109,8 +122,9 @@ class Autotuner:
             label = f"{threads}x{blocks}/{scan}"
             try:
                 plan = BatchPlan(batch.knot_offsets, counts,
-                                 make_config(threads=threads, blocks_per_item=blocks,
-                                             scan_knots=scan), self.device)
+                                 make_config(**{**self.base, "threads": threads,
+                                                "blocks_per_item": blocks, "scan_knots": scan}),
+                                 self.device)
             except RuntimeError:
                 continue  # geometry not supported for this shape (shared memory)
             events, rows, ws = plan.new_events(), plan.new_row_offsets(), plan.new_workspace()
@@ -148,7 +162,7 @@ class Autotuner:
             times[label] = ms
             if ms < best_ms:
                 best_ms = ms
-                best = dict(threads=threads, blocks_per_item=blocks, scan_knots=scan)
+                best = dict(self.base, threads=threads, blocks_per_item=blocks, scan_knots=scan)
             del plan, events, rows, ws
         if best is None:
             raise RuntimeError("no launch geometry of the batched sampler fits this batch")

@@ -219,44 +219,3 @@ def cotangent(n: int, seed: int = 0) -> np.ndarray:
     """Upstream cotangent ~ N(0, 1) of n events (fp32), from a fixed seed."""
     gen = torch.Generator().manual_seed(seed)
     return torch.randn(n, generator=gen, dtype=torch.float32).numpy()
-
-
-def run(name: str, steps: int = 3, threads: int = 0, blocks_per_item: int = 0,
-        device: str = "cuda:0") -> dict:
-    """Eager forward + backward steps of a named workload on one GPU (the
-    launches a profiler attaches to): each step is one forward launch and one
-    backward launch of the batched kernels.  Returns the kept-row count and
-    the device status of the last step."""
-    from . import batched as B
-
-    spec = WORKLOADS[name]()
-    dev = torch.device(device)
-    cfg = B.make_config(threads=threads, blocks_per_item=blocks_per_item)
-    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev)
-    step = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None)
-    step.grid.copy_(torch.from_numpy(spec.grid))
-    step.values.copy_(torch.from_numpy(spec.values))
-    if spec.x_cut is not None:
-        step.x_cut.copy_(torch.from_numpy(spec.x_cut))
-    step.grad_events.normal_(generator=torch.Generator(device=dev).manual_seed(0))
-    for _ in range(steps):
-        step.forward()
-        step.backward()
-    torch.cuda.synchronize(dev)
-    step.check_status()
-    return {"workload": name, "steps": steps, "events": spec.total_events,
-            "knots": spec.total_knots, "kept": int(step.row_offsets[-1].item()),
-            "launch": plan.config}
-
-
-if __name__ == "__main__":
-    import argparse
-    import json
-
-    ap = argparse.ArgumentParser(description="forward + backward steps of a named workload")
-    ap.add_argument("--workload", choices=sorted(WORKLOADS), default="uniform")
-    ap.add_argument("--steps", type=int, default=3)
-    ap.add_argument("--threads", type=int, default=0)
-    ap.add_argument("--blocks", type=int, default=0)
-    a = ap.parse_args()
-    print(json.dumps(run(a.workload, a.steps, a.threads, a.blocks)))

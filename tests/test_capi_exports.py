@@ -85,11 +85,15 @@ def test_batch_plan_rejects_bad_tables_on_host(native):
     rc, _ = _plan(native, [0, 2**28 + 1], [5])
     assert rc == native.LOITS_ERR_UNSUPPORTED
     # slot stride smaller than the largest event count
-    cfg = native.BatchConfig(0, 0, 0, 0, 0, 0, 3)
+    cfg = native.BatchConfig(slot_stride=3)
     rc, _ = _plan(native, [0, 3, 5], [10, 2], cfg)
     assert rc == native.LOITS_ERR_INVALID
     # unsupported launch geometry
-    cfg = native.BatchConfig(128, 0, 0, 0, 0, 0, 0)
+    cfg = native.BatchConfig(threads=128)
+    rc, _ = _plan(native, [0, 3], [10], cfg)
+    assert rc == native.LOITS_ERR_INVALID
+    # guide resolution out of range
+    cfg = native.BatchConfig(guide_ratio=7)
     rc, _ = _plan(native, [0, 3], [10], cfg)
     assert rc == native.LOITS_ERR_INVALID
 

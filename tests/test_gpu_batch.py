@@ -599,3 +599,34 @@ def test_non_finite_cotangent_poisons_only_its_density(B, threads):
         o, e = koff[b], koff[b + 1]
         assert np.isfinite(d[o:e]).all()
         np.testing.assert_allclose(d[o:e], c[o:e], rtol=1e-5, atol=1e-6 * np.abs(c[o:e]).max())
+
+
+@pytest.mark.parametrize("threads", [512, 1024])
+def test_fixed_point_backward_takes_outlier_cotangents_in_fp32(B, oracle_lib, threads):
+    """Three cotangents ~4e12 times the typical one, in the same interval and
+    far past the rows a chunk's fixed-point scale is taken from: each term is
+    below the old 2^63 limit, but their sum is not.  Terms above the chunk's
+    cap (2^62 / its kept rows) go through fp32 reductions instead, so the
+    gradient still matches the fp64 oracle within 1e-4 of its scale."""
+    case = _fixed_point_case(n_dens=3, events=60_000)
+    koff, counts = case["knot_offsets"], case["event_counts"]
+    eoff = np.concatenate([[0], np.cumsum(counts)])
+    seed, seq = int(case["scalars"][0]), int(case["scalars"][1])
+    ref = oracle_lib.d_forward(koff, eoff, case["grid"], case["values"], None, seed, seq)
+    cot = np.random.default_rng(11).standard_normal(len(ref["events"])).astype(np.float32)
+    # density 1's rows past its first 20000, three of them in one interval
+    lo, hi = int(ref["row_offsets"][1]) + 20_000, int(ref["row_offsets"][2])
+    ints = ref["intervals"][lo:hi]
+    vals, first, cnt = np.unique(ints, return_index=True, return_counts=True)
+    pick = lo + np.flatnonzero(ints == vals[np.argmax(cnt)])[:3]
+    assert len(pick) == 3
+    cot[pick] = 3.0e12
+    case["cotangent"] = cot
+    out = run_batch(B, case, B.make_config(threads=threads), with_intervals=False)
+    gref = oracle_lib.d_backward(koff, eoff, case["grid"], case["values"], None, seed, seq, cot,
+                                 fwd=ref)
+    for b in range(len(counts)):
+        o, e = koff[b], koff[b + 1]
+        assert np.isfinite(out["grad_values"][o:e]).all(), b
+        scale = np.abs(gref[o:e]).max()
+        assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b

@@ -62,7 +62,11 @@ def _rank_main(rank: int, world: int, port: int, out):
         # the whole batch on every rank (a consumer that needs all of it)
         import torch
 
-        ev_all, rows_all = sharding.gather_batch(torch.from_numpy(fwd["events"]),
+        # the rank's events as a sampler returns them in its capacity-sized
+        # buffer: kept rows first, then unused tail rows
+        ev_buf = np.full(sub["event_counts"].sum() + 7, -123.0)
+        ev_buf[:len(fwd["events"])] = fwd["events"]
+        ev_all, rows_all = sharding.gather_batch(torch.from_numpy(ev_buf),
                                                  torch.from_numpy(fwd["row_offsets"]))
         step_ms = sharding.max_over_ranks(1.5 + rank)
         if rank == 0:
