@@ -156,8 +156,14 @@ typedef struct loits_batch_config {
   int32_t ctas_per_sm;     /* persistent CTAs per SM (0 = as many as fit) */
   int32_t plain;           /* 1 = one launch per density (no persistent queue) */
   int32_t guide_ratio;     /* log2 of guide buckets per knot of a small density, 1..6;
-                              0 = 4 (16 buckets per knot), lowered where the guide
+                              0 = 2 (4 buckets per knot), lowered where the guide
                               would cost resident CTAs */
+  int32_t wait_limit;      /* polls of one device-side wait before it gives up and
+                              reports LOITS_ERR_TIMEOUT; 0 = the default (about 1 s) */
+  int32_t withhold_tile;   /* testing the bounded waits only: 1 + the index of a
+                              sampling tile that never publishes its compaction
+                              state, so that the next tile's wait runs out (the
+                              launch then reports LOITS_ERR_TIMEOUT); 0 = none */
   int64_t density_base;    /* global index of density 0 of this plan (sharding) */
   int64_t slot_stride;     /* Philox slots per density, >= max n_b (0 = max n_b) */
 } loits_batch_config;

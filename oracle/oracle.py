@@ -26,7 +26,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_LIB = HERE / "libloits_oracle.so"
 REF_DIR = HERE / "_ref"
-REFERENCE_TREE = Path(os.environ.get("LOITS_REFERENCE_TREE", "/root/reference"))
+# The reference project's source tree: LOITS_REFERENCE_TREE, else the
+# `reference` directory beside this repository's root.
+REFERENCE_TREE = Path(os.environ.get("LOITS_REFERENCE_TREE", str(HERE.parent.parent / "reference")))
 
 _i64 = C.c_int64
 _u64 = C.c_uint64

@@ -46,6 +46,7 @@ class Shape(C.Structure):
 class BatchConfig(C.Structure):
     _fields_ = [("threads", _i32), ("blocks_per_item", _i32), ("scan_knots", _i32),
                 ("ctas_per_sm", _i32), ("plain", _i32), ("guide_ratio", _i32),
+                ("wait_limit", _i32), ("withhold_tile", _i32),
                 ("density_base", _i64), ("slot_stride", _i64)]
 
     def as_dict(self) -> dict:

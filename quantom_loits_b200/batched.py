@@ -85,10 +85,12 @@ def default_config() -> N.BatchConfig:
 
 
 def make_config(threads=0, blocks_per_item=0, scan_knots=0, ctas_per_sm=0, plain=0,
-                density_base=0, slot_stride=0, guide_ratio=0) -> N.BatchConfig:
+                density_base=0, slot_stride=0, guide_ratio=0, wait_limit=0,
+                withhold_tile=0) -> N.BatchConfig:
     return N.BatchConfig(threads=int(threads), blocks_per_item=int(blocks_per_item),
                          scan_knots=int(scan_knots), ctas_per_sm=int(ctas_per_sm),
                          plain=int(plain), guide_ratio=int(guide_ratio),
+                         wait_limit=int(wait_limit), withhold_tile=int(withhold_tile),
                          density_base=int(density_base), slot_stride=int(slot_stride))
 
 

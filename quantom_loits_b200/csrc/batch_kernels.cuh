@@ -69,6 +69,9 @@ struct BatchArgs {
                                // memory to the guide
                                // (a larger guide is read every 2^s-th count)
   int32_t tiles_per_chunk;
+  uint32_t spin_limit;         // polls of one wait before it gives up (LOITS_ERR_TIMEOUT)
+  int32_t withhold_tile;       // a sampling tile whose look-back state is never published
+                               // (tests of the bounded waits); -1: none
   int64_t nmax;                // Philox slots per density (slot stride)
   int64_t dbase;               // global index of plan density 0
   uint64_t seed, stream_id;

@@ -329,7 +329,7 @@ __device__ __forceinline__ void cdf_pass2(const BatchArgs& a, int64_t k0, const 
 // aggregate, 2 inclusive.  Every poll is bounded.
 __device__ __forceinline__ double chained_lookback(uint32_t* flag, double* agg_arr, double* inc_arr,
                                                    int32_t* status, int32_t first, int32_t ct,
-                                                   double agg) {
+                                                   double agg, uint32_t limit) {
   const int lane = threadIdx.x & 31;
   double excl = 0.0;
   if (ct > first) {
@@ -346,7 +346,7 @@ __device__ __forceinline__ double chained_lookback(uint32_t* flag, double* agg_a
       // tiles before `first` do not exist: an inclusive zero
       const uint32_t fl = i >= first ? ld_acquire_u32(&flag[i]) : 2u;
       if (__any_sync(0xffffffffu, fl == 0)) {
-        if (++polls >= kSpinLimit ||
+        if (++polls >= limit ||
             ((polls & 63u) == 0u && __any_sync(0xffffffffu, launch_timed_out(status)))) {
           if (lane == 0) raise_status(status, LOITS_ERR_TIMEOUT);
           break;
@@ -375,7 +375,7 @@ __device__ __forceinline__ double chained_lookback(uint32_t* flag, double* agg_a
 }
 
 __device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first, int32_t ct, double agg) {
-  return chained_lookback(a.cflag, a.cagg, a.cinc, a.status, first, ct, agg);
+  return chained_lookback(a.cflag, a.cagg, a.cinc, a.status, first, ct, agg, a.spin_limit);
 }
 
 // Whether CDF item `it` (owner table first[]: scan or finalize items) can
@@ -508,7 +508,7 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
                      const_cast<float*>(kn.f));
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
-    if (lane == 0 && !wait_counter(&a.cdf_scanned[b], static_cast<uint32_t>(nci), a.status))
+    if (lane == 0 && !wait_counter(&a.cdf_scanned[b], static_cast<uint32_t>(nci), a.status, a.spin_limit))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
     __syncwarp();
     // largest unnormalised prefix of all earlier tiles (warp-strided max)
@@ -627,7 +627,7 @@ __device__ __forceinline__ float key_at(const float4* rec, int i) {
 // A density's sampling state.
 struct DensView {
   const float4* rec;      // records (shared or global)
-  const uint32_t* guide;  // small: packed (L[k], L[k+1]) in shared memory; large: L, global
+  const uint32_t* guide;  // small: packed entries in shared memory; large: L, global
   const uint32_t* cguide; // large, coarse: every 2^s-th count of L in shared memory
   const float* invd;      // backward weights (shared or global)
   int shift;              // 32 - m: bucket of a Philox word = word >> shift
@@ -664,7 +664,7 @@ struct SampleShared {
 __device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool large,
                                               bool wait_ready, SampleShared& sh) {
   if (threadIdx.x == 0) {
-    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status))
+    if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status, a.spin_limit))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
     sh.flags = ld_acquire_u32(&a.dflags[b]);
     sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
@@ -981,7 +981,8 @@ __device__ __forceinline__ bool tile_full(const TileGeom& tg) {
 // Called by warp 0; returns the base on every lane.
 __device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, const TileGeom& tg,
                                                 int cnt) {
-  const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(cnt), a.status);
+  const int64_t base = lookback_exclusive(a.tile_state, t, static_cast<uint64_t>(cnt), a.status,
+                                          a.spin_limit, t != a.withhold_tile);
   if ((threadIdx.x & 31) == 0) {
     a.tile_prefix[t] = base;
     if (t == __ldg(&a.tile_first[tg.b])) {
@@ -995,19 +996,37 @@ __device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, c
   return base;
 }
 
-// The threshold of a kThreshold density: the largest k in [-1, 2^24) with
-// x(k 2^-24) <= cut, found by one warp with a 33-ary search that evaluates
-// the sampler's own arithmetic (sample_slot) -- so slot p is kept exactly
-// when (word >> 8) > k, in the forward and in the backward alike.
+// The reference's inverse CDF at the uniform of `bits`, in fp64
+// (cpp/loits_core.cpp:193-196): the interval j by the sampler's exact search,
+// then g_j + m_j (u - c_j) with c_j = key_j - d_j and
+// m_j = (g_{j+1} - g_j) / (c_{j+1} - c_j + 1e-5).
+template <int kMode>
+__device__ __forceinline__ double exact_value(const DensView& d, uint32_t bits) {
+  const int j = sample_slot<kMode>(d, bits).j;
+  const float4 r0 = rec_at<kMode>(d.rec, j), r1 = rec_at<kMode>(d.rec, j + 1);
+  const double c0 = __dsub_rn(static_cast<double>(r0.x), static_cast<double>(r0.y));
+  const double c1 = __dsub_rn(static_cast<double>(r1.x), static_cast<double>(r1.y));
+  const double m = __ddiv_rn(__dsub_rn(static_cast<double>(r1.z), static_cast<double>(r0.z)),
+                             __dadd_rn(__dsub_rn(c1, c0), kEps));
+  const double u = static_cast<double>(uniform_from_bits(bits));
+  return __fma_rn(m, __dsub_rn(u, c0), static_cast<double>(r0.z));
+}
+
+// The threshold of a kThreshold density: the largest k in [-1, 2^24) whose
+// uniform k 2^-24 the reference would not keep (x <= cut, x in fp64), found
+// by one warp with a 33-ary search; slot p is kept exactly when
+// (word >> 8) > k, in the forward and in the backward alike.  (The written
+// event is x rounded to fp32.)
 template <int kMode>
 __device__ __forceinline__ int kept_threshold(const DensView& d) {
   const int lane = threadIdx.x & 31;
+  const double cut = static_cast<double>(d.cut);
   int lo = -1, hi = 1 << 24;  // x(lo) <= cut (lo = -1: none), x(hi) > cut (hi = 2^24: all)
   while (hi - lo > 1) {
     const int64_t span = hi - lo;
     const int p = lo + static_cast<int>(span * (lane + 1) / 33);
     bool le = true;
-    if (p > lo && p < hi) le = !(sample_slot<kMode>(d, static_cast<uint32_t>(p) << 8).x > d.cut);
+    if (p > lo && p < hi) le = !(exact_value<kMode>(d, static_cast<uint32_t>(p) << 8) > cut);
     const int lo2 = __reduce_max_sync(0xffffffffu, le ? p : lo);
     int hi2 = __reduce_min_sync(0xffffffffu, le ? hi : p);
     if (hi2 <= lo2) hi2 = lo2 + 1;  // only if x were not monotone: still ends
@@ -1876,7 +1895,7 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
   if (G > a.gcap) return;  // large density: reverse-scan tiles instead
   if (threadIdx.x == 0) {
-    if (!wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status))
+    if (!wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status, a.spin_limit))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
     sh.carry = 0.0;
   }
@@ -1976,7 +1995,7 @@ __device__ __forceinline__ void vjp_large_scan_item(const BatchArgs& a, int32_t 
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
   int64_t s0, s1;
   large_tile_range<TPB>(G, li - first, s0, s1);
-  if (threadIdx.x == 0 && !wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status))
+  if (threadIdx.x == 0 && !wait_counter(&a.chunks_done[b], static_cast<uint32_t>(nch), a.status, a.spin_limit))
     raise_status(a.status, LOITS_ERR_TIMEOUT);
   __syncthreads();
   const float2* gc = a.gcdf + __ldg(&a.gc_off[b]);
@@ -2001,7 +2020,8 @@ __device__ __forceinline__ void vjp_large_scan_item(const BatchArgs& a, int32_t 
   double seg_tot;
   const double later = block_exclusive_suffix_sum<double, TPB>(tot, seg_tot, sh.dscan);
   if (threadIdx.x < 32) {
-    const double carry_t = chained_lookback(a.lflag, a.lagg, a.linc, a.status, first, li, seg_tot);
+    const double carry_t =
+        chained_lookback(a.lflag, a.lagg, a.linc, a.status, first, li, seg_tot, a.spin_limit);
     if (threadIdx.x == 0) sh.carry = carry_t;
   }
   __syncthreads();
@@ -2051,7 +2071,7 @@ __device__ __forceinline__ void vjp_large_out_item(const BatchArgs& a, int32_t l
   large_tile_range<TPB>(G, li - first, s0, s1);
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
-    if (lane == 0 && !wait_counter(&a.lfin_done[b], static_cast<uint32_t>(nl), a.status))
+    if (lane == 0 && !wait_counter(&a.lfin_done[b], static_cast<uint32_t>(nl), a.status, a.spin_limit))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
     __syncwarp();
     double v = 0.0;

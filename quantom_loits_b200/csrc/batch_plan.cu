@@ -138,10 +138,11 @@ int default_blocks(int threads) { return threads == 1024 ? 8 : 16; }
 
 // Guide buckets per knot of a small density, as log2: M >= 2^ratio G buckets
 // where shared memory allows without lowering the CTAs an SM holds.  Finer
-// buckets hold fewer knots, so fewer slots need more than one key compare:
-// with 16 G buckets about 0.2 % of the benchmark densities' slots search,
-// against 3 % with 2 G (and a warp waits for its slowest lane).
-constexpr int kDefaultGuideRatio = 4;
+// buckets hold fewer knots, so fewer slots need more than one key compare
+// (about 1 % of the benchmark densities' slots search with 4 G buckets,
+// 3 % with 2 G), but cost more shared memory to copy per tile; 4 G measured
+// fastest on the uniform and ragged benchmark batches.
+constexpr int kDefaultGuideRatio = 2;
 constexpr int kMaxGuideRatio = 6;
 // Most guide bits a small density's packed guide takes in shared memory.
 constexpr int kMaxSmallGuideBits = 15;
@@ -161,6 +162,7 @@ int resolve_config(const loits_batch_config* in, loits_batch_config& out) {
   if (out.plain != 0 && out.plain != 1) return LOITS_ERR_INVALID;
   if (out.guide_ratio < 0 || out.guide_ratio > kMaxGuideRatio) return LOITS_ERR_INVALID;
   if (out.guide_ratio == 0) out.guide_ratio = kDefaultGuideRatio;
+  if (out.wait_limit < 0 || out.withhold_tile < 0) return LOITS_ERR_INVALID;
   if (out.density_base < 0 || out.slot_stride < 0) return LOITS_ERR_INVALID;
   return LOITS_OK;
 }
@@ -230,17 +232,20 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
   // smaller guide only widens buckets: the search finishes them exactly).
   // The backward reads every 2^s-th count when its budget is smaller: the
   // same guide with 2^s-times wider buckets.
-  auto cap_for = [&](size_t knot_bytes, int from) {
+  // forward and backward CTAs hold a small density's packed guide (4 bytes
+  // per bucket)
+  constexpr size_t kFwdEntry = sizeof(uint32_t), kBwdEntry = sizeof(uint32_t);
+  auto cap_for = [&](size_t knot_bytes, int from, size_t entry) {
     int mc = from;
-    while (mc > 2 && knot_bytes + g.static_smem + (size_t(1) << mc) * sizeof(uint32_t) > kSmemLimit)
-      --mc;
+    while (mc > 2 && knot_bytes + g.static_smem + (size_t(1) << mc) * entry > kSmemLimit) --mc;
     return mc;
   };
-  g.m_cap = cap_for(fwd_knots, kMaxSmallGuideBits);
-  g.m_cap_b = cap_for(bwd_knots, g.m_cap);
-  // sampling CTAs hold the guide as packed entries (pack_entry): M uint32;
+  g.m_cap = cap_for(fwd_knots, kMaxSmallGuideBits, kFwdEntry);
+  g.m_cap_b = cap_for(bwd_knots, kMaxSmallGuideBits, kBwdEntry);
+  // guide bytes of `entries` buckets (4-byte units, rounded up to 32 bytes);
   // kept events are staged in global memory, not here
   auto gbytes = [](int32_t entries) { return static_cast<size_t>((entries + 7) & ~7) * sizeof(uint32_t); };
+  auto fbytes = [&](int32_t entries) { return gbytes(entries); };
   // CTAs per SM that `bytes` of dynamic shared memory allow (at most the
   // register cap's 1280 / tpb)
   auto resident = [&](size_t bytes) {
@@ -253,7 +258,7 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
   // with records beside it; in the backward with records, weights and sums)
   const int m1 = guide_bits(max_g, g.m_cap, 1);
   int m = guide_bits(max_g, g.m_cap, ratio);
-  while (m > m1 && resident(fwd_knots + gbytes(1 << m)) < resident(fwd_knots + gbytes(1 << m1))) --m;
+  while (m > m1 && resident(fwd_knots + fbytes(1 << m)) < resident(fwd_knots + fbytes(1 << m1))) --m;
   g.m_cap = m;  // every small density's guide takes at most this many bits
   g.mcap = static_cast<int32_t>(int64_t(1) << m);
   const int mb1 = std::min(g.m_cap_b, m1);
@@ -264,7 +269,7 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
     --mb;
   g.m_cap_b = mb;
   const int32_t mcap_b = std::min<int32_t>(g.mcap, int32_t(1) << g.m_cap_b);
-  const size_t guide_f = gbytes(g.mcap);
+  const size_t guide_f = fbytes(g.mcap);
   size_t guide_b = gbytes(mcap_b);
   // Backward small-density slot: records, weights and either fp32 grad-CDF
   // sums (4 bytes per knot) or the fixed-point sums A, B (16 bytes per
@@ -415,6 +420,8 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.scan_knots = p->scan_knots;
   a.gcap = p->gcap;
   a.tiles_per_chunk = p->tiles_per_chunk;
+  a.spin_limit = p->cfg.wait_limit > 0 ? static_cast<uint32_t>(p->cfg.wait_limit) : kSpinLimit;
+  a.withhold_tile = p->cfg.withhold_tile - 1;
   a.nmax = p->nmax;
   a.dbase = p->dbase;
   const Layout& L = p->lay;

@@ -158,11 +158,11 @@ __device__ __forceinline__ bool launch_timed_out(const int32_t* status) {
   return status && *reinterpret_cast<const volatile int32_t*>(status) == LOITS_ERR_TIMEOUT;
 }
 
-// Wait until *counter >= target (acquire).  Returns false on timeout (or
-// when another wait of the launch has timed out).
+// Wait until *counter >= target (acquire), at most `limit` polls.  Returns
+// false on timeout (or when another wait of the launch has timed out).
 __device__ __forceinline__ bool wait_counter(const uint32_t* counter, uint32_t target,
-                                             const int32_t* status) {
-  for (uint32_t it = 0; it < kSpinLimit; ++it) {
+                                             const int32_t* status, uint32_t limit = kSpinLimit) {
+  for (uint32_t it = 0; it < limit; ++it) {
     if (ld_acquire_u32(counter) >= target) return true;
     if ((it & 63u) == 63u && launch_timed_out(status)) return false;
     spin_pause(it);

@@ -18,14 +18,19 @@ constexpr unsigned long long kFlagInclusive = 2ull << 62;
 constexpr unsigned long long kValueMask = (1ull << 62) - 1;
 
 // Called by every lane of ONE warp.  Returns the exclusive prefix of `tile`.
+// limit: polls of one predecessor before the wait gives up.  publish = false
+// leaves the tile's own state unpublished, so that its successors' waits run
+// out (a test of the bounded waits; never set in sampling).
 __device__ __forceinline__ int64_t lookback_exclusive(unsigned long long* states, int64_t tile,
-                                                      uint64_t count, int32_t* status) {
+                                                      uint64_t count, int32_t* status,
+                                                      uint32_t limit = kSpinLimit,
+                                                      bool publish = true) {
   const int lane = threadIdx.x & 31;
   if (tile == 0) {
-    if (lane == 0) st_release_u64(&states[0], kFlagInclusive | count);
+    if (lane == 0 && publish) st_release_u64(&states[0], kFlagInclusive | count);
     return 0;
   }
-  if (lane == 0) st_release_u64(&states[tile], kFlagAggregate | count);
+  if (lane == 0 && publish) st_release_u64(&states[tile], kFlagAggregate | count);
   uint64_t excl = 0;
   int64_t base = tile - 1;
   uint32_t polls = 0;
@@ -35,7 +40,7 @@ __device__ __forceinline__ int64_t lookback_exclusive(unsigned long long* states
     const unsigned long long s = idx >= 0 ? ld_acquire_u64(&states[idx]) : kFlagInclusive;
     const unsigned long long flag = s & ~kValueMask;
     if (__any_sync(0xffffffffu, flag == 0)) {
-      if (++polls >= kSpinLimit ||
+      if (++polls >= limit ||
           ((polls & 63u) == 0u && __any_sync(0xffffffffu, launch_timed_out(status)))) {
         timed_out = true;
         break;
@@ -51,7 +56,8 @@ __device__ __forceinline__ int64_t lookback_exclusive(unsigned long long* states
     base -= 32;
   }
   if (timed_out && lane == 0) raise_status(status, LOITS_ERR_TIMEOUT);
-  if (lane == 0) st_release_u64(&states[tile], kFlagInclusive | ((excl + count) & kValueMask));
+  if (lane == 0 && publish)
+    st_release_u64(&states[tile], kFlagInclusive | ((excl + count) & kValueMask));
   return static_cast<int64_t>(excl);
 }
 

@@ -1,7 +1,8 @@
 """Generate the golden vectors in this directory from the REFERENCE itself.
 
-Run in a container that has the reference tree (default /root/reference,
-override with LOITS_REFERENCE_TREE):
+Run in a container that has the reference tree (by default the `reference`
+directory beside this repository's root; override with
+LOITS_REFERENCE_TREE):
 
     python tests/golden/make_golden.py
 
@@ -34,7 +35,9 @@ import torch
 
 ROOT = Path(__file__).resolve().parents[2]
 sys.path.insert(0, str(ROOT))
-REF = Path(os.environ.get("LOITS_REFERENCE_TREE", "/root/reference"))
+# the reference project's source tree: LOITS_REFERENCE_TREE, else the
+# `reference` directory beside this repository's root
+REF = Path(os.environ.get("LOITS_REFERENCE_TREE", str(ROOT.parent / "reference")))
 sys.path.insert(0, str(REF))
 
 from oracle import oracle as O  # noqa: E402
