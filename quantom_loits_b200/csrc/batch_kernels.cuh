@@ -89,6 +89,7 @@ struct BatchArgs {
                                // bucket k | movable knots << 16), k = 0..M-1
   double* norm;
   uint32_t* dflags;            // bit 0: CDF not non-decreasing (count semantics)
+  int32_t* kstar;              // kThreshold densities: slot kept iff (word >> 8) > kstar
   uint32_t* cdf_ready;         // 1 once a density's records and packed guide are final
   uint32_t* cdf_scanned;       // scanned CDF tiles per density
   uint32_t* fin_done;          // finalized CDF tiles per density (multi-tile densities)

@@ -417,6 +417,26 @@ __device__ __forceinline__ Knots tile_knots(const BatchArgs& a, int64_t k0, int6
   }
 }
 
+__device__ __forceinline__ int density_threshold(const BatchArgs& a, int b, int64_t k0, int64_t G);
+
+// The end of a density's CDF, by thread 0 holding the density's flags `fl`
+// (on every lane of warp 0 after the call): a kThreshold density's kept
+// threshold is found by warp 0 and stored, then the density is published
+// ready (its records, guide, flags and threshold all visible first).
+__device__ __forceinline__ void publish_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
+                                                uint32_t fl) {
+  if (threadIdx.x >= 32) return;
+  fl = __shfl_sync(0xffffffffu, fl, 0);
+  if (fl & kThreshold) {
+    const int ks = density_threshold(a, b, k0, G);
+    if (threadIdx.x == 0) a.kstar[b] = ks;
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    atomicAdd(&a.cdf_ready[b], 1u);
+  }
+}
+
 template <int TPB, bool kS>
 __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared<TPB>& sh,
                                               float* stage_s) {
@@ -454,14 +474,15 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
                        __ldg(&a.gbits[b]), sh);
     if (!any_neg) pack_guide<TPB>(a, b);
     __syncthreads();
+    uint32_t fl = 0;
     if (threadIdx.x == 0) {
       a.norm[b] = tile_tot;
-      uint32_t fl = (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u);
+      fl = (any_neg ? kNonMonotone : 0u) | (any_bad ? kBadGrid : 0u);
       fl |= accept_all_flag(a, b, k0, G, tile_tot, fl);
-      a.dflags[b] = fl | threshold_flag(a, b, k0, G, tile_tot, fl);
-      __threadfence();
-      atomicAdd(&a.cdf_ready[b], 1u);
+      fl |= threshold_flag(a, b, k0, G, tile_tot, fl);
+      a.dflags[b] = fl;
     }
+    publish_density(a, b, k0, G, fl);
     return;
   }
   (void)tile_max;
@@ -568,13 +589,14 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
     __threadfence();
     if (!nonmono) pack_guide<TPB>(a, b);
     __syncthreads();
+    uint32_t fl = 0;
     if (threadIdx.x == 0) {
-      uint32_t fl = ld_acquire_u32(&a.dflags[b]) & (kNonMonotone | kBadGrid);
+      fl = ld_acquire_u32(&a.dflags[b]) & (kNonMonotone | kBadGrid);
       fl |= accept_all_flag(a, b, k0, G, norm, fl);
-      a.dflags[b] = fl | threshold_flag(a, b, k0, G, norm, fl);
-      __threadfence();
-      atomicAdd(&a.cdf_ready[b], 1u);
+      fl |= threshold_flag(a, b, k0, G, norm, fl);
+      a.dflags[b] = fl;
     }
+    publish_density(a, b, k0, G, fl);
   }
   __syncthreads();
 }
@@ -635,6 +657,7 @@ struct DensView {
   bool count_all;
   bool accept_all;
   bool threshold;         // kept = uniforms above one threshold (kThreshold)
+  int kstar;              // ... namely (word >> 8) > kstar
   bool skip;              // large density whose CDF is not non-decreasing: not sampled
   bool coarse;            // large: cguide in shared memory (shift covers its bits)
   bool fresh;             // large: the coarse guide was copied for this view
@@ -655,6 +678,7 @@ struct SampleShared {
   int win_b;         // density whose fixed-point window win_lo belongs to
   int win_lo;
   int run_k0;        // most_probable_run's result
+  int kstar;         // the density's kept threshold (kThreshold)
 };
 
 // Wait until density b's CDF is final (thread 0) and share its flags and cut.
@@ -667,6 +691,7 @@ __device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool la
     if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status, a.spin_limit))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
     sh.flags = ld_acquire_u32(&a.dflags[b]);
+    sh.kstar = (sh.flags & kThreshold) ? __ldcg(&a.kstar[b]) : 0;
     sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
     if (large && (sh.flags & kNonMonotone)) raise_status(a.status, LOITS_ERR_UNSUPPORTED);
   }
@@ -737,6 +762,7 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
   v.count_all = nonmono && !large;
   v.accept_all = (sh.flags & kAcceptAll) != 0;
   v.threshold = (sh.flags & kThreshold) != 0;
+  v.kstar = sh.kstar;
   v.skip = nonmono && large;
   v.coarse = coarse;
   v.cut = sh.cut;
@@ -1036,6 +1062,21 @@ __device__ __forceinline__ int kept_threshold(const DensView& d) {
   return lo;
 }
 
+// kept_threshold of density b from global memory (its records and full
+// guide, final once its CDF is): by one warp, in the item that finishes the
+// density's CDF, so that sampling tiles and backward chunks only read it.
+__device__ __forceinline__ int density_threshold(const BatchArgs& a, int b, int64_t k0, int64_t G) {
+  DensView d{};
+  d.rec = a.rec + k0;
+  d.guide = a.gl + __ldg(&a.goff[b]);
+  d.shift_full = 32 - __ldg(&a.gbits[b]);
+  d.shift = d.shift_full;
+  d.G = static_cast<int>(G);
+  d.coarse = false;
+  d.cut = __ldg(&a.x_cut[b]);
+  return kept_threshold<kL2>(d);
+}
+
 __device__ __forceinline__ uint32_t threshold_keep(uint4 w, int kstar) {
   return (static_cast<int>(w.x >> 8) > kstar ? 1u : 0u) |
          (static_cast<int>(w.y >> 8) > kstar ? 2u : 0u) |
@@ -1053,7 +1094,7 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
                                                       SampleShared& sh) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  const int kstar = kept_threshold<kMode>(d);
+  const int kstar = d.kstar;
   const bool full = tile_full<TPB, R>(tg);
   int cnt = 0;
 #pragma unroll 1
@@ -1271,7 +1312,7 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   __syncthreads();
   uint32_t* mine = hu + (lane & (rep - 1)) * stride;
   const bool full = tile_full<TPB, R>(tg);
-  const int kstar = d.threshold ? kept_threshold<kMode>(d) : 0;
+  const int kstar = d.kstar;
   int kept = 0;
 #pragma unroll 1
   for (int r = 0; r < R; ++r) {
@@ -1573,7 +1614,7 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
     return;
   }
   // kThreshold densities keep exactly the slots the forward kept by threshold
-  const int kstar = d.threshold ? kept_threshold<kMode>(d) : 0;
+  const int kstar = d.kstar;
   if (gh) {
     // histogram mode: every kept slot's cotangent comes from the histogram's
 #pragma unroll 1

@@ -35,7 +35,8 @@ size_t align_up(size_t v, size_t a = kAlign) { return (v + a - 1) / a * a; }
 struct Layout {
   size_t status, tickets_fwd, dflags, cdf_ready, cdf_scanned, fin_done, cflag, tile_state;  // zeroed by forward
   size_t tickets_bwd, chunks_done, lfin_done, lflag, gcdf;                        // zeroed by backward
-  size_t rec, invd, gl, gpk, norm, cagg, cinc, cmax, tile_prefix, warp_off, stage, partials, grho;
+  size_t rec, invd, gl, gpk, norm, kstar, cagg, cinc, cmax, tile_prefix, warp_off, stage, partials,
+      grho;
   size_t lagg, linc, lgn;
   size_t fwd_zero_lo, fwd_zero_hi, bwd_zero_lo, bwd_zero_hi, total;
 };
@@ -431,6 +432,7 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.gpk = carve<uint32_t>(ws, L.gpk);
   a.fin_done = carve<uint32_t>(ws, L.fin_done);
   a.norm = carve<double>(ws, L.norm);
+  a.kstar = carve<int32_t>(ws, L.kstar);
   a.dflags = carve<uint32_t>(ws, L.dflags);
   a.cdf_ready = carve<uint32_t>(ws, L.cdf_ready);
   a.cdf_scanned = carve<uint32_t>(ws, L.cdf_scanned);
@@ -677,6 +679,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   L.linc = o; o = align_up(o + static_cast<size_t>(p->n_lfin) * 8);
   L.lgn = o; o = align_up(o + static_cast<size_t>(p->n_lfin) * 8);
   L.norm = o; o = align_up(o + nd * 8);
+  L.kstar = o; o = align_up(o + nd * 4);
   L.cagg = o; o = align_up(o + static_cast<size_t>(nc) * 8);
   L.cinc = o; o = align_up(o + static_cast<size_t>(nc) * 8);
   L.cmax = o; o = align_up(o + static_cast<size_t>(nc) * 8);
