@@ -675,6 +675,7 @@ struct SampleShared {
   float cut;
   float fix_scale;   // backward chunk: fixed-point units per cotangent unit
   float fix_cap;     // backward chunk: largest scaled term a fixed-point sum takes
+  int fix_lbits;     // backward chunk: bits of a term in its low word
   int win_b;         // density whose fixed-point window win_lo belongs to
   int win_lo;
   int run_k0;        // most_probable_run's result
@@ -1463,51 +1464,48 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
 //  * small densities, fp32: gacc (shared memory), two fp32 atomics per kept
 //    slot;
 //  * small densities, fixed point (fix): per interval j the two sums
-//    A_j = sum g and B_j = sum g w, each a 64-bit two's-complement integer in
-//    units of 1/scale held as a low uint32 word and a high int32 word
-//    (alo/ahi/blo/bhi, planar so that consecutive intervals use consecutive
-//    banks).  Shared-memory fp32 atomicAdd is a compare-and-swap loop; uint32
-//    atomicAdd is one native instruction, and integer sums do not depend on
-//    their order.  The chunk's grad-CDF is formed from A and B when the chunk
-//    ends: gcdf_k = m_k (B_k - A_k) - m_{k-1} B_{k-1};
+//    A_j = sum g and B_j = sum g w of integer terms (units of 1/scale), each
+//    held as two uint32 words (alo/ahi/blo/bhi, planar so that consecutive
+//    intervals use consecutive banks): a term v is split into its low s bits
+//    v mod 2^s and its high part v >> s (arithmetic), and each part is added
+//    to its word with one native uint32 shared-memory reduction -- no
+//    returned value, no carry to propagate.  Shared-memory fp32 atomicAdd is
+//    a compare-and-swap loop, slow where many lanes hit one interval; uint32
+//    reductions are native even then, and integer sums do not depend on their
+//    order.  The chunk's grad-CDF is formed from A and B when the chunk ends:
+//    gcdf_k = m_k (B_k - A_k) - m_{k-1} B_{k-1};
 //  * large densities: the same fixed-point sums for the intervals of a window
 //    [win_lo, win_lo + win_n) (the most probable ones), one float2 global
 //    atomic per kept slot for the others (gc).
-// A fixed-point term is added only while its scaled magnitude stays below
-// cap = 2^63 / (the chunk's kept rows), so that no sum of the chunk can wrap
-// its 64 bits; a larger (or non-finite) cotangent's terms take the fp32 path
-// instead, as global fp32 reductions: into the chunk's partial (`spill`,
-// zeroed when the chunk starts and added to the fixed-point sums when it
-// ends) for small densities, into gc for large ones.  Non-finite values
-// therefore reach the gradient as they would through fp32 sums.
+// Neither word can wrap: with at most 2^lg kept rows in the chunk, s =
+// 32 - lg keeps the low words below 2^32, and a term is added only while its
+// scaled magnitude stays below cap = 2^min(30, 30 + s - lg), which keeps the
+// high words inside int32.  A larger (or non-finite) cotangent's terms take
+// the fp32 path instead, as global fp32 reductions: into the chunk's partial
+// (`spill`, zeroed when the chunk starts and added to the fixed-point sums
+// when it ends) for small densities, into gc for large ones.  Non-finite
+// values therefore reach the gradient as they would through fp32 sums.
 struct Acc {
   float* gacc;
   uint32_t *alo, *ahi, *blo, *bhi;
   float2* gc;
   float* spill;
   float scale, cap;
+  int lbits;       // s: bits of a term in its low word
+  uint32_t lmask;  // 2^s - 1
   int win_lo, win_n;
 };
 
-// Fixed-point value of f (already scaled): f rounded to an integer.
-__device__ __forceinline__ long long fix_round(float f) {
-  return fabsf(f) < 2.0e9f ? static_cast<long long>(__float2int_rn(f)) : __float2ll_rn(f);
+// Adds integer term v (|v| < 2^30) to the split sum (lo, hi) at index i.
+__device__ __forceinline__ void fix_add(const Acc& acc, uint32_t* lo, uint32_t* hi, int i, int v) {
+  atomicAdd(&lo[i], static_cast<uint32_t>(v) & acc.lmask);  // no return value: reductions
+  atomicAdd(&hi[i], static_cast<uint32_t>(v >> acc.lbits));
 }
 
-// Adds v to the 64-bit sum (lo, hi): one uint32 atomic on the low word; the
-// high word takes the carry and v's high part when they do not cancel (for
-// |v| < 2^31: only when the low word wraps).
-__device__ __forceinline__ void fix_add(uint32_t* lo, uint32_t* hi, int i, long long v) {
-  const uint32_t vl = static_cast<uint32_t>(v);
-  const uint32_t vh = static_cast<uint32_t>(static_cast<unsigned long long>(v) >> 32);
-  const uint32_t old = atomicAdd(&lo[i], vl);
-  const uint32_t h = vh + (old + vl < old ? 1u : 0u);
-  if (h != 0u) atomicAdd(&hi[i], h);
-}
-
-__device__ __forceinline__ double fix_value(uint32_t lo, uint32_t hi, double inv_scale) {
-  return static_cast<double>(static_cast<long long>((static_cast<unsigned long long>(hi) << 32) |
-                                                    lo)) * inv_scale;
+// The split sum's value (hi 2^s + lo) in cotangent units.
+__device__ __forceinline__ double fix_value(uint32_t lo, uint32_t hi, int lbits, double inv_scale) {
+  return (ldexp(static_cast<double>(static_cast<int32_t>(hi)), lbits) + static_cast<double>(lo)) *
+         inv_scale;
 }
 
 // One kept slot's (g, g w) into fixed-point slot i, when both scaled terms
@@ -1516,8 +1514,8 @@ __device__ __forceinline__ double fix_value(uint32_t lo, uint32_t hi, double inv
 __device__ __forceinline__ bool fix_pair(const Acc& acc, int i, float g, float w) {
   const float f0 = g * acc.scale, f1 = (g * w) * acc.scale;
   if (!(fabsf(f0) < acc.cap) || !(fabsf(f1) < acc.cap)) return false;
-  fix_add(acc.alo, acc.ahi, i, fix_round(f0));
-  fix_add(acc.blo, acc.bhi, i, fix_round(f1));
+  fix_add(acc, acc.alo, acc.ahi, i, __float2int_rn(f0));
+  fix_add(acc, acc.blo, acc.bhi, i, __float2int_rn(f1));
   return true;
 }
 
@@ -1715,13 +1713,14 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
 template <int TPB>
 constexpr bool kFixPaths = TPB >= 512;
 
-// Fixed-point scale of a backward chunk (into sh.fix_scale): a power of two
-// that puts the mean |cotangent| of up to TPB of the chunk's kept rows near
-// 2^20, so one unit is about 1e-6 of a typical contribution; larger values
-// take more bits.  Histogram mode: the mean histogram-cotangent step
-// instead.  sh.fix_cap = 2^62 / rows (rounded down to a power of two): `rows`
-// terms below it cannot wrap a 64-bit sum (rows: the chunk's kept rows, or
-// in histogram mode its slots).  Ends with a barrier.
+// Fixed-point geometry of a backward chunk of at most `rows` kept rows (in
+// histogram mode its slots), into sh: with rows <= 2^lg, the low-word bits
+// s = 32 - lg, the term bound cap = 2^min(30, 30 + s - lg) (see Acc), and
+// the scale, a power of two that puts the mean |cotangent| of up to TPB of
+// the chunk's kept rows near 2^p, p = min(20, log2(cap) - 10): one unit is
+// about 1e-6 of a typical contribution where the chunk allows, and terms up
+// to 2^10 times the mean stay in fixed point.  Histogram mode: the mean
+// histogram-cotangent step instead.  Ends with a barrier.
 template <int TPB>
 __device__ __forceinline__ void chunk_scale(const BatchArgs& a, const float* gh, int64_t r0,
                                             int64_t r1, int64_t rows, SampleShared& sh) {
@@ -1751,9 +1750,12 @@ __device__ __forceinline__ void chunk_scale(const BatchArgs& a, const float* gh,
     int e = 0;
     if (cnt > 0 && sum > 0.0f) frexpf(sum / cnt, &e);
     e = min(max(e, -100), 100);
-    sh.fix_scale = ldexpf(1.0f, 20 - e);
     const int lg = rows > 1 ? 64 - __clzll(static_cast<unsigned long long>(rows - 1)) : 0;
-    sh.fix_cap = ldexpf(1.0f, 62 - lg);
+    const int lbits = max(1, min(31, 32 - lg));
+    const int cap_log = min(30, 30 + lbits - lg);
+    sh.fix_scale = ldexpf(1.0f, min(20, cap_log - 10) - e);
+    sh.fix_cap = ldexpf(1.0f, cap_log);
+    sh.fix_lbits = lbits;
   }
   __syncthreads();
 }
@@ -1774,6 +1776,80 @@ __device__ __forceinline__ void large_window(const BatchArgs& a, const DensView&
     sh.win_b = b;
   }
   __syncthreads();
+}
+
+// Saved-state chunk of a small density with a non-decreasing CDF, in fixed
+// point: the weights 1/d_j in shared memory (smem[0, G)), the sums A, B
+// after them, the chunk's partial `part` taking the fp32 reductions of terms
+// above the cap; each kept row reads its interval, offset and cotangent
+// (coalesced) and one weight; the slopes enter per interval when the chunk
+// ends, read from the records in global memory.  Ends with every partial
+// written (not fenced).
+template <int TPB>
+__device__ __forceinline__ void vjp_state_chunk_fix(const BatchArgs& a, int64_t k0, int G,
+                                                    int64_t r0, int64_t r1, float* part,
+                                                    float* smem, SampleShared& sh) {
+  float* invd_s = smem;
+  uint32_t* base = reinterpret_cast<uint32_t*>(smem + ((G + 3) & ~3));
+  for (int i = threadIdx.x; i < G; i += TPB) {
+    invd_s[i] = __ldg(&a.invd[k0 + i]);
+    __stcg(&part[i], 0.0f);
+  }
+  for (int i = threadIdx.x; i < 4 * G; i += TPB) base[i] = 0u;
+  chunk_scale<TPB>(a, nullptr, r0, r1, r1 - r0, sh);
+  Acc acc{};
+  acc.alo = base;
+  acc.ahi = base + G;
+  acc.blo = base + 2 * G;
+  acc.bhi = base + 3 * G;
+  acc.scale = sh.fix_scale;
+  acc.cap = sh.fix_cap;
+  acc.lbits = sh.fix_lbits;
+  acc.lmask = (1u << acc.lbits) - 1u;
+  const float4* rec = a.rec + k0;
+  const int jmax = G - 2;
+  constexpr int U = 4;  // rows per thread in flight
+#pragma unroll 1
+  for (int64_t r_base = r0; r_base < r1; r_base += static_cast<int64_t>(TPB) * U) {
+    int j[U];
+    float t[U], g[U];
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      const int64_t r = r_base + i * TPB + threadIdx.x;
+      j[i] = -1;
+      t[i] = g[i] = 0.0f;
+      if (r < r1) {
+        j[i] = min(max(__ldcs(&a.st_intervals[r]), 0), jmax);
+        t[i] = __ldcs(&a.st_offsets[r]);
+        g[i] = __ldcs(&a.grad[r]);
+      }
+    }
+#pragma unroll
+    for (int i = 0; i < U; ++i) {
+      if (j[i] < 0) continue;
+      const float w = t[i] * invd_s[j[i]];
+      if (!fix_pair(acc, j[i], g[i], w)) {
+        const float mg = __ldg(&rec[j[i]].w) * g[i];
+        atomicAdd(&part[j[i]], mg * (w - 1.0f));  // no return value: reductions
+        atomicAdd(&part[j[i] + 1], -(mg * w));
+      }
+    }
+  }
+  __threadfence();
+  __syncthreads();
+  const double inv_scale = 1.0 / static_cast<double>(acc.scale);
+  for (int i = threadIdx.x; i < G; i += TPB) {
+    // gcdf_i = m_i (B_i - A_i) - m_{i-1} B_{i-1} (no interval starts at knot G-1)
+    double v = 0.0;
+    if (i + 1 < G)
+      v = static_cast<double>(__ldg(&rec[i].w)) *
+          (fix_value(acc.blo[i], acc.bhi[i], acc.lbits, inv_scale) -
+           fix_value(acc.alo[i], acc.ahi[i], acc.lbits, inv_scale));
+    if (i > 0)
+      v -= static_cast<double>(__ldg(&rec[i - 1].w)) *
+           fix_value(acc.blo[i - 1], acc.bhi[i - 1], acc.lbits, inv_scale);
+    __stcg(&part[i], static_cast<float>(v + static_cast<double>(__ldcg(&part[i]))));
+  }
 }
 
 // Backward chunk (density, run of sampling tiles).  kFix: the plan has small
@@ -1822,6 +1898,8 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       acc.bhi = base + 3 * a.win_n;
       acc.scale = sh.fix_scale;
       acc.cap = sh.fix_cap;
+      acc.lbits = sh.fix_lbits;
+      acc.lmask = (1u << acc.lbits) - 1u;
       acc.win_lo = sh.win_lo;
       acc.win_n = a.win_n;
     }
@@ -1832,8 +1910,8 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       for (int i = threadIdx.x; i < a.win_n; i += TPB) {
         if ((acc.alo[i] | acc.ahi[i] | acc.blo[i] | acc.bhi[i]) == 0u) continue;
         const int j = acc.win_lo + i;
-        const double A = fix_value(acc.alo[i], acc.ahi[i], inv_scale);
-        const double Bs = fix_value(acc.blo[i], acc.bhi[i], inv_scale);
+        const double A = fix_value(acc.alo[i], acc.ahi[i], acc.lbits, inv_scale);
+        const double Bs = fix_value(acc.blo[i], acc.bhi[i], acc.lbits, inv_scale);
         const double m = static_cast<double>(__ldg(reinterpret_cast<const float*>(d.rec + j) + 3));
         red_add_f32x2(&acc.gc[j], static_cast<float>(m * (Bs - A)), static_cast<float>(-m * Bs));
       }
@@ -1851,12 +1929,24 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   // share an interval (small, peaked densities) rarely collide
   int rep = 1;
   while (rep < 32 && 2 * rep * (G + 1) <= a.gcap) rep *= 2;
-  // Fixed-point sums instead where one fp32 copy would be shared by every
-  // lane, the density has at most 4096 knots (larger ones measured slower in
-  // fixed point) and its records, weights and sums (36 bytes per knot) fit
-  // the slot before the guide: records at 0, weights at 16 G, sums A, B at
-  // 20 G bytes.
-  if (kFix && kFixPaths<TPB> && rep == 1 && G <= 4096 && 36ll * G <= 4ll * a.bwd_guide_off) {
+  // Saved state: each kept row carries its interval and offset, so the chunk
+  // needs only the weights 1/d_j in shared memory (no records, no guide) and
+  // sums every row in fixed point.
+  if (kFixPaths<TPB> && a.st_intervals && 20ll * G <= 4ll * a.bwd_guide_off) {
+    density_flags(a, b, false, false, sh);
+    if (!(sh.flags & kNonMonotone)) {
+      vjp_state_chunk_fix<TPB>(a, tg.k0, G, r0, r1, part, reinterpret_cast<float*>(rec_s), sh);
+      __threadfence();
+      __syncthreads();
+      if (threadIdx.x == 0) atomicAdd(&a.chunks_done[b], 1u);
+      return;
+    }
+  }
+  // Fixed-point sums instead (native uint32 reductions, fast however many
+  // lanes share an interval) where the density's records, weights and sums
+  // (36 bytes per knot) fit the slot before the guide: records at 0,
+  // weights at 16 G, sums A, B at 20 G bytes.
+  if (kFix && kFixPaths<TPB> && 36ll * G <= 4ll * a.bwd_guide_off) {
     float4* rec_f = rec_s;
     float* invd_f = reinterpret_cast<float*>(rec_s + G);
     uint32_t* base = reinterpret_cast<uint32_t*>(invd_f + G);
@@ -1882,6 +1972,8 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
       acc.bhi = base + 3 * G;
       acc.scale = sh.fix_scale;
       acc.cap = sh.fix_cap;
+      acc.lbits = sh.fix_lbits;
+      acc.lmask = (1u << acc.lbits) - 1u;
       acc.spill = part;
       vjp_chunk_tiles<TPB, R, kShared, true>(a, d, tg, tb, t_first, t_end, acc, gh);
       __threadfence();
@@ -1891,11 +1983,12 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
         // gcdf_i = m_i (B_i - A_i) - m_{i-1} B_{i-1} (no interval starts at knot G-1)
         double v = 0.0;
         if (i + 1 < G)
-          v = static_cast<double>(rec_f[i].w) * (fix_value(acc.blo[i], acc.bhi[i], inv_scale) -
-                                                  fix_value(acc.alo[i], acc.ahi[i], inv_scale));
+          v = static_cast<double>(rec_f[i].w) *
+              (fix_value(acc.blo[i], acc.bhi[i], acc.lbits, inv_scale) -
+               fix_value(acc.alo[i], acc.ahi[i], acc.lbits, inv_scale));
         if (i > 0)
           v -= static_cast<double>(rec_f[i - 1].w) *
-               fix_value(acc.blo[i - 1], acc.bhi[i - 1], inv_scale);
+               fix_value(acc.blo[i - 1], acc.bhi[i - 1], acc.lbits, inv_scale);
         __stcg(&part[i], static_cast<float>(v + static_cast<double>(__ldcg(&part[i]))));
       }
     }

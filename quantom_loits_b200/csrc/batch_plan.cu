@@ -599,13 +599,12 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->fwin_n = sg.fwin_n;
   p->fwd_guide_off = sg.fwd_guide_off;
   // the backward variant with fixed-point sums, when some small density
-  // takes that path (one fp32 copy of its sums per CTA, at most 4096 knots,
-  // its 36 bytes per knot within the slot; see vjp_chunk_item)
+  // takes that path (its 36 bytes per knot within the slot; see
+  // vjp_chunk_item)
   if (p->tpb >= 512) {
     for (int64_t b = 0; b < n_densities && !p->fix_used; ++b) {
       const int64_t g = p->koff[b + 1] - p->koff[b];
-      p->fix_used = g <= p->gcap && 2 * (g + 1) > p->gcap && g <= 4096 &&
-                    36 * g <= 4 * static_cast<int64_t>(p->bwd_guide_off);
+      p->fix_used = g <= p->gcap && 36 * g <= 4 * static_cast<int64_t>(p->bwd_guide_off);
     }
   }
   p->fwd_smem = sg.fwd;
