@@ -65,9 +65,11 @@ PEAKS = ROOT / "MEASURED_PEAKS.json"
 TRAFFIC = ROOT / "profiles" / "traffic.json"
 FALLBACK_HBM_GBS = 6650.0
 # algorithmic bytes per kept event: the forward writes the event (4 B), the VJP
-# reads its cotangent (4 B); per knot the forward reads grid + value (8 B), the
-# VJP reads them again and writes the gradient (12 B)
-FWD_B_PER_EVENT, BWD_B_PER_EVENT = 4, 4
+# reads its cotangent (4 B); the saved-state form (the default) also writes,
+# and its VJP reads, the row's interval and offset (8 B); per knot the forward
+# reads grid + value (8 B), the VJP reads them again and writes the gradient
+# (12 B)
+FWD_B_PER_EVENT, BWD_B_PER_EVENT, STATE_B_PER_EVENT = 4, 4, 8
 FWD_B_PER_KNOT, BWD_B_PER_KNOT = 8, 12
 
 
@@ -293,7 +295,8 @@ def tune(spec, dev, args, plain: bool):
     if threads or blocks or args.no_tune:
         return dict(base, threads=threads, blocks_per_item=blocks, scan_knots=0), None
     tbatch = B.DensityBatch.from_spec(spec, dev)
-    tuner = Autotuner(dev, candidates=PLAIN_CANDIDATES if plain else CANDIDATES, base=base)
+    tuner = Autotuner(dev, candidates=PLAIN_CANDIDATES if plain else CANDIDATES, base=base,
+                      saved_state=True)
     best, times = tuner.tune(tbatch, spec.event_counts, spec.seed, 0)
     return best, times
 
@@ -368,7 +371,9 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     geom, tune_ms = tune(spec, dev, args, plain=False)
     pgeom, ptune_ms = tune(spec, dev, args, plain=True)
     args.geom = geom
-    plan, step = make_step(spec, dev, geom, rank)
+    # the measured form: saved state (the forward keeps each kept row's
+    # interval and offset, the backward reads them), persistent kernels
+    plan, step = make_step(spec, dev, geom, rank, saved_state=True)
     gen = torch.Generator(device=dev).manual_seed(1000 + rank)
     step.grad_events.normal_(generator=gen)
 
@@ -394,8 +399,8 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     valid = int(step.row_offsets[-1].item())
 
     # ---- plain form: one forward and one backward launch per density, its
-    # own tuned geometry, no graph
-    pplan, pstep = make_step(spec, dev, pgeom, rank)
+    # own tuned geometry, saved state, no graph
+    pplan, pstep = make_step(spec, dev, pgeom, rank, saved_state=True)
     pstep.grad_events.copy_(step.grad_events)
     for _ in range(args.warmup):
         pstep.step()
@@ -408,43 +413,42 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     plain_launch = pplan.config
     del pstep, pplan
 
-    # ---- saved-state form: the forward also writes (interval, offset) per
-    # kept row, the backward reads them instead of replaying the uniforms
-    splan, sstep = make_step(spec, dev, geom, rank, saved_state=True)
-    sstep.grad_events.copy_(step.grad_events)
+    # ---- replay form: no per-row state; the backward regenerates the
+    # uniforms, intervals and compaction ranks
+    rplan, rstep = make_step(spec, dev, geom, rank, saved_state=False)
+    rstep.grad_events.copy_(step.grad_events)
     for _ in range(max(args.warmup, 3)):
-        sstep.step()
+        rstep.step()
     torch.cuda.synchronize(dev)
-    sstep.check_status()
-    s_fwd, s_bwd = time_kernels(sstep, args.steps, stream)
-    sstep.capture()
+    rstep.check_status()
+    r_fwd, r_bwd = time_kernels(rstep, args.steps, stream)
+    rstep.capture()
     for _ in range(args.warmup):
-        sstep.step()
-    state_ms = time_steps(sstep, args.steps, barrier, stream)
-    sstep.check_status()
+        rstep.step()
+    replay_ms = time_steps(rstep, args.steps, barrier, stream)
+    rstep.check_status()
     if dist is not None:
-        state_ms = max_over_ranks(state_ms)
+        replay_ms = max_over_ranks(replay_ms)
     gscale = float(step.grad_values.abs().max().item()) or 1.0
-    saved_state = {
-        "value": events_step / (state_ms * 1e-3), "ms_per_step": state_ms,
-        "kernels_ms": {"batch_forward_kernel": s_fwd, "batch_backward_kernel": s_bwd},
-        "form": "forward writes interval (int32) + offset u - c_j (fp32) per kept row; "
-                "backward reads them, one CUDA graph",
-        "state_bytes": 8 * valid,
-        "events_identical": bool(torch.equal(sstep.events[:valid], step.events[:valid])),
-        "grad_max_diff_over_scale": float((sstep.grad_values - step.grad_values).abs().max()
+    replay = {
+        "value": events_step / (replay_ms * 1e-3), "ms_per_step": replay_ms,
+        "kernels_ms": {"batch_forward_kernel": r_fwd, "batch_backward_kernel": r_bwd},
+        "form": "no per-row state: the backward regenerates uniforms, intervals and "
+                "compaction ranks from (seed, sequence); one CUDA graph",
+        "events_identical": bool(torch.equal(rstep.events[:valid], step.events[:valid])),
+        "grad_max_diff_over_scale": float((rstep.grad_values - step.grad_values).abs().max()
                                           .item()) / gscale,
     }
-    sstep.graph = None
-    del sstep, splan
+    rstep.graph = None
+    del rstep, rplan
 
     # ---- end to end through LOITS(backend="cuda") with host buffers
     e2e = run_e2e(args, spec, dev, rank, world, dist)
 
     # ---- roofline of the dominant kernel
     knots = spec.total_knots
-    fwd_bytes = FWD_B_PER_EVENT * valid + FWD_B_PER_KNOT * knots
-    bwd_bytes = BWD_B_PER_EVENT * valid + BWD_B_PER_KNOT * knots
+    fwd_bytes = (FWD_B_PER_EVENT + STATE_B_PER_EVENT) * valid + FWD_B_PER_KNOT * knots
+    bwd_bytes = (BWD_B_PER_EVENT + STATE_B_PER_EVENT) * valid + BWD_B_PER_KNOT * knots
     kname, k_ms, k_bytes = (("batch_forward_kernel", f_ms, fwd_bytes) if f_ms >= b_ms
                             else ("batch_backward_kernel", b_ms, bwd_bytes))
     peak, peak_kind = hbm_peak()
@@ -452,7 +456,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
     traffic = None
     try:
         t = json.loads(TRAFFIC.read_text())
-        entry = t.get(spec.name, {}).get(kname)
+        entry = t.get(spec.name + "_state", {}).get(kname)
         if entry:
             # measured on this workload; scaled by kept events if they differ
             traffic = entry["bytes_per_launch"] * valid / entry["kept_events"]
@@ -466,21 +470,24 @@ def run_b200(args, spec, rank, world, dist) -> dict:
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic",
-        "config": {**describe(spec), "form": "persistent forward + backward, one CUDA graph",
+        "config": {**describe(spec),
+                   "form": "persistent forward + backward, saved state (interval and offset "
+                           "per kept row, 8 B), one CUDA graph",
                    "parallelism": f"density-sharded x{world} (no collective on the data path)",
-                   "l2": f"per step {4 * valid / 1e6:.0f} MB of events written and "
-                         f"{4 * valid / 1e6:.0f} MB of cotangents read, each larger than the "
-                         "126 MB L2 (no flush)" if 4 * valid > 126e6 else
+                   "l2": f"per step {12 * valid / 1e6:.0f} MB of events and state written "
+                         f"and {12 * valid / 1e6:.0f} MB of cotangents and state read, each "
+                         "larger than the 126 MB L2 (no flush)" if 4 * valid > 126e6 else
                          "inputs smaller than L2: not a valid roofline case",
                    "launch": plan.config, "accepted_events_per_step": valid * world,
                    "tuning_ms_per_step": tune_ms},
         "plain": {"value": events_step / (plain_ms * 1e-3), "ms_per_step": plain_ms,
-                  "form": "one forward + one backward launch per density, no graph",
+                  "form": "one forward + one backward launch per density, saved state, "
+                          "no graph",
                   "launch": plain_launch, "tuning_ms_per_step": ptune_ms,
                   "batched_over_plain": plain_ms / ms, "events_identical": bool(same),
                   "row_offsets_identical": bool(plain_rows_same)},
         "kernels_ms": {"batch_forward_kernel": f_ms, "batch_backward_kernel": b_ms},
-        "saved_state": saved_state,
+        "replay": replay,
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic,

@@ -355,12 +355,14 @@ class BatchedLOITS:
     ``loits_batch_config`` / dict, or ``"auto"``: the launch geometry is timed
     on the first batch of each shape bucket (:mod:`quantom_loits_b200.tuning`).
 
-    ``saved_state``: keep each kept row's interval and offset between forward
-    and backward (8 bytes per row) so that the backward reads them instead of
-    regenerating the uniforms and searching the intervals."""
+    ``saved_state`` (default True): keep each kept row's interval and offset
+    between forward and backward (8 bytes per row, as the reference keeps its
+    uniforms and intervals for its backward) so that the backward reads them;
+    False: keep nothing per row, the backward regenerates the uniforms and
+    searches the intervals again (slower, for callers short of memory)."""
 
     def __init__(self, device="cuda", seed=None, config=None, device_sequence=False,
-                 saved_state=False):
+                 saved_state=True):
         self.device = torch.device(device)
         N.require_device(self.device)
         self.seed = torch.initial_seed() if seed is None else int(seed)
@@ -384,8 +386,9 @@ class BatchedLOITS:
                     raise ValueError(f"unknown config {config!r} (expected 'auto')")
                 from .tuning import default_tuner
 
-                config = make_config(**default_tuner(self.device).config_for(
-                    batch, event_counts, self.seed, self.sequence, hist))
+                tuner = default_tuner(self.device, self.saved_state and hist is None)
+                config = make_config(**tuner.config_for(batch, event_counts, self.seed,
+                                                        self.sequence, hist))
             plan = BatchPlan(knot_offsets, event_counts, config, self.device)
             self._plans[key] = plan
         return plan

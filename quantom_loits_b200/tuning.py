@@ -64,11 +64,14 @@ class Autotuner:
     timing forward + backward on the batch being sampled."""
 
     def __init__(self, device="cuda", candidates=CANDIDATES, reps: int = 3,
-                 cache_path: str | os.PathLike | None = None, base: dict | None = None):
+                 cache_path: str | os.PathLike | None = None, base: dict | None = None,
+                 saved_state: bool = True):
         self.device = torch.device(device)
         self.candidates = tuple(candidates)
         # fields every candidate shares (e.g. plain=1, guide_ratio)
         self.base = dict(base or {})
+        # time the saved-state form (the sampler's default) or the replay form
+        self.saved_state = bool(saved_state)
         self.reps = max(1, int(reps))
         path = cache_path if cache_path is not None else os.environ.get("LOITS_TUNE_CACHE")
         self.cache_path = Path(path) if path else None
@@ -81,17 +84,25 @@ class Autotuner:
             except (OSError, ValueError):
                 pass
 
+    def key_for(self, batch, event_counts=None, hist=None) -> str:
+        """This tuner's table key of a batch: its shape bucket, the fields
+        every candidate shares, the timed form and the histogram mode."""
+        counts = batch.event_counts if event_counts is None else np.asarray(event_counts, np.int64)
+        key = shape_key(batch.knot_offsets, counts, batch.x_cut is not None)
+        for k in sorted(self.base):
+            key += f"-{k}{self.base[k]}"
+        key += "-state" if self.saved_state else "-replay"
+        if hist is not None:
+            key += f"-hist{int(hist[0])}"
+        return key
+
     def config_for(self, batch, event_counts=None, seed: int = 0, sequence: int = 0,
                    hist=None) -> dict:
         """The tuned configuration (a dict for ``make_config``) for this
         batch's shape bucket, timing the candidates on first use.  hist:
         (bins, lo, hi) to time the histogram mode instead of event writing."""
         counts = batch.event_counts if event_counts is None else np.asarray(event_counts, np.int64)
-        key = shape_key(batch.knot_offsets, counts, batch.x_cut is not None)
-        for k in sorted(self.base):
-            key += f"-{k}{self.base[k]}"
-        if hist is not None:
-            key += f"-hist{int(hist[0])}"
+        key = self.key_for(batch, counts, hist)
         with self._lock:
             hit = self.table.get(key)
         if hit is not None:
@@ -128,6 +139,7 @@ class Autotuner:
             except RuntimeError:
                 continue  # geometry not supported for this shape (shared memory)
             events, rows, ws = plan.new_events(), plan.new_row_offsets(), plan.new_workspace()
+            ints, offs = plan.new_state() if self.saved_state else (None, None)
             if hist is not None:
                 bins, lo, hi = int(hist[0]), float(hist[1]), float(hist[2])
                 hbuf = torch.empty((plan.n_densities, bins), dtype=torch.float32,
@@ -140,6 +152,11 @@ class Autotuner:
                                       kept, ws)
                     plan.backward_hist(grid, values, x_cut, seed, sequence, bins, lo, hi, ghist,
                                        grad_values, ws)
+            elif self.saved_state:
+                def step():
+                    plan.forward_state(grid, values, x_cut, seed, sequence, events, rows, ints,
+                                       offs, ws)
+                    plan.backward_state(grid, values, x_cut, ints, offs, cot, grad_values, ws)
             else:
                 def step():
                     plan.forward(grid, values, x_cut, seed, sequence, events, rows, ws)
@@ -163,7 +180,7 @@ class Autotuner:
             if ms < best_ms:
                 best_ms = ms
                 best = dict(self.base, threads=threads, blocks_per_item=blocks, scan_knots=scan)
-            del plan, events, rows, ws
+            del plan, events, rows, ws, ints, offs
         if best is None:
             raise RuntimeError("no launch geometry of the batched sampler fits this batch")
         return best, times
@@ -183,12 +200,12 @@ class Autotuner:
 _DEFAULT: dict[str, Autotuner] = {}
 
 
-def default_tuner(device) -> Autotuner:
-    """Process-wide tuner of a device (shared by every ``BatchedLOITS``
-    created with ``config="auto"``)."""
+def default_tuner(device, saved_state: bool = True) -> Autotuner:
+    """Process-wide tuner of a device and sampler form (shared by every
+    ``BatchedLOITS`` created with ``config="auto"``)."""
     dev = torch.device(device)
-    key = str(dev)
+    key = f"{dev}-{'state' if saved_state else 'replay'}"
     if key not in _DEFAULT:
         N.require_device(dev)
-        _DEFAULT[key] = Autotuner(dev)
+        _DEFAULT[key] = Autotuner(dev, saved_state=saved_state)
     return _DEFAULT[key]
