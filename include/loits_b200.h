@@ -199,6 +199,8 @@ int loits_batch_plan_config(const loits_batch_plan* plan, loits_batch_config* cf
  *   events: capacity fp32 rows; row_offsets: B+1 int64, kept rows of
  *   density b are [row_offsets[b], row_offsets[b+1]);
  *   intervals: capacity int32 (may be NULL), interval of each kept row.
+ * events and intervals start on 16-byte boundaries (rows are written as
+ * vectors of four where they can be). 
  * The workspace keeps the CDF state the backward needs.  Replaces, for a
  * batch, cpp/bindings.cpp:24-130 on the embedded tuple. */
 int loits_batch_forward(const loits_batch_plan* plan, const float* grid, const float* values,
@@ -221,7 +223,8 @@ int loits_batch_backward(const loits_batch_plan* plan, const float* grid, const 
  * reference saves for its backward (u_x / interval_x / packed / row_offsets,
  * openmp/bindings.cpp:85-131, read by interpolation_vjp_x,
  * cpp/loits_core.cpp:268-338): 8 bytes per kept row in row order instead of
- * padded per-slot arrays.  intervals, offsets: capacity entries each. */
+ * padded per-slot arrays.  intervals, offsets: capacity entries each, each
+ * starting on a 16-byte boundary. */
 int loits_batch_forward_state(const loits_batch_plan* plan, const float* grid,
                               const float* values, const float* x_cut, uint64_t seed,
                               uint64_t sequence, float* events, int64_t* row_offsets,

@@ -1085,6 +1085,46 @@ __device__ __forceinline__ uint32_t threshold_keep(uint4 w, int kstar) {
          (static_cast<int>(w.w >> 8) > kstar ? 8u : 0u);
 }
 
+// Rounds of a warp whose first block is wblk0 that hold slots of tile tg's
+// density: all R for a full tile, else up to the density's last block (a
+// warp past it has none).
+template <int R>
+__device__ __forceinline__ int warp_rounds(const TileGeom& tg, int64_t wblk0, bool full) {
+  if (full) return R;
+  if (tg.n <= 0) return 0;
+  const int64_t last = (tg.P0 + tg.n - 1) >> 2;  // the density's last block
+  const int64_t k = last - wblk0;
+  return k < 0 ? 0 : static_cast<int>(k / 32 + 1 < R ? k / 32 + 1 : R);
+}
+
+// Stores the kept slots of one Philox block at rows p, p + 1, ... in slot
+// order: events, and intervals / offsets when the launch writes them.
+__device__ __forceinline__ void store_kept(const BatchArgs& a, int64_t p, uint32_t keep,
+                                           const Slot& e0, const Slot& e1, const Slot& e2,
+                                           const Slot& e3) {
+  if (!keep) return;
+  const int c1 = keep & 1u, c2 = c1 + ((keep >> 1) & 1u), c3 = c2 + ((keep >> 2) & 1u);
+  float* ev = a.events + p;
+  if (keep & 1u) __stcs(ev, e0.x);
+  if (keep & 2u) __stcs(ev + c1, e1.x);
+  if (keep & 4u) __stcs(ev + c2, e2.x);
+  if (keep & 8u) __stcs(ev + c3, e3.x);
+  if (a.intervals) {
+    int32_t* iv = a.intervals + p;
+    if (keep & 1u) __stcs(iv, e0.j);
+    if (keep & 2u) __stcs(iv + c1, e1.j);
+    if (keep & 4u) __stcs(iv + c2, e2.j);
+    if (keep & 8u) __stcs(iv + c3, e3.j);
+  }
+  if (a.offsets) {
+    float* ov = a.offsets + p;
+    if (keep & 1u) __stcs(ov, e0.t);
+    if (keep & 2u) __stcs(ov + c1, e1.t);
+    if (keep & 4u) __stcs(ov + c2, e2.t);
+    if (keep & 8u) __stcs(ov + c3, e3.t);
+  }
+}
+
 // Tile of a kThreshold density: each warp counts its kept slots from the
 // Philox words alone, the tile publishes its count and takes its first row
 // from the look-back, then every warp samples and stores its kept events
@@ -1097,13 +1137,16 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int kstar = d.kstar;
   const bool full = tile_full<TPB, R>(tg);
+  const uint64_t sid = stream_of(a);
+  const int64_t wblk0 = tg.blk0 + static_cast<int64_t>(warp * R) * 32;
+  const int rounds = warp_rounds<R>(tg, wblk0, full);
   int cnt = 0;
 #pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+  for (int r = 0; r < rounds; ++r) {
+    const int64_t blk = wblk0 + r * 32 + lane;
     const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
     if (!range) continue;
-    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), sid, a.rk);
     cnt += __popc(threshold_keep(w, kstar) & range);
   }
   cnt = warp_sum(cnt);
@@ -1124,39 +1167,16 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
   __syncthreads();
   int64_t row = sh.base + warp_excl;
 #pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+  for (int r = 0; r < rounds; ++r) {
+    const int64_t blk = wblk0 + r * 32 + lane;
     const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
-    uint32_t keep = 0;
-    Slot e0, e1, e2, e3;
-    if (range) {
-      const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
-      keep = threshold_keep(w, kstar) & range;
-      e0 = sample_slot<kMode>(d, w.x);
-      e1 = sample_slot<kMode>(d, w.y);
-      e2 = sample_slot<kMode>(d, w.z);
-      e3 = sample_slot<kMode>(d, w.w);
-    }
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), sid, a.rk);
+    const uint32_t keep = threshold_keep(w, kstar) & range;
     int total;
-    int64_t pos = row + warp_exclusive_count(__popc(keep), total);
-    if (a.intervals) {
-      int64_t q = pos;
-      if (keep & 1u) a.intervals[q++] = e0.j;
-      if (keep & 2u) a.intervals[q++] = e1.j;
-      if (keep & 4u) a.intervals[q++] = e2.j;
-      if (keep & 8u) a.intervals[q] = e3.j;
-    }
-    if (a.offsets) {
-      int64_t q = pos;
-      if (keep & 1u) a.offsets[q++] = e0.t;
-      if (keep & 2u) a.offsets[q++] = e1.t;
-      if (keep & 4u) a.offsets[q++] = e2.t;
-      if (keep & 8u) a.offsets[q] = e3.t;
-    }
-    if (keep & 1u) __stcs(&a.events[pos++], e0.x);
-    if (keep & 2u) __stcs(&a.events[pos++], e1.x);
-    if (keep & 4u) __stcs(&a.events[pos++], e2.x);
-    if (keep & 8u) __stcs(&a.events[pos], e3.x);
+    const int excl = warp_exclusive_count(__popc(keep), total);
+    const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
+    const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
+    store_kept(a, row + excl, keep, e0, e1, e2, e3);
     row += total;
   }
 }
@@ -1173,34 +1193,30 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, const TileGe
   tile_slot_range<TPB, R>(tg, s_lo, s_hi);
   const int64_t shiftrow = base - s_lo;
   const bool full = tile_full<TPB, R>(tg);
+  const uint64_t sid = stream_of(a);
+  const int64_t wblk0 = tg.blk0 + static_cast<int64_t>(warp * R) * 32;
+  const int rounds = warp_rounds<R>(tg, wblk0, full);
 #pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+  for (int r = 0; r < rounds; ++r) {
+    const int64_t blk = wblk0 + r * 32 + lane;
     const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
     if (!range) continue;
-    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
+    const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), sid, a.rk);
     const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
     const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
     const int64_t row0 = (blk << 2) + shiftrow;
     if (range == 0xfu && (row0 & 3) == 0) {
+      // rows row0 .. row0 + 3, 16-byte aligned (events, intervals and offsets
+      // buffers start on 16-byte boundaries)
       __stcs(reinterpret_cast<float4*>(a.events + row0), make_float4(e0.x, e1.x, e2.x, e3.x));
+      if (a.intervals)
+        __stcs(reinterpret_cast<int4*>(a.intervals + row0), make_int4(e0.j, e1.j, e2.j, e3.j));
+      if (a.offsets)
+        __stcs(reinterpret_cast<float4*>(a.offsets + row0), make_float4(e0.t, e1.t, e2.t, e3.t));
     } else {
-      if (range & 1u) a.events[row0] = e0.x;
-      if (range & 2u) a.events[row0 + 1] = e1.x;
-      if (range & 4u) a.events[row0 + 2] = e2.x;
-      if (range & 8u) a.events[row0 + 3] = e3.x;
-    }
-    if (a.intervals) {
-      if (range & 1u) a.intervals[row0] = e0.j;
-      if (range & 2u) a.intervals[row0 + 1] = e1.j;
-      if (range & 4u) a.intervals[row0 + 2] = e2.j;
-      if (range & 8u) a.intervals[row0 + 3] = e3.j;
-    }
-    if (a.offsets) {
-      if (range & 1u) a.offsets[row0] = e0.t;
-      if (range & 2u) a.offsets[row0 + 1] = e1.t;
-      if (range & 4u) a.offsets[row0 + 2] = e2.t;
-      if (range & 8u) a.offsets[row0 + 3] = e3.t;
+      // the kept (in-range) slots at consecutive rows from the first one's
+      const int first = __ffs(range) - 1;
+      store_kept(a, row0 + first, range, e0, e1, e2, e3);
     }
   }
 }

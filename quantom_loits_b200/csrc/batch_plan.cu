@@ -861,6 +861,7 @@ extern "C" int loits_batch_forward(const loits_batch_plan* p, const float* grid,
                                    int32_t* intervals, void* workspace, void* stream) {
   if (!p || !grid || !values || !row_offsets || !workspace) return LOITS_ERR_INVALID;
   if (p->capacity > 0 && (!events || !aligned16(events))) return LOITS_ERR_INVALID;
+  if (intervals && !aligned16(intervals)) return LOITS_ERR_INVALID;
   if (!aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -895,7 +896,9 @@ extern "C" int loits_batch_forward_state(const loits_batch_plan* p, const float*
                                          void* stream) {
   if (p && p->capacity > 0 && (!intervals || !offsets)) return LOITS_ERR_INVALID;
   if (!p || !grid || !values || !row_offsets || !workspace) return LOITS_ERR_INVALID;
-  if (p->capacity > 0 && (!events || !aligned16(events))) return LOITS_ERR_INVALID;
+  if (p->capacity > 0 && (!events || !aligned16(events) || !aligned16(intervals) ||
+                          !aligned16(offsets)))
+    return LOITS_ERR_INVALID;
   if (!aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
