@@ -762,15 +762,38 @@ def run_tuple_b200(args, spec, rank, world, dist) -> dict:
         dist.barrier()
     torch.cuda.synchronize(dev)
     t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    # eager form: the reference call's shape, two host round trips per forward
+    t0.record(stream)
+    for _ in range(args.steps):
+        step()
+    t1.record(stream)
+    torch.cuda.synchronize(dev)
+    eager_ms = t0.elapsed_time(t1) / args.steps
+    if dist is not None:
+        eager_ms = max_over_ranks(eager_ms)
+    # measured form: forward + backward captured in one CUDA graph, counts
+    # kept on the device (TupleStep)
+    tstep = BK.TupleStep(*t, spec.n_events, spec.seed, seq)
+    tstep.grad_events.normal_(generator=gen)
+    tstep.capture()
+    for _ in range(args.warmup):
+        tstep.step()
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
     with ClockSampler(dev.index) as clocks:
         t0.record(stream)
         for _ in range(args.steps):
-            step()
+            tstep.step()
         t1.record(stream)
         torch.cuda.synchronize(dev)
+    tstep.check_status()
     ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
         ms = max_over_ranks(ms)
+    graph_same = bool(torch.equal(tstep.result()[0], ev))
+    tstep.graph = None
+    del tstep
     value = spec.n_events * world / (ms * 1e-3)
 
     # end to end through LOITS(backend="cuda") with host buffers
@@ -837,13 +860,19 @@ def run_tuple_b200(args, spec, rank, world, dist) -> dict:
                    "l2": "events + cotangent " + ("larger" if 32 * valid > 126e6 else "smaller")
                          + " than the 126 MB L2 (no flush)"},
         "kernels_ms": {"forward (prepare + sample)": fm, "backward": bm},
+        "form": "TupleStep: prepare + bounded sample + backward in one CUDA graph, counts on "
+                "the device",
+        "eager": {"value": spec.n_events * world / (eager_ms * 1e-3), "ms_per_step": eager_ms,
+                  "form": "tuple_forward + tuple_backward, two host round trips per forward",
+                  "graph_events_identical": graph_same},
         "roofline": {"bound": "hbm", "kernel": kname, "achieved": achieved, "peak": peak,
                      "peak_kind": peak_kind, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": traffic, "algorithmic_bytes": k_bytes},
         "e2e": {"value": spec.n_events * world / (e_ms * 1e-3), "unit": "events/s",
                 "ms_per_step": e_ms, "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                 "api": "LOITS(backend='cuda')(theory_outputs, n_events) + autograd backward"},
-        "gpu_launches": 3 * args.steps,
+        # per step: prepare (2 kernels), sample (1), backward (4)
+        "gpu_launches": 7 * args.steps,
         "clocks": clocks.summary(),
     }
     if rank == 0:

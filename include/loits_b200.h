@@ -123,6 +123,23 @@ int loits_tuple_sample_noalloc(const loits_shape* shape, const double* x_bins,
                                int64_t* packed, int16_t* interval_x, int16_t* interval_q,
                                int64_t* valid, int32_t* status, void* stream);
 
+/* loits_tuple_sample with the counts left on the device, for a caller that
+ * must not wait for them (a CUDA graph replaying prepare + sample + backward
+ * of a fixed tuple): alloc is loits_tuple_prepare's {nmax, active} in device
+ * memory; capacity, a host-known upper bound on active (at most
+ * trunc(|w| * n_events) slots per cell: n_events * sum |w| bounds it), sizes
+ * the launch, the outputs (capacity rows) and the workspace
+ * (loits_tuple_sample_workspace(capacity)).  valid receives the kept rows;
+ * an active count above capacity samples nothing and sets status to
+ * LOITS_ERR_CAPACITY.  Results equal loits_tuple_sample's. */
+int loits_tuple_sample_bounded(const loits_shape* shape, const double* x_bins,
+                               const double* q_bins, const double* cdf_x, const double* cdf_q,
+                               const int64_t* cell_offsets, const int64_t* alloc,
+                               int64_t capacity, uint64_t seed, uint64_t sequence,
+                               double* events, int64_t* packed, int16_t* interval_x,
+                               int16_t* interval_q, int64_t* valid, int32_t* status,
+                               void* workspace, size_t workspace_bytes, void* stream);
+
 /* Bytes of device workspace loits_tuple_backward needs for nvalid rows. */
 size_t loits_tuple_backward_workspace(const loits_shape* shape, int64_t nvalid);
 
@@ -141,6 +158,21 @@ int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
                          const double* norm_x, const double* norm_q, const double* cdf_x,
                          const double* cdf_q, double* grad_xsec_x, double* grad_xsec_q,
                          void* workspace, size_t workspace_bytes, void* stream);
+
+/* loits_tuple_backward of a loits_tuple_sample_bounded forward: the kept-row
+ * count (valid) and nmax (alloc[0]) are read on the device; capacity (the
+ * forward's) bounds the rows and sizes the workspace
+ * (loits_tuple_backward_workspace(shape, capacity)); grad_events and packed
+ * hold capacity rows, of which the first *valid are used. */
+int loits_tuple_backward_bounded(const loits_shape* shape, const double* grad_events,
+                                 const int64_t* packed, const int64_t* valid,
+                                 const int64_t* alloc, int64_t capacity, uint64_t seed,
+                                 uint64_t sequence, const double* x_bins, const double* xsec_x,
+                                 const double* q_bins, const double* xsec_q,
+                                 const uint8_t* acceptance, const double* norm_x,
+                                 const double* norm_q, const double* cdf_x, const double* cdf_q,
+                                 double* grad_xsec_x, double* grad_xsec_q, void* workspace,
+                                 size_t workspace_bytes, void* stream);
 
 /* ------------------------------------------------ batch (fp32, ragged 1-D) */
 

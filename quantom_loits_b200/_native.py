@@ -65,10 +65,16 @@ SIGNATURES = {
                                      _u64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _sz, _vp]),
     "loits_tuple_sample_noalloc": (C.c_int, [C.POINTER(Shape), _vp, _vp, _vp, _vp, _vp, _i64, _i64,
                                              _u64, _u64, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "loits_tuple_sample_bounded": (C.c_int, [C.POINTER(Shape), _vp, _vp, _vp, _vp, _vp, _vp,
+                                             _i64, _u64, _u64, _vp, _vp, _vp, _vp, _vp, _vp,
+                                             _vp, _sz, _vp]),
     "loits_tuple_backward_workspace": (_sz, [C.POINTER(Shape), _i64]),
     "loits_tuple_backward": (C.c_int, [C.POINTER(Shape), _vp, _vp, _i64, _i64, _u64, _u64, _vp,
                                        _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
                                        _sz, _vp]),
+    "loits_tuple_backward_bounded": (C.c_int, [C.POINTER(Shape), _vp, _vp, _vp, _vp, _i64, _u64,
+                                               _u64, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp,
+                                               _vp, _vp, _vp, _vp, _sz, _vp]),
     "loits_batch_plan_create": (C.c_int, [_i64, _vp, _vp, C.POINTER(BatchConfig),
                                           C.POINTER(_vp)]),
     "loits_batch_plan_destroy": (None, [_vp]),

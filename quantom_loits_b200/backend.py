@@ -28,6 +28,7 @@ reference; inside them the fused launches are ``loits::forward::prepare``
 from __future__ import annotations
 
 import ctypes as C
+import math
 from contextlib import contextmanager, nullcontext
 
 import torch
@@ -180,6 +181,129 @@ def tuple_backward(grad_events, x_bins, xsec_x, q_bins, xsec_q, acceptance, stat
         with _region(profile_regions, "loits::backward::state_pack"):
             pass
     return gx, gq
+
+
+class TupleStep:
+    """Forward + backward of the reference theory tuple on static buffers, so
+    that both can be captured in one CUDA graph (``capture()``, then
+    ``step()`` replays it).
+
+    The reference's call returns (valid, 2) events: a shape the host learns
+    only by waiting for the device (twice per forward in ``tuple_forward``).
+    Here every count stays on the device: prepare writes {nmax, active}, the
+    sampler covers a host-known bound on active -- each cell draws
+    trunc(|w| n_events) slots, so n_events * sum |w| bounds the total; the
+    weights are read once, here -- and writes the kept-row count to
+    ``valid``, which the backward reads.  ``events`` (capacity x 2) and
+    ``packed`` hold ``capacity`` rows, the first ``valid`` of them the sample
+    (the same rows, bit for bit, as ``tuple_forward``); put the cotangent of
+    those rows into ``grad_events`` before each backward.  The inputs are the
+    caller's tensors, read in place at every step; seed and sequence are
+    fixed.  ``grad_xsec_x`` / ``grad_xsec_q`` receive the gradients."""
+
+    def __init__(self, x_bins, xsec_x, q_bins, xsec_q, weights, acceptance, n_events, seed,
+                 sequence=0):
+        shape = _check_tuple(x_bins, xsec_x, q_bins, xsec_q, weights, acceptance)
+        n_events = int(n_events)
+        if n_events < 0:
+            raise ValueError("n_events must be >= 0")
+        dev = x_bins.device
+        self.device, self.shape = dev, shape
+        self.inputs = (x_bins, xsec_x, q_bins, xsec_q, weights, acceptance)
+        self.n_events, self.seed, self.sequence = n_events, int(seed), int(sequence)
+        B, nx, ny = shape.batch, shape.nx, shape.ny
+        ncell = B * nx * ny
+        w_sum = float(weights.abs().sum().item())  # the only host read, at set-up
+        self.capacity = max(int(math.ceil(n_events * w_sum * (1.0 + 1e-12))) + ncell, 1)
+        f64 = dict(dtype=torch.float64, device=dev)
+        i64 = dict(dtype=torch.int64, device=dev)
+        self.counts = torch.empty(ncell, **i64)
+        self.cell_offsets = torch.empty(ncell + 1, **i64)
+        self.norm_x = torch.empty((B, ny, nx), **f64)
+        self.norm_q = torch.empty((B, nx, ny), **f64)
+        self.cdf_x = torch.empty_like(xsec_x)
+        self.cdf_q = torch.empty_like(xsec_q)
+        self.alloc = torch.zeros(2, **i64)
+        self.events = torch.zeros((self.capacity, 2), **f64)
+        self.packed = torch.zeros(self.capacity, **i64)
+        self.valid = torch.zeros(1, **i64)
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
+        lib = N.lib()
+        self.ws_sample = torch.empty(max(int(lib.loits_tuple_sample_workspace(self.capacity)), 16),
+                                     dtype=torch.uint8, device=dev)
+        self.grad_events = torch.zeros((self.capacity, 2), **f64)
+        self.grad_xsec_x = torch.empty_like(xsec_x)
+        self.grad_xsec_q = torch.empty_like(xsec_q)
+        nb = int(lib.loits_tuple_backward_workspace(C.byref(shape), self.capacity))
+        self.ws_backward = torch.empty(max(nb, 16), dtype=torch.uint8, device=dev)
+        self.graph = None
+
+    def forward(self):
+        x_bins, xsec_x, q_bins, xsec_q, weights, acceptance = self.inputs
+        lib = N.lib()
+        with torch.cuda.device(self.device):
+            stream = N.stream_of(self.device)
+            N.check(lib.loits_tuple_prepare(C.byref(self.shape), x_bins.data_ptr(),
+                                            xsec_x.data_ptr(), q_bins.data_ptr(),
+                                            xsec_q.data_ptr(), weights.data_ptr(),
+                                            acceptance.view(torch.uint8).data_ptr(),
+                                            self.n_events, self.counts.data_ptr(),
+                                            self.cell_offsets.data_ptr(), self.norm_x.data_ptr(),
+                                            self.norm_q.data_ptr(), self.cdf_x.data_ptr(),
+                                            self.cdf_q.data_ptr(), self.alloc.data_ptr(), stream),
+                    "loits_tuple_prepare")
+            N.check(lib.loits_tuple_sample_bounded(
+                C.byref(self.shape), x_bins.data_ptr(), q_bins.data_ptr(), self.cdf_x.data_ptr(),
+                self.cdf_q.data_ptr(), self.cell_offsets.data_ptr(), self.alloc.data_ptr(),
+                self.capacity, self.seed, self.sequence, self.events.data_ptr(),
+                self.packed.data_ptr(), None, None, self.valid.data_ptr(), self.status.data_ptr(),
+                self.ws_sample.data_ptr(), self.ws_sample.numel(), stream),
+                "loits_tuple_sample_bounded")
+
+    def backward(self):
+        x_bins, xsec_x, q_bins, xsec_q, _, acceptance = self.inputs
+        with torch.cuda.device(self.device):
+            N.check(N.lib().loits_tuple_backward_bounded(
+                C.byref(self.shape), self.grad_events.data_ptr(), self.packed.data_ptr(),
+                self.valid.data_ptr(), self.alloc.data_ptr(), self.capacity, self.seed,
+                self.sequence, x_bins.data_ptr(), xsec_x.data_ptr(), q_bins.data_ptr(),
+                xsec_q.data_ptr(), acceptance.view(torch.uint8).data_ptr(),
+                self.norm_x.data_ptr(), self.norm_q.data_ptr(), self.cdf_x.data_ptr(),
+                self.cdf_q.data_ptr(), self.grad_xsec_x.data_ptr(), self.grad_xsec_q.data_ptr(),
+                self.ws_backward.data_ptr(), self.ws_backward.numel(), N.stream_of(self.device)),
+                "loits_tuple_backward_bounded")
+
+    def step(self):
+        if self.graph is not None:
+            self.graph.replay()
+        else:
+            self.forward()
+            self.backward()
+
+    def capture(self):
+        """Capture forward + backward into one CUDA graph (warms up first)."""
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(torch.cuda.current_stream(self.device))
+        with torch.cuda.stream(side):
+            self.forward()
+            self.backward()
+        torch.cuda.current_stream(self.device).wait_stream(side)
+        torch.cuda.synchronize(self.device)
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            self.forward()
+            self.backward()
+        self.graph = g
+        return g
+
+    def check_status(self):
+        """Synchronising read of the device status word."""
+        N.check(int(self.status.item()), "loits_tuple_sample_bounded (device)")
+
+    def result(self):
+        """(events, packed) of the last step: the first ``valid`` rows (a sync)."""
+        n = int(self.valid.item())
+        return self.events[:n], self.packed[:n]
 
 
 def fill_uniform(count: int, seed: int, stream_id: int, device="cuda") -> torch.Tensor:

@@ -179,6 +179,9 @@ struct TupleSampleArgs {
   uint32_t* ticket;
   unsigned long long* tile_state;
   int64_t n_tiles;
+  const int64_t* alloc;  // when set: {nmax, active} read here (the launch has n_tiles for
+                         // `capacity` active slots, an upper bound)
+  int64_t capacity;
 };
 
 // Three CTAs per SM (80 registers, no spills) instead of two at 118.
@@ -189,6 +192,18 @@ __global__ void __launch_bounds__(kSampleThreads, 3) tuple_sample_kernel(TupleSa
   if (threadIdx.x == 0) s_tile = atomicAdd(a.ticket, 1u);
   __syncthreads();
   const int64_t tile = s_tile;
+  if (a.alloc) {
+    // counts on the device: the launch covers `capacity` slots; a larger
+    // count is an error (nothing sampled), tiles past the count do nothing
+    a.nmax = a.alloc[0];
+    a.active = a.alloc[1];
+    if (a.active > a.capacity) {
+      if (tile == 0 && threadIdx.x == 0) raise_status(a.status, LOITS_ERR_CAPACITY);
+      return;
+    }
+    a.n_tiles = (a.active + kSampleTile - 1) / kSampleTile;
+    if (tile >= a.n_tiles) return;  // the whole CTA: no later tile waits on it
+  }
   const int64_t ncell = a.g.batch * a.g.cells;
   const int64_t e0 = tile * kSampleTile + threadIdx.x * kSampleEPT;
 
@@ -280,6 +295,8 @@ struct TupleBackwardArgs {
   const double* cdf_q;
   double* grad_x;
   double* grad_q;
+  const int64_t* valid_dev;  // when set: the kept-row count (nvalid is then an upper bound)
+  const int64_t* nmax_dev;   // when set: nmax
 };
 
 // First row whose packed index is >= key (packed is strictly increasing).
@@ -348,12 +365,15 @@ constexpr int kChunkRows = 256;
 __global__ void tuple_rows_kernel(TupleBackwardArgs a, int64_t* __restrict__ cell_rows,
                                   int64_t* __restrict__ chunks) {
   const int64_t ncell = a.g.batch * a.g.cells;
+  int64_t nvalid = a.nvalid, nmax = a.nmax;
+  if (a.valid_dev) nvalid = min(*a.valid_dev, nvalid);
+  if (a.nmax_dev) nmax = *a.nmax_dev;
   for (int64_t c = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; c <= ncell;
        c += (int64_t)gridDim.x * blockDim.x) {
-    const int64_t r0 = lower_bound_i64(a.packed, a.nvalid, c * a.nmax);
+    const int64_t r0 = lower_bound_i64(a.packed, nvalid, c * nmax);
     cell_rows[c] = r0;
     if (c < ncell) {
-      const int64_t r1 = lower_bound_i64(a.packed, a.nvalid, (c + 1) * a.nmax);
+      const int64_t r1 = lower_bound_i64(a.packed, nvalid, (c + 1) * nmax);
       chunks[c] = (r1 - r0 + kChunkRows - 1) / kChunkRows;
     }
   }
@@ -567,16 +587,20 @@ extern "C" size_t loits_tuple_sample_workspace(int64_t active) {
   return 16 + static_cast<size_t>(tiles) * sizeof(unsigned long long);
 }
 
-extern "C" int loits_tuple_sample(const loits_shape* shape, const double* x_bins,
-                                  const double* q_bins, const double* cdf_x, const double* cdf_q,
-                                  const int64_t* cell_offsets, int64_t nmax, int64_t active,
-                                  uint64_t seed, uint64_t sequence, double* events,
-                                  int64_t* packed, int16_t* interval_x, int16_t* interval_q,
-                                  int64_t* valid, int32_t* status, void* workspace,
-                                  size_t workspace_bytes, void* stream) {
+namespace {
+
+// The sampling launch; alloc (device {nmax, active}) set: active is the
+// capacity the launch covers and the counts are read on the device.
+int tuple_sample_launch(const loits_shape* shape, const double* x_bins, const double* q_bins,
+                        const double* cdf_x, const double* cdf_q, const int64_t* cell_offsets,
+                        int64_t nmax, int64_t active, const int64_t* alloc, uint64_t seed,
+                        uint64_t sequence, double* events, int64_t* packed, int16_t* interval_x,
+                        int16_t* interval_q, int64_t* valid, int32_t* status, void* workspace,
+                        size_t workspace_bytes, void* stream) {
   if (!valid_shape(shape) || nmax < 0 || active < 0 || !valid || !status) return LOITS_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
   if (cudaMemsetAsync(status, 0, sizeof(int32_t), st) != cudaSuccess) return LOITS_ERR_CUDA;
+  if (alloc && cudaMemsetAsync(valid, 0, sizeof(int64_t), st) != cudaSuccess) return LOITS_ERR_CUDA;
   if (active == 0) return launch_status(cudaMemsetAsync(valid, 0, sizeof(int64_t), st));
   if (!x_bins || !q_bins || !cdf_x || !cdf_q || !cell_offsets || !events || !packed || !workspace)
     return LOITS_ERR_INVALID;
@@ -605,9 +629,39 @@ extern "C" int loits_tuple_sample(const loits_shape* shape, const double* x_bins
   a.ticket = static_cast<uint32_t*>(workspace);
   a.tile_state = reinterpret_cast<unsigned long long*>(static_cast<char*>(workspace) + 16);
   a.n_tiles = (active + kSampleTile - 1) / kSampleTile;
+  a.alloc = alloc;
+  a.capacity = active;
   if (a.n_tiles > 0x7fffffff) return LOITS_ERR_UNSUPPORTED;
   tuple_sample_kernel<<<static_cast<unsigned>(a.n_tiles), kSampleThreads, 0, st>>>(a);
   return launch_status(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" int loits_tuple_sample(const loits_shape* shape, const double* x_bins,
+                                  const double* q_bins, const double* cdf_x, const double* cdf_q,
+                                  const int64_t* cell_offsets, int64_t nmax, int64_t active,
+                                  uint64_t seed, uint64_t sequence, double* events,
+                                  int64_t* packed, int16_t* interval_x, int16_t* interval_q,
+                                  int64_t* valid, int32_t* status, void* workspace,
+                                  size_t workspace_bytes, void* stream) {
+  return tuple_sample_launch(shape, x_bins, q_bins, cdf_x, cdf_q, cell_offsets, nmax, active,
+                             nullptr, seed, sequence, events, packed, interval_x, interval_q,
+                             valid, status, workspace, workspace_bytes, stream);
+}
+
+extern "C" int loits_tuple_sample_bounded(const loits_shape* shape, const double* x_bins,
+                                          const double* q_bins, const double* cdf_x,
+                                          const double* cdf_q, const int64_t* cell_offsets,
+                                          const int64_t* alloc, int64_t capacity, uint64_t seed,
+                                          uint64_t sequence, double* events, int64_t* packed,
+                                          int16_t* interval_x, int16_t* interval_q,
+                                          int64_t* valid, int32_t* status, void* workspace,
+                                          size_t workspace_bytes, void* stream) {
+  if (!alloc) return LOITS_ERR_INVALID;
+  return tuple_sample_launch(shape, x_bins, q_bins, cdf_x, cdf_q, cell_offsets, 0, capacity,
+                             alloc, seed, sequence, events, packed, interval_x, interval_q,
+                             valid, status, workspace, workspace_bytes, stream);
 }
 
 namespace {
@@ -645,15 +699,16 @@ extern "C" size_t loits_tuple_backward_workspace(const loits_shape* shape, int64
   return backward_layout(geom_of(shape), nvalid).total;
 }
 
-extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
-                                    const int64_t* packed, int64_t nvalid, int64_t nmax,
-                                    uint64_t seed, uint64_t sequence, const double* x_bins,
-                                    const double* xsec_x, const double* q_bins,
-                                    const double* xsec_q, const uint8_t* acceptance,
-                                    const double* norm_x, const double* norm_q,
-                                    const double* cdf_x, const double* cdf_q,
-                                    double* grad_xsec_x, double* grad_xsec_q, void* workspace,
-                                    size_t workspace_bytes, void* stream) {
+namespace {
+
+int tuple_backward_launch(const loits_shape* shape, const double* grad_events,
+                          const int64_t* packed, int64_t nvalid, int64_t nmax,
+                          const int64_t* valid_dev, const int64_t* nmax_dev, uint64_t seed,
+                          uint64_t sequence, const double* x_bins, const double* xsec_x,
+                          const double* q_bins, const double* xsec_q, const uint8_t* acceptance,
+                          const double* norm_x, const double* norm_q, const double* cdf_x,
+                          const double* cdf_q, double* grad_xsec_x, double* grad_xsec_q,
+                          void* workspace, size_t workspace_bytes, void* stream) {
   if (!valid_shape(shape) || nvalid < 0 || nmax < 0) return LOITS_ERR_INVALID;
   const TupleGeom g = geom_of(shape);
   const int64_t ncell = g.batch * g.cells;
@@ -685,6 +740,8 @@ extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad
   a.cdf_q = cdf_q;
   a.grad_x = grad_xsec_x;
   a.grad_q = grad_xsec_q;
+  a.valid_dev = valid_dev;
+  a.nmax_dev = nmax_dev;
   char* ws = static_cast<char*>(workspace);
   int64_t* cell_rows = reinterpret_cast<int64_t*>(ws + L.cell_rows);
   int64_t* chunks = reinterpret_cast<int64_t*>(ws + L.chunks);
@@ -727,6 +784,41 @@ extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad
   tuple_cell_kernel<<<static_cast<unsigned>(blocks), wpc * 32, smem, st>>>(a, chunk_first,
                                                                           partials);
   return launch_status(cudaGetLastError());
+}
+
+}  // namespace
+
+extern "C" int loits_tuple_backward(const loits_shape* shape, const double* grad_events,
+                                    const int64_t* packed, int64_t nvalid, int64_t nmax,
+                                    uint64_t seed, uint64_t sequence, const double* x_bins,
+                                    const double* xsec_x, const double* q_bins,
+                                    const double* xsec_q, const uint8_t* acceptance,
+                                    const double* norm_x, const double* norm_q,
+                                    const double* cdf_x, const double* cdf_q,
+                                    double* grad_xsec_x, double* grad_xsec_q, void* workspace,
+                                    size_t workspace_bytes, void* stream) {
+  return tuple_backward_launch(shape, grad_events, packed, nvalid, nmax, nullptr, nullptr, seed,
+                               sequence, x_bins, xsec_x, q_bins, xsec_q, acceptance, norm_x,
+                               norm_q, cdf_x, cdf_q, grad_xsec_x, grad_xsec_q, workspace,
+                               workspace_bytes, stream);
+}
+
+extern "C" int loits_tuple_backward_bounded(const loits_shape* shape, const double* grad_events,
+                                            const int64_t* packed, const int64_t* valid,
+                                            const int64_t* alloc, int64_t capacity,
+                                            uint64_t seed, uint64_t sequence,
+                                            const double* x_bins, const double* xsec_x,
+                                            const double* q_bins, const double* xsec_q,
+                                            const uint8_t* acceptance, const double* norm_x,
+                                            const double* norm_q, const double* cdf_x,
+                                            const double* cdf_q, double* grad_xsec_x,
+                                            double* grad_xsec_q, void* workspace,
+                                            size_t workspace_bytes, void* stream) {
+  if (!valid || !alloc) return LOITS_ERR_INVALID;
+  return tuple_backward_launch(shape, grad_events, packed, capacity, 0, valid, alloc, seed,
+                               sequence, x_bins, xsec_x, q_bins, xsec_q, acceptance, norm_x,
+                               norm_q, cdf_x, cdf_q, grad_xsec_x, grad_xsec_q, workspace,
+                               workspace_bytes, stream);
 }
 
 // ============================================== allocation-free sampling call

@@ -170,3 +170,51 @@ def test_large_tuple_matches_oracle(backend, oracle_lib):
     rgx, rgq = oracle_lib.r_backward(g, ref, x_bins, xsec_x, q_bins, xsec_q, acc, seed, seq)
     np.testing.assert_allclose(gx.cpu().numpy(), rgx, rtol=1e-9, atol=1e-10)
     np.testing.assert_allclose(gq.cpu().numpy(), rgq, rtol=1e-9, atol=1e-10)
+
+
+@pytest.mark.parametrize("name", TUPLE_CASES[:3])
+def test_tuple_step_captured_in_one_graph(backend, golden, name):
+    """Forward + backward of the reference tuple captured in one CUDA graph
+    (counts kept on the device, outputs sized by n_events * sum |w|): every
+    replay gives the events, packed rows and gradients of the eager
+    tuple_forward / tuple_backward, bit for bit."""
+    c = golden_case(golden, name)
+    n_events, seed, seq = (int(v) for v in c["scalars"])
+    t = tensors(c)
+    events, st = backend.tuple_forward(*t, n_events, seed, seq)
+    valid = events.shape[0]
+    g = torch.randn((valid, 2), generator=torch.Generator(device=DEV).manual_seed(4),
+                    device=DEV, dtype=torch.float64)
+    gx, gq = backend.tuple_backward(g, t[0], t[1], t[2], t[3], t[5], st, seed, seq)
+    step = backend.TupleStep(*t, n_events, seed, seq)
+    assert step.capacity >= st["active"]
+    step.grad_events.zero_()
+    step.grad_events[:valid] = g
+    step.capture()
+    for _ in range(2):
+        step.events.zero_()
+        step.grad_xsec_x.zero_()
+        step.step()
+        torch.cuda.synchronize()
+        step.check_status()
+        ev, packed = step.result()
+        assert torch.equal(ev, events) and torch.equal(packed, st["packed"])
+        assert torch.equal(step.grad_xsec_x, gx) and torch.equal(step.grad_xsec_q, gq)
+
+
+def test_tuple_step_reports_a_capacity_overrun(backend, golden):
+    """Weights raised after the step was sized: the sampler writes nothing
+    and reports LOITS_ERR_CAPACITY on the device instead of overrunning."""
+    from quantom_loits_b200 import _native as N
+
+    c = golden_case(golden, TUPLE_CASES[0])
+    n_events, seed, seq = (int(v) for v in c["scalars"])
+    t = list(tensors(c))
+    step = backend.TupleStep(*t, n_events, seed, seq)
+    t[4].mul_(4.0)  # the step reads the caller's weights in place
+    step.forward()
+    torch.cuda.synchronize()
+    with pytest.raises(N.LoitsError) as err:
+        step.check_status()
+    assert err.value.code == N.LOITS_ERR_CAPACITY
+    assert int(step.valid.item()) == 0
