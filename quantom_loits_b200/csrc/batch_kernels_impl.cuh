@@ -699,17 +699,26 @@ __device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool la
   __syncthreads();
 }
 
+// A CTA's bulk-copy barrier (shared memory) and the parity of its next phase
+// (shared, advanced by thread 0 after each use).
+struct BulkStage {
+  uint64_t* bar;
+  uint32_t* phase;
+};
+
 // The density's sampling view: small densities copy their records, packed
-// guide and (backward) weights into shared memory; large densities keep
-// records and weights in global memory and copy a coarse guide when
-// lguide_bits > 0 (the forward adds a window of records: sample_item).  Ends
-// with a barrier.  guide_key (shared) names the density whose coarse guide
-// guide_s holds, so a CTA's consecutive items on one large density copy it
-// once.
+// guide and (backward) weights into shared memory -- records and the full
+// packed guide by the copy engine (one bulk copy each, issued by the CTA's
+// last thread so that warp 0 may run a look-back meanwhile), the weights
+// and a coarser guide by the threads; large densities keep records and
+// weights in global memory and copy a coarse guide when lguide_bits > 0 (the
+// forward adds a window of records: sample_item).  Ends with a barrier.
+// guide_key (shared) names the density whose coarse guide guide_s holds, so
+// a CTA's consecutive items on one large density copy it once.
 __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int64_t k0, int64_t G,
                                                  bool large, float4* rec_s, uint32_t* guide_s,
                                                  float* invd_s, const SampleShared& sh,
-                                                 int& guide_key) {
+                                                 int& guide_key, BulkStage bulk) {
   const bool nonmono = (sh.flags & kNonMonotone) != 0;
   const int m_full = __ldg(&a.gbits[b]);
   const bool coarse = large && a.lguide_bits > 0;
@@ -729,15 +738,36 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
     v.guide = L;
     v.cguide = guide_s;
   } else {
-    for (int64_t i = threadIdx.x; i < G; i += blockDim.x) {
-      rec_s[i] = __ldcg(&a.rec[k0 + i]);
-      if (invd_s) invd_s[i] = __ldcg(&a.invd[k0 + i]);
+    const bool full_guide = !nonmono && m == m_full;
+    const uint4* gsrc = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.pkoff[b]));
+    const uint32_t rec_bytes = static_cast<uint32_t>(G) * 16u;
+    const uint32_t guide_bytes = full_guide ? (4u << m) : 0u;
+    if (bulk.bar && threadIdx.x == blockDim.x - 1) {
+      // records (16 G bytes) and the packed guide (4 M bytes, M >= 4) start on
+      // 16-byte boundaries in the workspace and in shared memory
+      bulk_arm(bulk.bar, rec_bytes + guide_bytes);
+      bulk_copy(rec_s, a.rec + k0, rec_bytes, bulk.bar);
+      if (full_guide) bulk_copy(guide_s, gsrc, guide_bytes, bulk.bar);
     }
-    if (!nonmono && m == m_full) {
-      const uint4* src = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.pkoff[b]));
-      uint4* dst = reinterpret_cast<uint4*>(guide_s);
-      for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&src[i]);
-    } else if (!nonmono) {
+    if (invd_s)
+      for (int64_t i = threadIdx.x; i < G; i += blockDim.x) invd_s[i] = __ldcg(&a.invd[k0 + i]);
+    if (!bulk.bar) {
+      for (int64_t i = threadIdx.x; i < G; i += blockDim.x) rec_s[i] = __ldcg(&a.rec[k0 + i]);
+      if (full_guide) {
+        uint4* dst = reinterpret_cast<uint4*>(guide_s);
+        for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&gsrc[i]);
+      }
+    } else if (!bulk_wait(bulk.bar, *bulk.phase, a.spin_limit)) {
+      // the copy did not complete within the wait limit: the launch reports
+      // it and the threads copy the same bytes themselves
+      raise_status(a.status, LOITS_ERR_TIMEOUT);
+      for (int64_t i = threadIdx.x; i < G; i += blockDim.x) rec_s[i] = __ldcg(&a.rec[k0 + i]);
+      if (full_guide) {
+        uint4* dst = reinterpret_cast<uint4*>(guide_s);
+        for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&gsrc[i]);
+      }
+    }
+    if (!full_guide && !nonmono) {
       // every 2^s-th count: the guide with 2^s-times wider buckets
       const int sft = m_full - m;
       const uint32_t* L = a.gl + __ldg(&a.goff[b]);
@@ -752,9 +782,12 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
     v.fresh = false;
   }
   __syncthreads();
-  // every thread has read guide_key above; the next read follows the item
-  // loop's barriers
-  if (threadIdx.x == 0) guide_key = large ? (nonmono || !coarse ? guide_key : b) : -1;
+  // every thread has read guide_key and the bulk phase above; the next reads
+  // follow the item loop's barriers
+  if (threadIdx.x == 0) {
+    guide_key = large ? (nonmono || !coarse ? guide_key : b) : -1;
+    if (!large && bulk.bar) *bulk.phase ^= 1u;
+  }
   v.shift = 32 - m;
   v.shift_full = 32 - m_full;
   v.wrec = nullptr;
@@ -775,9 +808,9 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
 __device__ __forceinline__ DensView load_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
                                                  bool large, float4* rec_s, uint32_t* guide_s,
                                                  float* invd_s, bool wait_ready, SampleShared& sh,
-                                                 int& guide_key) {
+                                                 int& guide_key, BulkStage bulk) {
   density_flags(a, b, large, wait_ready, sh);
-  return density_view(a, b, k0, G, large, rec_s, guide_s, invd_s, sh, guide_key);
+  return density_view(a, b, k0, G, large, rec_s, guide_s, invd_s, sh, guide_key, bulk);
 }
 
 // One slot: uniform from its Philox word, interval, value, acceptance.
@@ -1431,7 +1464,7 @@ __device__ __forceinline__ void forward_window(const BatchArgs& a, DensView& d, 
 template <int TPB, int R, bool kLarge>
 __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float4* rec_s,
                                             uint32_t* guide_s, float* stage, SampleShared& sh,
-                                            int& guide_key, int2& win) {
+                                            int& guide_key, int2& win, BulkStage bulk) {
   const TileGeom tg = tile_geom<TPB, R>(a, t);
   const bool large = kLarge && tg.G > a.gcap;
   density_flags(a, tg.b, large, true, sh);
@@ -1439,12 +1472,12 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
     float* hs = reinterpret_cast<float*>(rec_s) + a.hist_smem_off;
     if (large) {
       DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
-                                guide_key);
+                                guide_key, bulk);
       if (d.coarse) forward_window<TPB>(a, d, tg.k0, rec_s, win, sh);
       sample_tile_hist<TPB, R, kL2>(a, tg, d, hs);
     } else {
       const DensView d = density_view(a, tg.b, tg.k0, tg.G, false, rec_s, guide_s, nullptr, sh,
-                                     guide_key);
+                                     guide_key, bulk);
       sample_tile_hist<TPB, R, kShared>(a, tg, d, hs);
     }
     return;
@@ -1460,14 +1493,14 @@ __device__ __forceinline__ void sample_item(const BatchArgs& a, int32_t t, float
   // one view per branch: each sees constant `large` (shared or global loads)
   if (large) {
     DensView d = density_view(a, tg.b, tg.k0, tg.G, true, rec_s, guide_s, nullptr, sh,
-                              guide_key);
+                              guide_key, bulk);
     if (d.coarse) forward_window<TPB>(a, d, tg.k0, rec_s, win, sh);
     if (d.accept_all) sample_tile_all<TPB, R, kL2>(a, tg, d, sh.base);
     else if (d.threshold) sample_tile_threshold<TPB, R, kL2>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kL2>(a, t, tg, d, stage, sh);
   } else {
     const DensView d = density_view(a, tg.b, tg.k0, tg.G, false, rec_s, guide_s, nullptr, sh,
-                                   guide_key);
+                                   guide_key, bulk);
     if (d.accept_all) sample_tile_all<TPB, R, kShared>(a, tg, d, sh.base);
     else if (d.threshold) sample_tile_threshold<TPB, R, kShared>(a, t, tg, d, sh);
     else sample_tile_general<TPB, R, kShared>(a, t, tg, d, stage, sh);
@@ -1874,7 +1907,7 @@ __device__ __forceinline__ void vjp_state_chunk_fix(const BatchArgs& a, int64_t 
 template <int TPB, int R, bool kLarge, bool kFix>
 __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
                                                uint32_t* guide_s, float* invd_s, float* gacc_s,
-                                               SampleShared& sh, int& guide_key) {
+                                               SampleShared& sh, int& guide_key, BulkStage bulk) {
   const int b = find_owner(a.chunk_first, a.d_lo, a.d_hi, k);
   const int32_t ki = k - __ldg(&a.chunk_first[b]);
   const int32_t tb = __ldg(&a.tile_first[b]);
@@ -1899,7 +1932,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   Acc acc{};
   if (kLarge && tg.G > a.gcap) {
     const DensView d = load_density(a, b, tg.k0, tg.G, true, nullptr, guide_s, nullptr, false,
-                                    sh, guide_key);
+                                    sh, guide_key, bulk);
     acc.gc = a.gcdf + __ldg(&a.gc_off[b]);
     const bool win = kFixPaths<TPB> && a.win_n > 0 && d.coarse && !d.skip && G - 1 > a.win_n;
     if (win) {
@@ -1967,7 +2000,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
     float* invd_f = reinterpret_cast<float*>(rec_s + G);
     uint32_t* base = reinterpret_cast<uint32_t*>(invd_f + G);
     const DensView d = load_density(a, b, tg.k0, tg.G, false, rec_f, guide_s, invd_f, false, sh,
-                                    guide_key);
+                                    guide_key, bulk);
     if (d.count_all) {
       // count semantics: intervals and offsets are not bounded, fp32 sums
       float* gacc = reinterpret_cast<float*>(base);
@@ -2010,7 +2043,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
     }
   } else {
     const DensView d = load_density(a, b, tg.k0, tg.G, false, rec_s, guide_s, invd_s, false, sh,
-                                    guide_key);
+                                    guide_key, bulk);
     const int stride = rep > 1 ? G + 1 : G;  // rep * stride <= gcap
     for (int i = threadIdx.x; i < rep * stride; i += TPB) gacc_s[i] = 0.0f;
     __syncthreads();
@@ -2265,7 +2298,14 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
   __shared__ uint32_t s_item;
   __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
   __shared__ int2 s_win;       // ... and its window of records in rec_s
-  if (threadIdx.x == 0) s_guide_key = -1;
+  __shared__ __align__(8) uint64_t s_bar;  // bulk copies of density views
+  __shared__ uint32_t s_phase;
+  if (threadIdx.x == 0) {
+    s_guide_key = -1;
+    s_phase = 0;
+    bulk_barrier_init(&s_bar);
+  }
+  const BulkStage bulk{&s_bar, &s_phase};
   const int32_t nC = a.c_hi - a.c_lo, nF = a.f_hi - a.f_lo, nT = a.t_hi - a.t_lo;
   const uint32_t n_items = static_cast<uint32_t>(nC + nF + nT);
   while (true) {
@@ -2284,7 +2324,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
       else cdf_finalize_item<TPB, false>(a, fi, sh.cdf, stage_s);
     } else {
       sample_item<TPB, R, kLarge>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s,
-                                  guide_s, stage, sh.smp, s_guide_key, s_win);
+                                  guide_s, stage, sh.smp, s_guide_key, s_win, bulk);
     }
   }
 }
@@ -2302,10 +2342,15 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
   } sh;
   __shared__ uint32_t s_item;
   __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
+  __shared__ __align__(8) uint64_t s_bar;  // bulk copies of density views
+  __shared__ uint32_t s_phase;
   if (threadIdx.x == 0) {
     s_guide_key = -1;
     sh.smp.win_b = -1;  // no fixed-point window chosen yet
+    s_phase = 0;
+    bulk_barrier_init(&s_bar);
   }
+  const BulkStage bulk{&s_bar, &s_phase};
   const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo, nL = a.l_hi - a.l_lo;
   const uint32_t n_items = static_cast<uint32_t>(nK + nD + 2 * nL);
   while (true) {
@@ -2316,7 +2361,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nK)) {
       vjp_chunk_item<TPB, R, kLarge, kFix>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s,
-                                     invd_s, gacc_s, sh.smp, s_guide_key);
+                                     invd_s, gacc_s, sh.smp, s_guide_key, bulk);
     } else if (item < static_cast<uint32_t>(nK + nD)) {
       vjp_finalize_item<TPB>(a, a.d_lo + static_cast<int32_t>(item) - nK, grho, sh.fin);
     } else if constexpr (kLarge) {

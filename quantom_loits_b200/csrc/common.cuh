@@ -170,6 +170,56 @@ __device__ __forceinline__ bool wait_counter(const uint32_t* counter, uint32_t t
   return false;
 }
 
+// -------------------------------------------- bulk copies into shared memory
+//
+// A CTA stages a density's records and guide with the copy engine
+// (cp.async.bulk, global -> shared, this GPU's own memory, no multicast):
+// one thread arms an mbarrier with the byte count and issues the copies,
+// every thread waits for the barrier's phase.  Both addresses and the size
+// of each copy are multiples of 16 bytes.
+
+__device__ __forceinline__ uint32_t smem_addr(const void* p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// Once per CTA (one thread), before any bulk copy; a barrier must follow.
+__device__ __forceinline__ void bulk_barrier_init(uint64_t* bar) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_addr(bar)) : "memory");
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
+// One thread: earlier accesses to shared memory (ordered by a barrier)
+// before the copy engine's writes; arm the barrier for `bytes`.
+__device__ __forceinline__ void bulk_arm(uint64_t* bar, uint32_t bytes) {
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  asm volatile("{\n\t.reg .b64 st;\n\t"
+               "mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n\t}"
+               ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+
+// One thread: bytes (a multiple of 16) from global src to shared dst, both
+// 16-byte aligned, completing on bar.
+__device__ __forceinline__ void bulk_copy(void* dst, const void* src, uint32_t bytes,
+                                          uint64_t* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+      ::"r"(smem_addr(dst)), "l"(src), "r"(bytes), "r"(smem_addr(bar)) : "memory");
+}
+
+// Every thread: wait for phase `parity` of bar to complete, at most `limit`
+// polls; false when the wait ran out.
+__device__ __forceinline__ bool bulk_wait(uint64_t* bar, uint32_t parity, uint32_t limit) {
+  for (uint32_t it = 0; it < limit; ++it) {
+    uint32_t done;
+    asm volatile("{\n\t.reg .pred p;\n\t"
+                 "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+                 "selp.u32 %0, 1, 0, p;\n\t}"
+                 : "=r"(done) : "r"(smem_addr(bar)), "r"(parity) : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
 // ---------------------------------------------------------------- scans
 
 template <typename T>
