@@ -296,17 +296,21 @@ def tune(spec, dev, args, plain: bool):
         return dict(base, threads=threads, blocks_per_item=blocks, scan_knots=0), None
     tbatch = B.DensityBatch.from_spec(spec, dev)
     tuner = Autotuner(dev, candidates=PLAIN_CANDIDATES if plain else CANDIDATES, base=base,
-                      saved_state=True)
+                      saved_state=True, buckets=not args.no_bucket_tune)
     best, times = tuner.tune(tbatch, spec.event_counts, spec.seed, 0)
     return best, times
 
 
 def make_step(spec, dev, geom, rank, saved_state=False):
     from quantom_loits_b200 import batched as B
+    from quantom_loits_b200.tuning import density_tables, plain_config
 
     nmax = int(spec.event_counts.max())
-    cfg = B.make_config(**geom, density_base=rank * spec.n_densities, slot_stride=nmax)
-    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev)
+    cfg = B.make_config(**plain_config(geom), density_base=rank * spec.n_densities,
+                        slot_stride=nmax)
+    blocks, scan = density_tables(spec.knot_offsets, geom)
+    plan = B.BatchPlan(spec.knot_offsets, spec.event_counts, cfg, dev, density_blocks=blocks,
+                       density_scan=scan)
     step = B.BatchStep(plan, seed=spec.seed, with_cut=spec.x_cut is not None,
                        saved_state=saved_state)
     step.grid.copy_(torch_from(spec.grid))
@@ -479,6 +483,7 @@ def run_b200(args, spec, rank, world, dist) -> dict:
                          "larger than the 126 MB L2 (no flush)" if 4 * valid > 126e6 else
                          "inputs smaller than L2: not a valid roofline case",
                    "launch": plan.config, "accepted_events_per_step": valid * world,
+                   "bucket_tables": {k: geom.get(k) for k in ("bucket_blocks", "bucket_scan")},
                    "tuning_ms_per_step": tune_ms},
         "plain": {"value": events_step / (plain_ms * 1e-3), "ms_per_step": plain_ms,
                   "form": "one forward + one backward launch per density, saved state, "
@@ -590,7 +595,8 @@ def run_e2e(args, spec, dev, rank, world, dist) -> dict:
     from quantom_loits_b200.loits import LOITS
 
     nmax = int(spec.event_counts.max())
-    cfg = B.make_config(**args.geom, density_base=rank * spec.n_densities, slot_stride=nmax)
+    # the tuned geometry (with its per-bucket tables) as the sampler's config
+    cfg = dict(args.geom, density_base=rank * spec.n_densities, slot_stride=nmax)
     sampler = LOITS(backend="cuda", device=dev, batch_config=cfg)
     h_vals = torch_from(spec.values).pin_memory()
     h_grid = torch_from(spec.grid).pin_memory()
@@ -1037,6 +1043,8 @@ def main(argv=None) -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-tune", action="store_true",
                     help="use the plan's default launch geometry instead of tuning it")
+    ap.add_argument("--no-bucket-tune", action="store_true",
+                    help="tune one launch geometry for the whole batch, not per grid-size bucket")
     args = ap.parse_args(argv)
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")

@@ -215,6 +215,19 @@ int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_offsets,
                             loits_batch_plan** plan);
 void loits_batch_plan_destroy(loits_batch_plan* plan);
 
+/* loits_batch_plan_create with geometry per density (host arrays of B, or
+ * NULL for the config's value): blocks_per_density[b] in
+ * [1, cfg->blocks_per_item] sets density b's sampling tile to threads *
+ * blocks_per_density[b] Philox blocks, scan_knots_per_density[b] in [1, 64]
+ * its knots per thread in the CDF scan -- so that one launch serves small and
+ * large densities each at its own tuned tile length and scan width (the
+ * autotuner's per-bucket tables).  No counterpart in the reference (its
+ * launch geometry is fixed). */
+int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* knot_offsets,
+                               const int64_t* event_counts, const loits_batch_config* cfg,
+                               const int32_t* blocks_per_density,
+                               const int32_t* scan_knots_per_density, loits_batch_plan** plan);
+
 /* Sizes of the caller buffers of a plan. */
 int64_t loits_batch_capacity(const loits_batch_plan* plan);      /* sum n_b: events rows */
 int64_t loits_batch_total_knots(const loits_batch_plan* plan);   /* knot_offsets[B] */

@@ -77,6 +77,8 @@ SIGNATURES = {
                                                _vp, _vp, _vp, _vp, _sz, _vp]),
     "loits_batch_plan_create": (C.c_int, [_i64, _vp, _vp, C.POINTER(BatchConfig),
                                           C.POINTER(_vp)]),
+    "loits_batch_plan_create_ex": (C.c_int, [_i64, _vp, _vp, C.POINTER(BatchConfig), _vp, _vp,
+                                             C.POINTER(_vp)]),
     "loits_batch_plan_destroy": (None, [_vp]),
     "loits_batch_capacity": (_i64, [_vp]),
     "loits_batch_total_knots": (_i64, [_vp]),

@@ -95,10 +95,16 @@ def make_config(threads=0, blocks_per_item=0, scan_knots=0, ctas_per_sm=0, plain
 
 
 class BatchPlan:
-    """Native plan for one batch shape (offsets table + launch geometry)."""
+    """Native plan for one batch shape (offsets table + launch geometry).
+
+    ``density_blocks`` / ``density_scan`` (optional, one int per density):
+    each density's Philox blocks per thread per sampling tile (at most the
+    config's blocks_per_item) and knots per thread in its CDF scan, e.g.
+    from :meth:`tuning.Autotuner.density_tables`; the config's values
+    otherwise."""
 
     def __init__(self, knot_offsets, event_counts, config: N.BatchConfig | dict | None = None,
-                 device="cuda"):
+                 device="cuda", density_blocks=None, density_scan=None):
         self.device = torch.device(device)
         N.require_device(self.device)
         self.knot_offsets = _host_i64(knot_offsets)
@@ -106,13 +112,25 @@ class BatchPlan:
         self.n_densities = len(self.knot_offsets) - 1
         if isinstance(config, dict):
             config = make_config(**config)
+        tables = []
+        for t in (density_blocks, density_scan):
+            if t is None:
+                tables.append(None)
+                continue
+            t = np.ascontiguousarray(np.asarray(t, dtype=np.int32))
+            if t.shape != (self.n_densities,):
+                raise ValueError("per-density tables need one entry per density")
+            tables.append(t)
+        self._tables = tables  # kept alive for the call
         lib = N.lib()
         handle = C.c_void_p()
         with torch.cuda.device(self.device):
-            N.check(lib.loits_batch_plan_create(
+            N.check(lib.loits_batch_plan_create_ex(
                 self.n_densities, self.knot_offsets.ctypes.data, self.event_counts.ctypes.data,
-                C.byref(config) if config is not None else None, C.byref(handle)),
-                "loits_batch_plan_create")
+                C.byref(config) if config is not None else None,
+                None if tables[0] is None else tables[0].ctypes.data,
+                None if tables[1] is None else tables[1].ctypes.data, C.byref(handle)),
+                "loits_batch_plan_create_ex")
         self._lib = lib
         self.handle = handle
         self.capacity = int(lib.loits_batch_capacity(handle))
@@ -352,8 +370,10 @@ class BatchedLOITS:
     flow to ``batch.values``.  Plans are cached per batch shape.
 
     ``config``: None (the plan's defaults: CTA size by occupancy), a
-    ``loits_batch_config`` / dict, or ``"auto"``: the launch geometry is timed
-    on the first batch of each shape bucket (:mod:`quantom_loits_b200.tuning`).
+    ``loits_batch_config`` / dict (a tuned dict may carry per-bucket tables,
+    :func:`quantom_loits_b200.tuning.density_tables`), or ``"auto"``: the
+    launch geometry is timed on the first batch of each shape bucket
+    (:mod:`quantom_loits_b200.tuning`).
 
     ``saved_state`` (default True): keep each kept row's interval and offset
     between forward and backward (8 bytes per row, as the reference keeps its
@@ -387,9 +407,16 @@ class BatchedLOITS:
                 from .tuning import default_tuner
 
                 tuner = default_tuner(self.device, self.saved_state and hist is None)
-                config = make_config(**tuner.config_for(batch, event_counts, self.seed,
-                                                        self.sequence, hist))
-            plan = BatchPlan(knot_offsets, event_counts, config, self.device)
+                config = tuner.config_for(batch, event_counts, self.seed, self.sequence, hist)
+            blocks = scan = None
+            if isinstance(config, dict):
+                # a tuned geometry, possibly with per-bucket tables
+                from .tuning import density_tables, plain_config
+
+                blocks, scan = density_tables(knot_offsets, config)
+                config = make_config(**plain_config(config))
+            plan = BatchPlan(knot_offsets, event_counts, config, self.device,
+                             density_blocks=blocks, density_scan=scan)
             self._plans[key] = plan
         return plan
 

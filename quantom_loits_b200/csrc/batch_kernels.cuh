@@ -56,7 +56,8 @@ struct BatchArgs {
   int32_t d_lo, d_hi;          // densities (backward finalize items)
   int32_t l_lo, l_hi;          // reverse-scan tiles of large densities (each run twice)
   int32_t tiles_total;         // sampling tiles of the whole plan
-  int32_t scan_knots;          // knots per thread per CDF tile
+  const int32_t* tile_r;       // [B] Philox blocks per thread per sampling tile (<= R)
+  const int32_t* scan_k;       // [B] knots per thread per CDF tile
   int32_t gcap;                // knots a sampling CTA holds in shared memory
   int32_t mcap;                // guide entries (M + 1) a sampling CTA holds
   int32_t gbits_cap;           // most guide bits this launch copies to shared memory

@@ -385,7 +385,7 @@ __device__ __forceinline__ bool cdf_tile_fits(const BatchArgs& a, const int32_t*
                                               int tpb) {
   const int b = find_owner(first, a.d_lo, a.d_hi, it);
   const int64_t G = __ldg(&a.knot_off[b + 1]) - __ldg(&a.knot_off[b]);
-  const int64_t KT = static_cast<int64_t>(tpb) * a.scan_knots;
+  const int64_t KT = static_cast<int64_t>(tpb) * __ldg(&a.scan_k[b]);
   const int64_t n = (G < KT ? G : KT) + 2;
   return 8 * n <= 4ll * a.fwd_guide_off;
 }
@@ -445,7 +445,8 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   const int32_t ci = ct - first, nci = __ldg(&a.cdf_first[b + 1]) - first;
   const int64_t k0 = __ldg(&a.knot_off[b]);
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
-  const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
+  const int sk = __ldg(&a.scan_k[b]);  // knots per thread in this density's CDF tiles
+  const int64_t KT = static_cast<int64_t>(TPB) * sk;
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
   const Knots kn = tile_knots<kS>(a, k0, G, lo, hi, stage_s);
   if constexpr (kS) {
@@ -453,9 +454,9 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
                      const_cast<float*>(kn.f));
     __syncthreads();
   }
-  const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * a.scan_knots;
+  const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * sk;
   const int64_t my_lo = my_lo_raw < hi ? my_lo_raw : hi;
-  const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
+  const int64_t my_hi = my_lo_raw + sk < hi ? my_lo_raw + sk : hi;
   double tot, maxp;
   bool neg;
   bool bad_grid;
@@ -521,7 +522,8 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   const int32_t ct = first + ci;
   const int64_t k0 = __ldg(&a.knot_off[b]);
   const int64_t G = __ldg(&a.knot_off[b + 1]) - k0;
-  const int64_t KT = static_cast<int64_t>(TPB) * a.scan_knots;
+  const int sk = __ldg(&a.scan_k[b]);  // knots per thread in this density's CDF tiles
+  const int64_t KT = static_cast<int64_t>(TPB) * sk;
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
   const Knots kn = tile_knots<kS>(a, k0, G, lo, hi, stage_s);
   if constexpr (kS)  // made visible by the barrier after the lane-0 work below
@@ -566,9 +568,9 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   __syncthreads();
   const double norm = sh.norm, tile_excl = sh.tile_excl, mprev = sh.mprev, cnext = sh.cnext;
   const bool nonmono = sh.nonmono != 0, has_next = sh.has_next != 0;
-  const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * a.scan_knots;
+  const int64_t my_lo_raw = lo + static_cast<int64_t>(threadIdx.x) * sk;
   const int64_t my_lo = my_lo_raw < hi ? my_lo_raw : hi;
-  const int64_t my_hi = my_lo_raw + a.scan_knots < hi ? my_lo_raw + a.scan_knots : hi;
+  const int64_t my_hi = my_lo_raw + sk < hi ? my_lo_raw + sk : hi;
   double tot, maxp;
   bool neg, bad_grid;
   cdf_pass1<kS>(kn, my_lo, my_hi, tot, maxp, neg, bad_grid);
@@ -604,9 +606,10 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
 // --------------------------------------------------------- sampling phase
 
 // Geometry of sampling tile t of density b: Philox blocks
-// [blk0, blk0 + TPB*R) clipped to the density's slots [P0, P0 + n).
+// [blk0, blk0 + TPB*rb) clipped to the density's slots [P0, P0 + n).
 struct TileGeom {
   int b;
+  int rb;  // Philox blocks per thread per tile of this density (at most the launch's R)
   int64_t k0, G, n, P0, blk0;
 };
 
@@ -615,11 +618,12 @@ __device__ __forceinline__ TileGeom tile_geom(const BatchArgs& a, int32_t t) {
   TileGeom tg;
   tg.b = find_owner(a.tile_first, a.d_lo, a.d_hi, t);
   const int32_t si = t - __ldg(&a.tile_first[tg.b]);
+  tg.rb = min(max(__ldg(&a.tile_r[tg.b]), 1), R);
   tg.k0 = __ldg(&a.knot_off[tg.b]);
   tg.G = __ldg(&a.knot_off[tg.b + 1]) - tg.k0;
   tg.n = __ldg(&a.n_events[tg.b]);
   tg.P0 = (a.dbase + tg.b) * a.nmax;
-  tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(si) * TPB * R;
+  tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(si) * TPB * tg.rb;
   return tg;
 }
 
@@ -927,7 +931,7 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
 }
 
 // Warp-granular work layout of a sampling tile: warp w of the CTA owns
-// Philox blocks blk0 + (w*R + r)*32 + lane for rounds r = 0..R-1, i.e. the
+// Philox blocks blk0 + (w*rb + r)*32 + lane for rounds r = 0..rb-1, i.e. the
 // 128 consecutive slots of each round, rounds in order.  A warp therefore
 // ranks its kept events with one warp scan per round, and the kept events of
 // a tile are the concatenation of its warps' kept events in warp order.
@@ -990,8 +994,8 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   int64_t row = row0;
 #pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+  for (int r = 0; r < tg.rb; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * tg.rb + r) * 32 + lane;
     const uint32_t range = d.skip ? 0u : block_range_mask(tg, blk);
     int js[4] = {0, 0, 0, 0};
     float ts[4] = {0.f, 0.f, 0.f, 0.f};
@@ -1022,7 +1026,7 @@ __device__ __forceinline__ void write_intervals(const BatchArgs& a, const TileGe
 // First and one-past-last absolute slot of tile tg inside its density.
 template <int TPB, int R>
 __device__ __forceinline__ void tile_slot_range(const TileGeom& tg, int64_t& s_lo, int64_t& s_hi) {
-  const int64_t pb = tg.blk0 << 2, pe = (tg.blk0 + static_cast<int64_t>(TPB) * R) << 2;
+  const int64_t pb = tg.blk0 << 2, pe = (tg.blk0 + static_cast<int64_t>(TPB) * tg.rb) << 2;
   const int64_t dend = tg.P0 + tg.n;
   s_lo = pb > tg.P0 ? pb : tg.P0;
   s_hi = pe < dend ? pe : dend;
@@ -1032,7 +1036,7 @@ __device__ __forceinline__ void tile_slot_range(const TileGeom& tg, int64_t& s_l
 // density's first and last tiles): every block's range mask is then 0xf.
 template <int TPB, int R>
 __device__ __forceinline__ bool tile_full(const TileGeom& tg) {
-  const int64_t pb = tg.blk0 << 2, pe = (tg.blk0 + static_cast<int64_t>(TPB) * R) << 2;
+  const int64_t pb = tg.blk0 << 2, pe = (tg.blk0 + static_cast<int64_t>(TPB) * tg.rb) << 2;
   return pb >= tg.P0 && pe <= tg.P0 + tg.n;
 }
 
@@ -1119,15 +1123,14 @@ __device__ __forceinline__ uint32_t threshold_keep(uint4 w, int kstar) {
 }
 
 // Rounds of a warp whose first block is wblk0 that hold slots of tile tg's
-// density: all R for a full tile, else up to the density's last block (a
+// density: all rb for a full tile, else up to the density's last block (a
 // warp past it has none).
-template <int R>
 __device__ __forceinline__ int warp_rounds(const TileGeom& tg, int64_t wblk0, bool full) {
-  if (full) return R;
+  if (full) return tg.rb;
   if (tg.n <= 0) return 0;
   const int64_t last = (tg.P0 + tg.n - 1) >> 2;  // the density's last block
   const int64_t k = last - wblk0;
-  return k < 0 ? 0 : static_cast<int>(k / 32 + 1 < R ? k / 32 + 1 : R);
+  return k < 0 ? 0 : static_cast<int>(k / 32 + 1 < tg.rb ? k / 32 + 1 : tg.rb);
 }
 
 // Stores the kept slots of one Philox block at rows p, p + 1, ... in slot
@@ -1171,8 +1174,8 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
   const int kstar = d.kstar;
   const bool full = tile_full<TPB, R>(tg);
   const uint64_t sid = stream_of(a);
-  const int64_t wblk0 = tg.blk0 + static_cast<int64_t>(warp * R) * 32;
-  const int rounds = warp_rounds<R>(tg, wblk0, full);
+  const int64_t wblk0 = tg.blk0 + static_cast<int64_t>(warp * tg.rb) * 32;
+  const int rounds = warp_rounds(tg, wblk0, full);
   int cnt = 0;
 #pragma unroll 1
   for (int r = 0; r < rounds; ++r) {
@@ -1227,8 +1230,8 @@ __device__ __forceinline__ void sample_tile_all(const BatchArgs& a, const TileGe
   const int64_t shiftrow = base - s_lo;
   const bool full = tile_full<TPB, R>(tg);
   const uint64_t sid = stream_of(a);
-  const int64_t wblk0 = tg.blk0 + static_cast<int64_t>(warp * R) * 32;
-  const int rounds = warp_rounds<R>(tg, wblk0, full);
+  const int64_t wblk0 = tg.blk0 + static_cast<int64_t>(warp * tg.rb) * 32;
+  const int rounds = warp_rounds(tg, wblk0, full);
 #pragma unroll 1
   for (int r = 0; r < rounds; ++r) {
     const int64_t blk = wblk0 + r * 32 + lane;
@@ -1262,12 +1265,12 @@ __device__ __forceinline__ void sample_tile_general(const BatchArgs& a, int32_t 
                                                     float* stage, SampleShared& sh) {
   constexpr int W = TPB / 32;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  float* sw = stage + warp * (R * 128);
+  float* sw = stage + warp * (tg.rb * 128);
   int acc = 0;
   const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+  for (int r = 0; r < tg.rb; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * tg.rb + r) * 32 + lane;
     const uint32_t range = d.skip ? 0u : (full ? 0xfu : block_range_mask(tg, blk));
     float x0 = 0.f, x1 = 0.f, x2 = 0.f, x3 = 0.f;
     uint32_t keep = 0;
@@ -1365,8 +1368,8 @@ __device__ __forceinline__ void sample_tile_hist(const BatchArgs& a, const TileG
   const int kstar = d.kstar;
   int kept = 0;
 #pragma unroll 1
-  for (int r = 0; r < R; ++r) {
-    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+  for (int r = 0; r < tg.rb; ++r) {
+    const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * tg.rb + r) * 32 + lane;
     const uint32_t range = d.skip ? 0u : (full ? 0xfu : block_range_mask(tg, blk));
     if (!range) continue;
     const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
@@ -1666,11 +1669,11 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
     // histogram mode: every kept slot's cotangent comes from the histogram's
 #pragma unroll 1
     for (int32_t t = t_first; t < t_end; ++t) {
-      tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
+      tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * tg.rb;
       const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
-      for (int r = 0; r < R; ++r) {
-        const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+      for (int r = 0; r < tg.rb; ++r) {
+        const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * tg.rb + r) * 32 + lane;
         const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
         if (!range) continue;
         const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
@@ -1691,14 +1694,14 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
     // identity compaction: slot p of tile t is row p + (tile_prefix[t] - s_lo)
 #pragma unroll 1
     for (int32_t t = t_first; t < t_end; ++t) {
-      tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
+      tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * tg.rb;
       int64_t s_lo, s_hi;
       tile_slot_range<TPB, R>(tg, s_lo, s_hi);
       const int64_t shiftrow = __ldcg(&a.tile_prefix[t]) - s_lo;
       const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
-      for (int r = 0; r < R; ++r) {
-        const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+      for (int r = 0; r < tg.rb; ++r) {
+        const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * tg.rb + r) * 32 + lane;
         const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
         if (!range) continue;
         const uint4 w = philox4x32_10(static_cast<uint64_t>(blk), stream_of(a), a.rk);
@@ -1726,12 +1729,12 @@ __device__ __forceinline__ void vjp_chunk_tiles(const BatchArgs& a, const DensVi
   }
 #pragma unroll 1
   for (int32_t t = t_first; t < t_end; ++t) {
-    tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * R;
+    tg.blk0 = (tg.P0 >> 2) + static_cast<int64_t>(t - tb) * TPB * tg.rb;
     int64_t row = __ldcg(&a.tile_prefix[t]) + __ldcg(&a.warp_off[static_cast<int64_t>(t) * W + warp]);
     const bool full = tile_full<TPB, R>(tg);
 #pragma unroll 1
-    for (int r = 0; r < R; ++r) {
-      const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * R + r) * 32 + lane;
+    for (int r = 0; r < tg.rb; ++r) {
+      const int64_t blk = tg.blk0 + static_cast<int64_t>(warp * tg.rb + r) * 32 + lane;
       const uint32_t range = full ? 0xfu : block_range_mask(tg, blk);
       Slot e0, e1, e2, e3;
       uint32_t keep = 0;
@@ -1928,7 +1931,7 @@ __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, fl
   const int64_t r1 = gh ? 0 : __ldcg(&a.tile_prefix[t_end]);
   // an upper bound on the chunk's kept rows (histogram mode: its slots)
   const int64_t chunk_rows =
-      gh ? static_cast<int64_t>(t_end - t_first) * TPB * R * 4 : r1 - r0;
+      gh ? static_cast<int64_t>(t_end - t_first) * TPB * tg.rb * 4 : r1 - r0;
   Acc acc{};
   if (kLarge && tg.G > a.gcap) {
     const DensView d = load_density(a, b, tg.k0, tg.G, true, nullptr, guide_s, nullptr, false,

@@ -59,6 +59,7 @@ struct loits_batch_plan {
   bool has_large = false;  // densities above the shared-memory limit
   int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
+  std::vector<int32_t> tile_r, scan_k;  // per density: blocks per thread per tile, CDF width
   std::vector<int64_t> part_off, goff, pkoff, gc_off;
   std::vector<int32_t> lfin_first;
   void* dtab = nullptr;
@@ -66,7 +67,8 @@ struct loits_batch_plan {
                 *d_pkoff = nullptr, *d_gc_off = nullptr;
   const int32_t* d_lfin_first = nullptr;
   const int32_t *d_tile_first = nullptr, *d_cdf_first = nullptr, *d_fin_first = nullptr,
-                *d_chunk_first = nullptr, *d_rowfill_lo = nullptr, *d_gbits = nullptr;
+                *d_chunk_first = nullptr, *d_rowfill_lo = nullptr, *d_gbits = nullptr,
+                *d_tile_r = nullptr, *d_scan_k = nullptr;
   Layout lay{};
   size_t fwd_smem = 0, bwd_smem = 0;
   // dynamic shared memory already allowed for the kernels (histogram mode
@@ -418,7 +420,8 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.nd = static_cast<int32_t>(p->nd);
   a.last_nonempty = p->last_nonempty;
   a.tiles_total = p->n_tiles;
-  a.scan_knots = p->scan_knots;
+  a.tile_r = p->d_tile_r;
+  a.scan_k = p->d_scan_k;
   a.gcap = p->gcap;
   a.tiles_per_chunk = p->tiles_per_chunk;
   a.spin_limit = p->cfg.wait_limit > 0 ? static_cast<uint32_t>(p->cfg.wait_limit) : kSpinLimit;
@@ -463,6 +466,16 @@ bool aligned16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 
 extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_offsets,
                                        const int64_t* event_counts,
                                        const loits_batch_config* cfg, loits_batch_plan** out) {
+  return loits_batch_plan_create_ex(n_densities, knot_offsets, event_counts, cfg, nullptr,
+                                    nullptr, out);
+}
+
+extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* knot_offsets,
+                                          const int64_t* event_counts,
+                                          const loits_batch_config* cfg,
+                                          const int32_t* blocks_per_density,
+                                          const int32_t* scan_knots_per_density,
+                                          loits_batch_plan** out) {
   if (!out) return LOITS_ERR_INVALID;
   *out = nullptr;
   if (n_densities < 1 || n_densities > (1 << 24) || !knot_offsets || !event_counts)
@@ -518,9 +531,25 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   SmemGeometry sg;
   rc = smem_geometry(p->tpb, p->r, large_g, p->gcap, p->small_max_g, c.guide_ratio, sg);
   if (rc != LOITS_OK) { delete p; return rc; }
+  // ---- per-density tile length (at most the launch's blocks per item) and
+  // CDF scan width (1..64): the defaults, or the caller's tables
+  p->tile_r.assign(n_densities, p->r);
+  p->scan_k.assign(n_densities, p->scan_knots);
+  for (int64_t b = 0; b < n_densities; ++b) {
+    if (blocks_per_density) {
+      if (blocks_per_density[b] < 1 || blocks_per_density[b] > p->r) { delete p; return LOITS_ERR_INVALID; }
+      p->tile_r[b] = blocks_per_density[b];
+    }
+    if (scan_knots_per_density) {
+      if (scan_knots_per_density[b] < 1 || scan_knots_per_density[b] > 64) {
+        delete p;
+        return LOITS_ERR_INVALID;
+      }
+      p->scan_k[b] = scan_knots_per_density[b];
+    }
+  }
   // ---- work items
-  const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;
-  const int64_t kt = static_cast<int64_t>(p->tpb) * p->scan_knots;
+  const int64_t blocks_per_tile = static_cast<int64_t>(p->tpb) * p->r;  // the longest tile
   p->tile_first.resize(n_densities + 1);
   p->cdf_first.resize(n_densities + 1);
   p->fin_first.resize(n_densities + 1);
@@ -532,6 +561,7 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
     p->cdf_first[b] = static_cast<int32_t>(nc);
     p->fin_first[b] = static_cast<int32_t>(nf);
     const int64_t g = p->koff[b + 1] - p->koff[b];
+    const int64_t kt = static_cast<int64_t>(p->tpb) * p->scan_k[b];
     const int64_t tiles_c = (g + kt - 1) / kt;
     nc += tiles_c;
     if (tiles_c > 1) nf += tiles_c;
@@ -539,7 +569,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
     if (n > 0) {
       const int64_t P0 = (p->dbase + b) * p->nmax;
       const int64_t nblk = ((P0 + n - 1) >> 2) - (P0 >> 2) + 1;
-      nt += (nblk + blocks_per_tile - 1) / blocks_per_tile;
+      const int64_t bpt = static_cast<int64_t>(p->tpb) * p->tile_r[b];
+      nt += (nblk + bpt - 1) / bpt;
       p->rowfill_lo[b] = next_fill;
       next_fill = static_cast<int32_t>(b + 1);
     } else {
@@ -710,6 +741,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   const size_t o_pk = push(p->pkoff.data(), p->pkoff.size() * 8);
   const size_t o_gc = push(p->gc_off.data(), p->gc_off.size() * 8);
   const size_t o_lf = push(p->lfin_first.data(), p->lfin_first.size() * 4);
+  const size_t o_tr = push(p->tile_r.data(), p->tile_r.size() * 4);
+  const size_t o_sk = push(p->scan_k.data(), p->scan_k.size() * 4);
   if (cudaMalloc(&p->dtab, host.size()) != cudaSuccess) { delete p; return LOITS_ERR_CUDA; }
   if (cudaMemcpy(p->dtab, host.data(), host.size(), cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(p->dtab);
@@ -730,6 +763,8 @@ extern "C" int loits_batch_plan_create(int64_t n_densities, const int64_t* knot_
   p->d_pkoff = reinterpret_cast<const int64_t*>(d + o_pk);
   p->d_gc_off = reinterpret_cast<const int64_t*>(d + o_gc);
   p->d_lfin_first = reinterpret_cast<const int32_t*>(d + o_lf);
+  p->d_tile_r = reinterpret_cast<const int32_t*>(d + o_tr);
+  p->d_scan_k = reinterpret_cast<const int32_t*>(d + o_sk);
   *out = p;
   return LOITS_OK;
 }

@@ -414,7 +414,7 @@ def test_autotuner_picks_a_geometry_that_samples_identically(B, tmp_path):
     case = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
                 values=spec.values, x_cut=spec.x_cut, scalars=np.array([spec.seed, 0]))
     a = run_batch(B, case)
-    b = run_batch(B, case, B.make_config(**cfg))
+    b = run_batch(B, case, B.make_config(**tuning.plain_config(cfg)))
     assert np.array_equal(a["rows"], b["rows"]) and np.array_equal(a["events"], b["events"])
     # BatchedLOITS(config="auto") goes through the same tuner
     sampler = B.BatchedLOITS(DEV, seed=spec.seed, config="auto")
@@ -631,3 +631,50 @@ def test_fixed_point_backward_takes_outlier_cotangents_in_fp32(B, oracle_lib, th
         assert np.isfinite(out["grad_values"][o:e]).all(), b
         scale = np.abs(gref[o:e]).max()
         assert np.abs(out["grad_values"][o:e] - gref[o:e]).max() <= GRAD_TOL * scale, b
+
+
+def test_per_density_tile_lengths_and_scan_widths_change_no_result(B):
+    """A plan whose densities each have their own sampling tile length and
+    CDF scan width (loits_batch_plan_create_ex, the autotuner's per-bucket
+    tables) samples the same events and rows as the uniform geometry, and its
+    gradient agrees to fp32 accumulation order; out-of-range tables are
+    rejected on the host."""
+    from quantom_loits_b200 import _native as N
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.ragged(scale=0.02, n_densities=20)
+    case = dict(knot_offsets=spec.knot_offsets, event_counts=spec.event_counts, grid=spec.grid,
+                values=spec.values, x_cut=spec.x_cut, scalars=np.array([spec.seed, 3]))
+    cfg = B.make_config(threads=512, blocks_per_item=16, scan_knots=8)
+    kept = run_batch(B, case, cfg, with_intervals=False)["valid"]
+    case["cotangent"] = np.random.default_rng(2).standard_normal(kept).astype(np.float32)
+    ref = run_batch(B, case, cfg)
+    rng = np.random.default_rng(5)
+    blocks = rng.choice([1, 2, 4, 7, 16], size=spec.n_densities).astype(np.int32)
+    scan = rng.choice([1, 3, 8, 16, 64], size=spec.n_densities).astype(np.int32)
+    koff, counts = spec.knot_offsets, spec.event_counts
+    plan = B.BatchPlan(koff, counts, cfg, DEV, density_blocks=blocks, density_scan=scan)
+    grid = torch.from_numpy(spec.grid).to(DEV)
+    values = torch.from_numpy(spec.values).to(DEV)
+    x_cut = torch.from_numpy(spec.x_cut).to(DEV)
+    events, rows, ws = plan.new_events(), plan.new_row_offsets(), plan.new_workspace()
+    ints = torch.full((max(plan.capacity, 1),), -1, dtype=torch.int32, device=DEV)
+    plan.forward(grid, values, x_cut, spec.seed, 3, events, rows, ws, ints)
+    plan.check_status(ws)
+    n = int(rows[-1].item())
+    assert np.array_equal(rows.cpu().numpy(), ref["rows"])
+    assert np.array_equal(events[:n].cpu().numpy(), ref["events"])
+    assert np.array_equal(ints[:n].cpu().numpy(), ref["intervals"])
+    g = torch.zeros(max(plan.capacity, 4), dtype=torch.float32, device=DEV)
+    g[:n] = torch.from_numpy(case["cotangent"][:n]).to(DEV)
+    gv = torch.empty_like(values)
+    plan.backward(grid, values, x_cut, spec.seed, 3, g, gv, ws)
+    plan.check_status(ws)
+    scale = np.abs(ref["grad_values"]).max()
+    assert np.abs(gv.cpu().numpy() - ref["grad_values"]).max() <= GRAD_REPRO * scale
+    for bad in (dict(density_blocks=np.full(spec.n_densities, 17, np.int32)),
+                dict(density_blocks=np.zeros(spec.n_densities, np.int32)),
+                dict(density_scan=np.full(spec.n_densities, 65, np.int32))):
+        with pytest.raises(N.LoitsError) as err:
+            B.BatchPlan(koff, counts, cfg, DEV, **bad)
+        assert err.value.code == N.LOITS_ERR_INVALID
