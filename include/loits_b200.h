@@ -182,8 +182,9 @@ typedef struct loits_batch_plan loits_batch_plan; /* opaque, host object */
 typedef struct loits_batch_config {
   int32_t threads;         /* threads per CTA of the sampling kernels: 256, 512 or 1024;
                               0 = the size with the most resident threads per SM */
-  int32_t blocks_per_item; /* Philox blocks (4 slots each) per thread per tile: 2,4,8,16;
-                              default 16 (8 with 1024 threads) */
+  int32_t blocks_per_item; /* Philox blocks (4 slots each) per thread per tile, at
+                              most: 2,4,8,16; default 16 (8 with 1024 threads); a
+                              density's tiles are evened out below this length */
   int32_t scan_knots;      /* knots per thread in the CDF scan: 1..64, default 8 */
   int32_t ctas_per_sm;     /* persistent CTAs per SM (0 = as many as fit) */
   int32_t plain;           /* 1 = one launch per density (no persistent queue) */
@@ -217,8 +218,10 @@ void loits_batch_plan_destroy(loits_batch_plan* plan);
 
 /* loits_batch_plan_create with geometry per density (host arrays of B, or
  * NULL for the config's value): blocks_per_density[b] in
- * [1, cfg->blocks_per_item] sets density b's sampling tile to threads *
- * blocks_per_density[b] Philox blocks, scan_knots_per_density[b] in [1, 64]
+ * [1, cfg->blocks_per_item] caps density b's sampling tile at threads *
+ * blocks_per_density[b] Philox blocks (every plan then evens out a density's
+ * tiles: the same tile count, the fewest blocks per thread that cover the
+ * density), scan_knots_per_density[b] in [1, 64]
  * its knots per thread in the CDF scan -- so that one launch serves small and
  * large densities each at its own tuned tile length and scan width (the
  * autotuner's per-bucket tables).  No counterpart in the reference (its

@@ -569,6 +569,14 @@ extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* kn
     if (n > 0) {
       const int64_t P0 = (p->dbase + b) * p->nmax;
       const int64_t nblk = ((P0 + n - 1) >> 2) - (P0 >> 2) + 1;
+      // even out the density's tiles: keep the tile count its length cap
+      // gives, with the fewest blocks per thread that still cover it, so
+      // that a density smaller than one tile spreads over every warp of
+      // the CTA instead of the first few
+      const int64_t cap_bpt = static_cast<int64_t>(p->tpb) * p->tile_r[b];
+      const int64_t tiles_b = (nblk + cap_bpt - 1) / cap_bpt;
+      const int64_t per_tile = (nblk + tiles_b - 1) / tiles_b;
+      p->tile_r[b] = static_cast<int32_t>((per_tile + p->tpb - 1) / p->tpb);
       const int64_t bpt = static_cast<int64_t>(p->tpb) * p->tile_r[b];
       nt += (nblk + bpt - 1) / bpt;
       p->rowfill_lo[b] = next_fill;
