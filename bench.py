@@ -246,26 +246,38 @@ REFERENCE_INFEASIBLE = {
 }
 
 
-def run_reference(args, spec) -> dict:
-    if spec.name in REFERENCE_INFEASIBLE:
-        return {"impl": "reference", "unavailable": REFERENCE_INFEASIBLE[spec.name],
-                "metric": METRIC, "config": describe(spec)}
-    # calibrate on one density, then take a sample of ~args.ref_seconds per step
-    n1, t1 = reference_sample(spec, 1)
-    per_density = max(t1, 1e-6)
-    n_dens = int(max(1, min(spec.n_densities, args.ref_seconds / per_density)))
-    for _ in range(max(args.warmup, 0) if n_dens * per_density < 5 else 1):
+def reference_timing(spec, seconds: float, warmup: int, repeats: int):
+    """The one method both CPU legs use: calibrate on one density, take the
+    first n densities that make about `seconds` of reference work, run that
+    sample `warmup` times untimed and `repeats` times timed.  Returns
+    (events/s of the mean timed run, n densities, events per run, mean s)."""
+    _, t1 = reference_sample(spec, 1)
+    n_dens = int(max(1, min(spec.n_densities, seconds / max(t1, 1e-6))))
+    for _ in range(max(warmup, 0)):
         reference_sample(spec, n_dens)
     times, evs = [], 0
-    for _ in range(args.steps):
+    for _ in range(max(repeats, 1)):
         ev, dt = reference_sample(spec, n_dens)
         times.append(dt)
         evs = ev
     t = float(np.mean(times))
-    value = evs / t
-    sample = (f"first {n_dens} of {spec.n_densities} densities ({evs} events, "
-              f"{spec.knot_offsets[1] - spec.knot_offsets[0]} knots) per step, exact embedding "
-              f"into the reference tuple; forward + backward wall clock")
+    return evs / t, n_dens, evs, t
+
+
+def reference_sample_text(spec, n_dens: int, evs: int, warmup: int, repeats: int) -> str:
+    return (f"first {n_dens} of {spec.n_densities} densities ({evs} events) per run, exact "
+            f"embedding into the reference tuple, reference openmp core on {cpu_cores()} "
+            f"threads; forward + backward wall clock, mean of {repeats} runs after {warmup} "
+            f"untimed")
+
+
+def run_reference(args, spec) -> dict:
+    if spec.name in REFERENCE_INFEASIBLE:
+        return {"impl": "reference", "unavailable": REFERENCE_INFEASIBLE[spec.name],
+                "metric": METRIC, "config": describe(spec)}
+    warm = 1
+    value, n_dens, evs, t = reference_timing(spec, args.ref_seconds, warm, args.steps)
+    sample = reference_sample_text(spec, n_dens, evs, warm, args.steps)
     return {"metric": METRIC, "value": value, "unit": "events/s", "impl": "reference",
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
@@ -670,17 +682,16 @@ def tuple_cpu_baseline(args, spec) -> dict:
 
 
 def cpu_baseline_leg(args, spec) -> dict:
-    """The reference openmp core on a bounded sample, rank 0 / N=1 only."""
+    """The reference openmp core on a bounded sample, rank 0 / N=1 only: the
+    reference arm's own method (reference_timing), three timed runs."""
     if spec.name in REFERENCE_INFEASIBLE:
         return {"value": None, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
                 "sample": REFERENCE_INFEASIBLE[spec.name]}
     try:
-        n1, t1 = reference_sample(spec, 1)
-        n_dens = int(max(1, min(spec.n_densities, args.ref_seconds / max(t1, 1e-6))))
-        ev, dt = reference_sample(spec, n_dens)
-        return {"value": ev / dt, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
-                "sample": f"first {n_dens} of {spec.n_densities} densities ({ev} events), "
-                          "reference openmp core on the exact embedding, fwd + bwd wall clock"}
+        warm, reps = 1, 3
+        value, n_dens, evs, _ = reference_timing(spec, args.ref_seconds, warm, reps)
+        return {"value": value, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
+                "sample": reference_sample_text(spec, n_dens, evs, warm, reps)}
     except Exception as exc:
         return {"value": None, "unit": "events/s", "cores": cpu_cores(), "kind": "reference",
                 "sample": f"unavailable: {exc}"}

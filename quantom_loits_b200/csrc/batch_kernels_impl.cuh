@@ -118,6 +118,8 @@ struct CdfShared {
   double cfirst[TPB];
   double tile_excl, norm, mprev, cnext;
   int nonmono, has_next;
+  int tmax[32];      // kept threshold: per-warp last interval at or below the cut
+  uint32_t flags;    // the density's flags, shared by publish_density
 };
 
 // Double-float prefix step for knot t of density (g, f): adds the area of
@@ -418,18 +420,34 @@ __device__ __forceinline__ Knots tile_knots(const BatchArgs& a, int64_t k0, int6
 }
 
 __device__ __forceinline__ int density_threshold(const BatchArgs& a, int b, int64_t k0, int64_t G);
+template <int TPB>
+__device__ __forceinline__ int threshold_scan(const BatchArgs& a, int b, int64_t k0, int64_t G,
+                                              CdfShared<TPB>& sh);
 
-// The end of a density's CDF, by thread 0 holding the density's flags `fl`
-// (on every lane of warp 0 after the call): a kThreshold density's kept
-// threshold is found by warp 0 and stored, then the density is published
-// ready (its records, guide, flags and threshold all visible first).
+// Densities up to this many knots per CTA thread find their kept threshold
+// with every thread of the CTA (threshold_scan); larger ones by one warp's
+// search over the uniforms (density_threshold).
+constexpr int kThresholdScanPerThread = 32;
+
+// The end of a density's CDF, by every thread of the CTA, thread 0 holding
+// the density's flags `fl`: a kThreshold density's kept threshold is found
+// and stored, then the density is published ready (its records, guide,
+// flags and threshold all visible first).  Every record of the density was
+// written and made visible (barrier, fence) before the call.
+template <int TPB>
 __device__ __forceinline__ void publish_density(const BatchArgs& a, int b, int64_t k0, int64_t G,
-                                                uint32_t fl) {
-  if (threadIdx.x >= 32) return;
-  fl = __shfl_sync(0xffffffffu, fl, 0);
+                                                uint32_t fl, CdfShared<TPB>& sh) {
+  if (threadIdx.x == 0) sh.flags = fl;
+  __syncthreads();
+  fl = sh.flags;
   if (fl & kThreshold) {
-    const int ks = density_threshold(a, b, k0, G);
-    if (threadIdx.x == 0) a.kstar[b] = ks;
+    if (G <= static_cast<int64_t>(kThresholdScanPerThread) * TPB) {
+      const int ks = threshold_scan<TPB>(a, b, k0, G, sh);
+      if (threadIdx.x == 0) a.kstar[b] = ks;
+    } else if (threadIdx.x < 32) {
+      const int ks = density_threshold(a, b, k0, G);
+      if (threadIdx.x == 0) a.kstar[b] = ks;
+    }
   }
   if (threadIdx.x == 0) {
     __threadfence();
@@ -483,7 +501,7 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
       fl |= threshold_flag(a, b, k0, G, tile_tot, fl);
       a.dflags[b] = fl;
     }
-    publish_density(a, b, k0, G, fl);
+    publish_density<TPB>(a, b, k0, G, fl, sh);
     return;
   }
   (void)tile_max;
@@ -598,7 +616,7 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
       fl |= threshold_flag(a, b, k0, G, norm, fl);
       a.dflags[b] = fl;
     }
-    publish_density(a, b, k0, G, fl);
+    publish_density<TPB>(a, b, k0, G, fl, sh);
   }
   __syncthreads();
 }
@@ -1060,6 +1078,30 @@ __device__ __forceinline__ int64_t publish_tile(const BatchArgs& a, int32_t t, c
   return base;
 }
 
+// Slope of interval j in fp64 from its records r0 = rec[j], r1 = rec[j + 1]:
+// m_j = (g_{j+1} - g_j) / (c_{j+1} - c_j + 1e-5), c = key - d
+// (cpp/loits_core.cpp:193-196).
+__device__ __forceinline__ double exact_slope(float4 r0, float4 r1) {
+  const double c0 = __dsub_rn(static_cast<double>(r0.x), static_cast<double>(r0.y));
+  const double c1 = __dsub_rn(static_cast<double>(r1.x), static_cast<double>(r1.y));
+  return __ddiv_rn(__dsub_rn(static_cast<double>(r1.z), static_cast<double>(r0.z)),
+                   __dadd_rn(__dsub_rn(c1, c0), kEps));
+}
+
+// g_j + m_j (u - c_j) in fp64 at the uniform u = k 2^-24 of interval j.
+__device__ __forceinline__ double value_at(float4 r0, float4 r1, double m, int k) {
+  (void)r1;
+  const double c0 = __dsub_rn(static_cast<double>(r0.x), static_cast<double>(r0.y));
+  const double u = static_cast<double>(uniform_from_bits(static_cast<uint32_t>(k) << 8));
+  return __fma_rn(m, __dsub_rn(u, c0), static_cast<double>(r0.z));
+}
+
+// The first 24-bit uniform index k (u = k 2^-24) with u >= key, in [0, 2^24].
+__device__ __forceinline__ int first_index_at(float key) {
+  const float s = ceilf(key * 16777216.0f);  // exact: a power-of-two scale
+  return s <= 0.0f ? 0 : (s >= 16777216.0f ? (1 << 24) : static_cast<int>(s));
+}
+
 // The reference's inverse CDF at the uniform of `bits`, in fp64
 // (cpp/loits_core.cpp:193-196): the interval j by the sampler's exact search,
 // then g_j + m_j (u - c_j) with c_j = key_j - d_j and
@@ -1068,12 +1110,7 @@ template <int kMode>
 __device__ __forceinline__ double exact_value(const DensView& d, uint32_t bits) {
   const int j = sample_slot<kMode>(d, bits).j;
   const float4 r0 = rec_at<kMode>(d.rec, j), r1 = rec_at<kMode>(d.rec, j + 1);
-  const double c0 = __dsub_rn(static_cast<double>(r0.x), static_cast<double>(r0.y));
-  const double c1 = __dsub_rn(static_cast<double>(r1.x), static_cast<double>(r1.y));
-  const double m = __ddiv_rn(__dsub_rn(static_cast<double>(r1.z), static_cast<double>(r0.z)),
-                             __dadd_rn(__dsub_rn(c1, c0), kEps));
-  const double u = static_cast<double>(uniform_from_bits(bits));
-  return __fma_rn(m, __dsub_rn(u, c0), static_cast<double>(r0.z));
+  return value_at(r0, r1, exact_slope(r0, r1), bits >> 8);
 }
 
 // The threshold of a kThreshold density: the largest k in [-1, 2^24) whose
@@ -1113,6 +1150,50 @@ __device__ __forceinline__ int density_threshold(const BatchArgs& a, int b, int6
   d.coarse = false;
   d.cut = __ldg(&a.x_cut[b]);
   return kept_threshold<kL2>(d);
+}
+
+// kept_threshold of density b by every thread of the CTA, from its final
+// records in global memory.  With a non-decreasing CDF, the uniforms
+// k 2^-24 of interval t are those with key_t <= u < key_{t+1} (interval 0
+// also below key_1, interval G-2 up to the last uniform), so x(k) there is
+// value_at with interval t's records -- exact_value's arithmetic without its
+// search.  x is non-decreasing in k (kThreshold), so the threshold lies in
+// the last interval whose first uniform gives x <= cut, where thread 0
+// finishes with a binary search.  Returns the threshold on thread 0.
+template <int TPB>
+__device__ __forceinline__ int threshold_scan(const BatchArgs& a, int b, int64_t k0, int64_t G,
+                                              CdfShared<TPB>& sh) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const double cut = static_cast<double>(__ldg(&a.x_cut[b]));
+  const float4* rec = a.rec + k0;
+  const int n_int = static_cast<int>(G) - 1;
+  int best = -1;  // last interval (of this thread's) whose first uniform has x <= cut
+  for (int t = threadIdx.x; t < n_int; t += TPB) {
+    const float4 r0 = __ldcg(rec + t), r1 = __ldcg(rec + t + 1);
+    const int klo = t == 0 ? 0 : first_index_at(r0.x);
+    const int khi = t == n_int - 1 ? (1 << 24) - 1 : first_index_at(r1.x) - 1;
+    if (klo <= khi && !(value_at(r0, r1, exact_slope(r0, r1), klo) > cut)) best = t;
+  }
+  best = __reduce_max_sync(0xffffffffu, best);
+  if (lane == 0) sh.tmax[warp] = best;
+  __syncthreads();
+  int ks = -1;
+  if (threadIdx.x == 0) {
+    int t = -1;
+    for (int w = 0; w < TPB / 32; ++w) t = sh.tmax[w] > t ? sh.tmax[w] : t;
+    if (t >= 0) {
+      const float4 r0 = __ldcg(rec + t), r1 = __ldcg(rec + t + 1);
+      const double m = exact_slope(r0, r1);
+      int lo = t == 0 ? 0 : first_index_at(r0.x);  // x(lo) <= cut
+      int hi = t == n_int - 1 ? (1 << 24) : first_index_at(r1.x);  // the next interval's first
+      while (hi - lo > 1) {
+        const int mid = lo + ((hi - lo) >> 1);
+        if (value_at(r0, r1, m, mid) > cut) hi = mid; else lo = mid;
+      }
+      ks = lo;
+    }
+  }
+  return ks;
 }
 
 __device__ __forceinline__ uint32_t threshold_keep(uint4 w, int kstar) {
@@ -1163,8 +1244,10 @@ __device__ __forceinline__ void store_kept(const BatchArgs& a, int64_t p, uint32
 
 // Tile of a kThreshold density: each warp counts its kept slots from the
 // Philox words alone, the tile publishes its count and takes its first row
-// from the look-back, then every warp samples and stores its kept events
-// straight to their final rows (no staging).
+// from the look-back, then every warp samples again and stores its kept
+// events straight to their final rows (no staging).  Generating the words
+// twice measured faster than keeping them in an L2-resident run between
+// the passes.
 template <int TPB, int R, int kMode>
 __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_t t,
                                                       const TileGeom& tg, const DensView& d,
@@ -1201,7 +1284,14 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
     if (lane == 0) sh.base = base;
   }
   __syncthreads();
-  int64_t row = sh.base + warp_excl;
+  const int64_t row = sh.base + warp_excl;
+  // rows of this warp relative to its first (a tile holds < 2^31 rows)
+  float* const evb = a.events + row;
+  int32_t* const ivb = a.intervals ? a.intervals + row : nullptr;
+  float* const ovb = a.offsets ? a.offsets + row : nullptr;
+  int rrow = 0;
+  DensView dd = d;
+  dd.count_all = false;  // a kThreshold density's CDF is non-decreasing
 #pragma unroll 1
   for (int r = 0; r < rounds; ++r) {
     const int64_t blk = wblk0 + r * 32 + lane;
@@ -1210,10 +1300,29 @@ __device__ __forceinline__ void sample_tile_threshold(const BatchArgs& a, int32_
     const uint32_t keep = threshold_keep(w, kstar) & range;
     int total;
     const int excl = warp_exclusive_count(__popc(keep), total);
-    const Slot e0 = sample_slot<kMode>(d, w.x), e1 = sample_slot<kMode>(d, w.y);
-    const Slot e2 = sample_slot<kMode>(d, w.z), e3 = sample_slot<kMode>(d, w.w);
-    store_kept(a, row + excl, keep, e0, e1, e2, e3);
-    row += total;
+    const Slot e0 = sample_slot<kMode>(dd, w.x), e1 = sample_slot<kMode>(dd, w.y);
+    const Slot e2 = sample_slot<kMode>(dd, w.z), e3 = sample_slot<kMode>(dd, w.w);
+    if (keep) {
+      const int p = rrow + excl;
+      const int c1 = keep & 1u, c2 = c1 + ((keep >> 1) & 1u), c3 = c2 + ((keep >> 2) & 1u);
+      if (keep & 1u) __stcs(evb + p, e0.x);
+      if (keep & 2u) __stcs(evb + p + c1, e1.x);
+      if (keep & 4u) __stcs(evb + p + c2, e2.x);
+      if (keep & 8u) __stcs(evb + p + c3, e3.x);
+      if (ivb) {
+        if (keep & 1u) __stcs(ivb + p, e0.j);
+        if (keep & 2u) __stcs(ivb + p + c1, e1.j);
+        if (keep & 4u) __stcs(ivb + p + c2, e2.j);
+        if (keep & 8u) __stcs(ivb + p + c3, e3.j);
+      }
+      if (ovb) {
+        if (keep & 1u) __stcs(ovb + p, e0.t);
+        if (keep & 2u) __stcs(ovb + p + c1, e1.t);
+        if (keep & 4u) __stcs(ovb + p + c2, e2.t);
+        if (keep & 8u) __stcs(ovb + p + c3, e3.t);
+      }
+    }
+    rrow += total;
   }
 }
 
