@@ -256,12 +256,17 @@ __device__ __forceinline__ uint32_t threshold_flag(const BatchArgs& a, int b, in
 // that can still move the interval, span = min(hi, G - 1) - lo (a count past
 // G - 1 only moves past the last interval, which the interval clamp undoes).
 // Interval of u in the bucket: ja + #{t in [lo, lo + span) : key_t <= u}.
-// Clamps make every entry safe (ja + span <= G - 2) whatever L holds.
-__device__ __forceinline__ uint32_t pack_entry(uint32_t lo, uint32_t hi, int G) {
+// Clamps make every entry safe (ja + span <= G - 2) whatever L holds.  The
+// entry is 8 bytes: {ja | span << 16, key_{ja+1}} -- the key the first
+// compare needs rides with the entry, so a slot's search loads the entry and
+// then its record, two dependent shared-memory loads instead of three.
+// rec: the density's final records (global memory).
+__device__ __forceinline__ uint2 pack_entry(uint32_t lo, uint32_t hi, int G, const float4* rec) {
   const int l = static_cast<int>(lo), h = min(static_cast<int>(hi), G - 1);
   const int ja = max(min(l - 1, G - 2), 0);
   const int span = max(h - (ja + 1), 0);
-  return static_cast<uint32_t>(ja) | (static_cast<uint32_t>(span) << 16);
+  return make_uint2(static_cast<uint32_t>(ja) | (static_cast<uint32_t>(span) << 16),
+                    __float_as_uint(__ldcg(reinterpret_cast<const float*>(rec + ja + 1))));
 }
 
 // Pack small density b's guide for sampling from shared memory:
@@ -274,8 +279,9 @@ __device__ __forceinline__ void pack_guide(const BatchArgs& a, int b) {
   const int M = 1 << __ldg(&a.gbits[b]);
   const int G = static_cast<int>(__ldg(&a.knot_off[b + 1]) - __ldg(&a.knot_off[b]));
   const uint32_t* L = a.gl + __ldg(&a.goff[b]);
-  uint32_t* P = a.gpk + po;
-  for (int k = threadIdx.x; k < M; k += TPB) P[k] = pack_entry(__ldcg(&L[k]), __ldcg(&L[k + 1]), G);
+  uint2* P = reinterpret_cast<uint2*>(a.gpk + po);
+  const float4* rec = a.rec + __ldg(&a.knot_off[b]);
+  for (int k = threadIdx.x; k < M; k += TPB) P[k] = pack_entry(__ldcg(&L[k]), __ldcg(&L[k + 1]), G, rec);
   __threadfence();
 }
 
@@ -763,9 +769,9 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
     const bool full_guide = !nonmono && m == m_full;
     const uint4* gsrc = reinterpret_cast<const uint4*>(a.gpk + __ldg(&a.pkoff[b]));
     const uint32_t rec_bytes = static_cast<uint32_t>(G) * 16u;
-    const uint32_t guide_bytes = full_guide ? (4u << m) : 0u;
+    const uint32_t guide_bytes = full_guide ? (8u << m) : 0u;
     if (bulk.bar && threadIdx.x == blockDim.x - 1) {
-      // records (16 G bytes) and the packed guide (4 M bytes, M >= 4) start on
+      // records (16 G bytes) and the packed guide (8 M bytes, M >= 4) start on
       // 16-byte boundaries in the workspace and in shared memory
       bulk_arm(bulk.bar, rec_bytes + guide_bytes);
       bulk_copy(rec_s, a.rec + k0, rec_bytes, bulk.bar);
@@ -777,7 +783,7 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
       for (int64_t i = threadIdx.x; i < G; i += blockDim.x) rec_s[i] = __ldcg(&a.rec[k0 + i]);
       if (full_guide) {
         uint4* dst = reinterpret_cast<uint4*>(guide_s);
-        for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&gsrc[i]);
+        for (int i = threadIdx.x; i < (1 << m) / 2; i += blockDim.x) dst[i] = __ldcg(&gsrc[i]);
       }
     } else if (!bulk_wait(bulk.bar, *bulk.phase, a.spin_limit)) {
       // the copy did not complete within the wait limit: the launch reports
@@ -786,7 +792,7 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
       for (int64_t i = threadIdx.x; i < G; i += blockDim.x) rec_s[i] = __ldcg(&a.rec[k0 + i]);
       if (full_guide) {
         uint4* dst = reinterpret_cast<uint4*>(guide_s);
-        for (int i = threadIdx.x; i < (1 << m) / 4; i += blockDim.x) dst[i] = __ldcg(&gsrc[i]);
+        for (int i = threadIdx.x; i < (1 << m) / 2; i += blockDim.x) dst[i] = __ldcg(&gsrc[i]);
       }
     }
     if (!full_guide && !nonmono) {
@@ -795,7 +801,8 @@ __device__ __forceinline__ DensView density_view(const BatchArgs& a, int b, int6
       const uint32_t* L = a.gl + __ldg(&a.goff[b]);
       const int Gi = static_cast<int>(G);
       for (int k = threadIdx.x; k < (1 << m); k += blockDim.x)
-        guide_s[k] = pack_entry(__ldcg(&L[k << sft]), __ldcg(&L[(k + 1) << sft]), Gi);
+        reinterpret_cast<uint2*>(guide_s)[k] =
+            pack_entry(__ldcg(&L[k << sft]), __ldcg(&L[(k + 1) << sft]), Gi, a.rec + k0);
     }
     v.rec = rec_s;
     v.guide = guide_s;
@@ -871,16 +878,17 @@ __device__ __forceinline__ void pick_interval(const float4* rec, int G, float u,
 }
 
 // Interval of u from a small density's packed guide entry (pack_entry), the
-// records in shared memory: one key load and compare move u from the
-// bucket's first interval to the next (always in bounds: ja + 1 <= G - 1);
-// only a bucket with two or more movable knots -- rare with M >= 16 G
-// buckets -- finishes with a binary search.  The record itself is loaded
+// records in shared memory: one compare with the entry's key moves u from
+// the bucket's first interval to the next (always in bounds:
+// ja + 1 <= G - 1); only a bucket with two or more movable knots finishes
+// with a binary search over the records' keys.  The record itself is loaded
 // once, after the interval is known.
-__device__ __forceinline__ int pick_packed(const float4* rec, uint32_t pk, float u) {
+__device__ __forceinline__ int pick_packed(const float4* rec, uint2 pk2, float u) {
   const float* keys = reinterpret_cast<const float*>(rec);
+  const uint32_t pk = pk2.x;
   const int ja = static_cast<int>(pk & 0xffffu);
   const int span = static_cast<int>(pk >> 16);
-  const bool step = (span > 0) & (u >= keys[4 * (ja + 1)]);
+  const bool step = (span > 0) & (u >= __uint_as_float(pk2.y));
   int j = ja + (step ? 1 : 0);
   if (step & (span >= 2)) {
     // first key above u among knots [ja + 2, ja + 1 + span)
@@ -903,7 +911,7 @@ __device__ __forceinline__ Slot sample_slot(const DensView& d, uint32_t bits) {
     j = interval_count_all(d.rec, u, d.G);
     r = d.rec[j];
   } else if constexpr (kMode == kShared) {
-    j = pick_packed(d.rec, d.guide[bits >> d.shift], u);
+    j = pick_packed(d.rec, reinterpret_cast<const uint2*>(d.guide)[bits >> d.shift], u);
     r = d.rec[j];
   } else if constexpr (kMode == kL2) {
     // forward, large density: when the coarse bucket's knots all lie in the

@@ -235,9 +235,9 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
   // smaller guide only widens buckets: the search finishes them exactly).
   // The backward reads every 2^s-th count when its budget is smaller: the
   // same guide with 2^s-times wider buckets.
-  // forward and backward CTAs hold a small density's packed guide (4 bytes
-  // per bucket)
-  constexpr size_t kFwdEntry = sizeof(uint32_t), kBwdEntry = sizeof(uint32_t);
+  // forward and backward CTAs hold a small density's packed guide (8 bytes
+  // per bucket: the entry and the key its first compare needs)
+  constexpr size_t kFwdEntry = sizeof(uint2), kBwdEntry = sizeof(uint2);
   auto cap_for = [&](size_t knot_bytes, int from, size_t entry) {
     int mc = from;
     while (mc > 2 && knot_bytes + g.static_smem + (size_t(1) << mc) * entry > kSmemLimit) --mc;
@@ -245,9 +245,9 @@ int smem_geometry(int tpb, int r, int64_t large_g, int32_t gcap, int64_t max_g, 
   };
   g.m_cap = cap_for(fwd_knots, kMaxSmallGuideBits, kFwdEntry);
   g.m_cap_b = cap_for(bwd_knots, kMaxSmallGuideBits, kBwdEntry);
-  // guide bytes of `entries` buckets (4-byte units, rounded up to 32 bytes);
+  // guide bytes of `entries` buckets (8-byte entries, rounded up to 8 entries);
   // kept events are staged in global memory, not here
-  auto gbytes = [](int32_t entries) { return static_cast<size_t>((entries + 7) & ~7) * sizeof(uint32_t); };
+  auto gbytes = [](int32_t entries) { return static_cast<size_t>((entries + 7) & ~7) * sizeof(uint2); };
   auto fbytes = [&](int32_t entries) { return gbytes(entries); };
   // CTAs per SM that `bytes` of dynamic shared memory allow (at most the
   // register cap's 1280 / tpb)
@@ -592,10 +592,9 @@ extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* kn
   p->n_tiles = static_cast<int32_t>(nt);
   p->n_cdf = static_cast<int32_t>(nc);
   p->n_fin = static_cast<int32_t>(nf);
-  // guide tables, M + 1 uint16 counts and M packed uint32 pairs per density
-  // at the same entry offsets
-  // (small densities also keep the packed copy the sampling CTAs load); a
-  // large density's guide is capped by kMaxLargeGuideBits, not shared memory
+  // guide tables: M + 1 uint32 counts per density, and for small densities
+  // also M packed 8-byte entries (the copy the sampling CTAs load); a large
+  // density's guide is capped by kMaxLargeGuideBits, not shared memory
   p->gbits.resize(n_densities);
   p->goff.resize(n_densities);
   p->pkoff.resize(n_densities);
@@ -618,7 +617,7 @@ extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* kn
       nl += (g + lseg - 1) / lseg;
     } else {
       p->pkoff[b] = pko;
-      pko += ((int64_t(1) << m) + 7) & ~int64_t(7);
+      pko += 2 * (((int64_t(1) << m) + 7) & ~int64_t(7));
       p->gc_off[b] = -1;
       p->mcap = std::max<int32_t>(p->mcap, static_cast<int32_t>(int64_t(1) << m));
     }
