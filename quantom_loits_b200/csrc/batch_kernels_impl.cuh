@@ -719,8 +719,13 @@ __device__ __forceinline__ void density_flags(const BatchArgs& a, int b, bool la
   if (threadIdx.x == 0) {
     if (wait_ready && !wait_counter(&a.cdf_ready[b], 1u, a.status, a.spin_limit))
       raise_status(a.status, LOITS_ERR_TIMEOUT);
-    sh.flags = ld_acquire_u32(&a.dflags[b]);
-    sh.kstar = (sh.flags & kThreshold) ? __ldcg(&a.kstar[b]) : 0;
+    // plain loads, in flight together: the wait's acquire (or the kernel
+    // boundary, without a wait) already orders them after the density's
+    // flags and threshold were written
+    const uint32_t fl = __ldcg(&a.dflags[b]);
+    const int ks = __ldcg(&a.kstar[b]);
+    sh.flags = fl;
+    sh.kstar = (fl & kThreshold) ? ks : 0;
     sh.cut = a.x_cut ? __ldg(&a.x_cut[b]) : -__int_as_float(0x7f800000);
     if (large && (sh.flags & kNonMonotone)) raise_status(a.status, LOITS_ERR_UNSUPPORTED);
   }
@@ -1665,7 +1670,9 @@ struct Acc {
   int win_lo, win_n;
 };
 
-// Adds integer term v (|v| < 2^30) to the split sum (lo, hi) at index i.
+// Adds integer term v (|v| < 2^30) to the split sum (lo, hi) at index i: its
+// low s bits to lo, its (signed) high part to hi.  Skipping the zero high
+// parts measured slower: the lanes of a warp diverge on the sign.
 __device__ __forceinline__ void fix_add(const Acc& acc, uint32_t* lo, uint32_t* hi, int i, int v) {
   atomicAdd(&lo[i], static_cast<uint32_t>(v) & acc.lmask);  // no return value: reductions
   atomicAdd(&hi[i], static_cast<uint32_t>(v >> acc.lbits));
