@@ -678,3 +678,41 @@ def test_per_density_tile_lengths_and_scan_widths_change_no_result(B):
         with pytest.raises(N.LoitsError) as err:
             B.BatchPlan(koff, counts, cfg, DEV, **bad)
         assert err.value.code == N.LOITS_ERR_INVALID
+
+
+def test_kept_threshold_edges_match_oracle(B, oracle_lib):
+    """Threshold compaction (monotone densities, cut >= 0) at its edges: a cut
+    below every value (everything kept), above every value (nothing kept),
+    exactly at a knot, and inside a stretch of zero density (a flat CDF);
+    densities from 2 to 8000 knots.  Row offsets exact, events within
+    tolerance of the oracle."""
+    rng = np.random.default_rng(31)
+    sizes = [2, 3, 64, 500, 4096, 8000]
+    grids, vals, cuts = [], [], []
+    for i, g in enumerate(sizes):
+        x = np.linspace(0.05, 1.0, g, dtype=np.float32)
+        f = (1.0 + rng.uniform(0, 1, g)).astype(np.float32)
+        if g >= 64:
+            f[g // 3: g // 2] = 0.0  # a flat stretch of the CDF
+        grids.append(x)
+        vals.append(f)
+    koff = np.concatenate([[0], np.cumsum(sizes)])
+    grid, values = np.concatenate(grids), np.concatenate(vals)
+    counts = np.array([3000, 2000, 50_000, 20_000, 120_000, 70_000])
+    for mode in ("below", "above", "at_knot", "flat"):
+        for i, g in enumerate(sizes):
+            x = grids[i]
+            cuts.append({"below": 0.0, "above": 2.0, "at_knot": float(x[g // 4]),
+                         "flat": float(0.5 * (x[g // 3] + x[g // 2 - 1])) if g >= 64 else float(x[0])}[mode])
+        cut = np.array(cuts[-len(sizes):], np.float32)
+        case = dict(knot_offsets=koff, event_counts=counts, grid=grid, values=values, x_cut=cut,
+                    scalars=np.array([17, 4]))
+        out = run_batch(B, case)
+        ref = oracle_lib.d_forward(koff, np.concatenate([[0], np.cumsum(counts)]), grid, values,
+                                   cut, 17, 4)
+        assert np.array_equal(out["rows"], ref["row_offsets"]), mode
+        np.testing.assert_allclose(out["events"], ref["events"], rtol=EVENT_RTOL)
+        if mode == "above":
+            assert out["valid"] == 0
+        if mode == "below":
+            assert out["valid"] == counts.sum()

@@ -218,3 +218,34 @@ def test_tuple_step_reports_a_capacity_overrun(backend, golden):
         step.check_status()
     assert err.value.code == N.LOITS_ERR_CAPACITY
     assert int(step.valid.item()) == 0
+
+
+def test_sparse_cells_match_oracle(backend, oracle_lib):
+    """A tuple whose cells hold 0-3 events each, so that one 1024-slot
+    sampling tile spans hundreds of cells (the tile's cells are found by one
+    warp-wide search, each event's cell by a search among them) and the
+    backward's chunks start in far-apart cells; bit-exact with the oracle."""
+    rng = np.random.default_rng(23)
+    B, nx, ny, kx, kq = 1, 120, 150, 6, 5
+    x_bins = np.sort(rng.uniform(0.001, 0.999, (B, nx, kx)), axis=-1)
+    q_bins = np.sort(rng.uniform(0.001, 0.999, (B, ny, kq)), axis=-1)
+    xsec_x = rng.uniform(0.1, 2.0, (B, ny, nx, kx))
+    xsec_q = rng.uniform(0.1, 2.0, (B, nx, ny, kq))
+    # heavy-tailed weights: most cells get trunc(|w| n) = 0, a few get many
+    w = rng.pareto(1.2, (B, nx, ny))
+    w /= w.sum()
+    acc = np.ones((B, nx, ny), bool)
+    n_events, seed, seq = 30_000, 7, 2
+    t = [torch.from_numpy(a).to(DEV) for a in (x_bins, xsec_x, q_bins, xsec_q, w, acc)]
+    ev, st = backend.tuple_forward(*t, n_events, seed, seq)
+    ref = oracle_lib.r_forward(x_bins, xsec_x, q_bins, xsec_q, w, acc, n_events, seed, seq)
+    counts = np.trunc(np.abs(w.reshape(-1) * n_events))
+    assert (counts == 0).mean() > 0.5  # the shape this test is about
+    assert np.array_equal(st["packed"].cpu().numpy(), ref["packed"])
+    assert np.array_equal(ev.cpu().numpy(), ref["events"])
+    g = rng.standard_normal(ref["events"].shape)
+    gx, gq = backend.tuple_backward(torch.from_numpy(g).to(DEV), t[0], t[1], t[2], t[3], t[5], st,
+                                    seed, seq)
+    rgx, rgq = oracle_lib.r_backward(g, ref, x_bins, xsec_x, q_bins, xsec_q, acc, seed, seq)
+    np.testing.assert_allclose(gx.cpu().numpy(), rgx, rtol=1e-9, atol=1e-10)
+    np.testing.assert_allclose(gq.cpu().numpy(), rgq, rtol=1e-9, atol=1e-10)
