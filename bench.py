@@ -250,11 +250,21 @@ def reference_timing(spec, seconds: float, warmup: int, repeats: int):
     """The one method both CPU legs use: calibrate on one density, take the
     first n densities that make about `seconds` of reference work, run that
     sample `warmup` times untimed and `repeats` times timed.  Returns
-    (events/s of the mean timed run, n densities, events per run, mean s)."""
+    (events/s of the mean timed run, n densities, events per run, mean s).
+    The reference's search counts every knot, so a density's work is taken
+    as its events times its knots."""
     _, t1 = reference_sample(spec, 1)
-    n_dens = int(max(1, min(spec.n_densities, seconds / max(t1, 1e-6))))
-    for _ in range(max(warmup, 0)):
-        reference_sample(spec, n_dens)
+    knots = np.diff(np.asarray(spec.knot_offsets, np.int64)).astype(np.float64)
+    work = np.cumsum(np.asarray(spec.event_counts, np.float64) * knots)
+
+    def pick(target_work):
+        return int(max(1, min(spec.n_densities, np.searchsorted(work, target_work, "right"))))
+
+    n_dens = pick(seconds * work[0] / max(t1, 1e-6))
+    # the untimed runs also refine the sample toward `seconds`
+    for _ in range(max(warmup, 1)):
+        _, t = reference_sample(spec, n_dens)
+        n_dens = pick(work[n_dens - 1] * seconds / max(t, 1e-6))
     times, evs = [], 0
     for _ in range(max(repeats, 1)):
         ev, dt = reference_sample(spec, n_dens)
