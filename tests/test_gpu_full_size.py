@@ -96,3 +96,26 @@ def test_full_size_workload_matches_oracle_on_sampled_densities(name, oracle_lib
                                      slot_stride=nmax)
         scale = max(np.abs(gref).max(), 1e-30)
         assert np.abs(gvals[k0:k1] - gref).max() <= GRAD_TOL * scale, (name, b)
+
+
+def test_reference_tuple_at_benchmark_scale_matches_oracle(oracle_lib):
+    """The reference's 2-D tuple at its GPU-benchmark scale (grid 100: 99 x 99
+    cells, K = 10, 1e7 events): packed slots and events bit-exact with the
+    oracle's restatement of the reference core, gradients within the tuple
+    tolerance (rtol 1e-9)."""
+    from quantom_loits_b200 import backend
+    from quantom_loits_b200 import workloads
+
+    spec = workloads.theory_tuple(grid=100, knots=10, n_events=10_000_000)
+    t = [torch.from_numpy(np.ascontiguousarray(a)).to(DEV) for a in spec.arrays]
+    ev, st = backend.tuple_forward(*t, spec.n_events, spec.seed, spec.sequence)
+    ref = oracle_lib.r_forward(*spec.arrays, spec.n_events, spec.seed, spec.sequence)
+    assert np.array_equal(st["packed"].cpu().numpy(), ref["packed"])
+    assert np.array_equal(ev.cpu().numpy(), ref["events"])
+    g = np.random.default_rng(5).standard_normal(ref["events"].shape)
+    gx, gq = backend.tuple_backward(torch.from_numpy(g).to(DEV), t[0], t[1], t[2], t[3], t[5], st,
+                                    spec.seed, spec.sequence)
+    rgx, rgq = oracle_lib.r_backward(g, ref, spec.x_bins, spec.xsec_x, spec.q_bins, spec.xsec_q,
+                                     spec.acceptance, spec.seed, spec.sequence)
+    np.testing.assert_allclose(gx.cpu().numpy(), rgx, rtol=1e-9, atol=1e-10)
+    np.testing.assert_allclose(gq.cpu().numpy(), rgq, rtol=1e-9, atol=1e-10)
