@@ -967,14 +967,15 @@ def run_gan_b200(args, rank, world, dist) -> dict:
     ms = t0.elapsed_time(t1) / args.steps
     if dist is not None:
         ms = max_over_ranks(ms)
-    # the sampler alone on the same shapes: 2 histogram forwards + 1 VJP
-    values = tr.theory(tr.generator(tr.latent_noise())).detach().requires_grad_(True)
+    # the sampler alone on the same shapes: 2 histogram forwards + 1 VJP (with
+    # the theory evaluated inside it, as the step runs it)
+    params = tr.generator(tr.latent_noise()).detach().requires_grad_(True)
     w = torch.randn((tr.batch, tr.bins), device=dev)
 
     def sampler_only():
         with torch.no_grad():
-            tr.histogram(values)
-        (tr.histogram(values) * w).sum().backward()
+            tr.generate_from(params)
+        (tr.generate_from(params) * w).sum().backward()
 
     for _ in range(3):
         sampler_only()

@@ -326,6 +326,32 @@ int loits_batch_backward_hist(const loits_batch_plan* plan, const float* grid, c
                               float lo, float hi, const float* grad_hist, float* grad_values,
                               void* workspace, const uint64_t* sequence_dev, void* stream);
 
+/* loits_batch_forward_hist / loits_batch_backward_hist with the densities
+ * given by the power-law theory's parameters (loits_theory_powerlaw below)
+ * instead of tabulated values: the CDF tiles evaluate each knot's value from
+ * params (B x 6 fp32) and the knot position as they load the knots, so the
+ * densities are never written to or read from global memory, and the
+ * backward reduces the theory's VJP into grad_params (B x 6, every entry
+ * written) where it would write grad_values.  Results equal those of
+ * loits_theory_powerlaw followed by the tabulated-value calls (the same
+ * values, bit for bit; grad_params to fp32 summation order).  Every density
+ * must be one CDF tile staged in shared memory (at most the plan's
+ * shared-memory knot count, and threads * scan_knots); otherwise
+ * LOITS_ERR_UNSUPPORTED.  The grid is the plan's concatenated knots (each
+ * density's own).  Fuses the theory map of pytorch/theory.py:37-126 into the
+ * sampler for batched theories. */
+int loits_batch_forward_hist_powerlaw(const loits_batch_plan* plan, const float* grid,
+                                      const float* params, const float* x_cut, uint64_t seed,
+                                      uint64_t sequence, int32_t bins, float lo, float hi,
+                                      float* hist, int64_t* kept, void* workspace,
+                                      const uint64_t* sequence_dev, void* stream);
+int loits_batch_backward_hist_powerlaw(const loits_batch_plan* plan, const float* grid,
+                                       const float* params, const float* x_cut, uint64_t seed,
+                                       uint64_t sequence, int32_t bins, float lo, float hi,
+                                       const float* grad_hist, float* grad_params,
+                                       void* workspace, const uint64_t* sequence_dev,
+                                       void* stream);
+
 /* Two-component power-law theory of the batched GAN step (replaces, for
  * batched densities, the theory map of pytorch/theory.py:37-126): params is
  * B x 6 fp32 raw generator outputs p; with s(z) = 1 / (1 + e^-z),

@@ -96,6 +96,12 @@ SIGNATURES = {
                                            C.c_float, _vp, _vp, _vp, _vp, _vp]),
     "loits_batch_backward_hist": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _i32, C.c_float,
                                             C.c_float, _vp, _vp, _vp, _vp, _vp]),
+    "loits_batch_forward_hist_powerlaw": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _i32,
+                                                    C.c_float, C.c_float, _vp, _vp, _vp, _vp,
+                                                    _vp]),
+    "loits_batch_backward_hist_powerlaw": (C.c_int, [_vp, _vp, _vp, _vp, _u64, _u64, _i32,
+                                                     C.c_float, C.c_float, _vp, _vp, _vp, _vp,
+                                                     _vp]),
     "loits_theory_powerlaw": (C.c_int, [_i64, _i64, _vp, _vp, _vp, _vp]),
     "loits_theory_powerlaw_vjp": (C.c_int, [_i64, _i64, _vp, _vp, _vp, _vp, _vp]),
 }

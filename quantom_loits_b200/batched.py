@@ -231,6 +231,30 @@ class BatchPlan:
                 workspace.data_ptr(), seq_dev, N.stream_of(self.device)),
                 "loits_batch_backward_hist")
 
+    def forward_hist_powerlaw(self, grid, params, x_cut, seed, sequence, bins, lo, hi, hist,
+                              kept, workspace) -> None:
+        """forward_hist with the densities given by power-law theory
+        parameters (B x 6, the GAN theory), evaluated in the kernels' CDF
+        tile loads instead of read from a values tensor."""
+        seq, seq_dev = _sequence_args(sequence)
+        with torch.cuda.device(self.device):
+            N.check(self._lib.loits_batch_forward_hist_powerlaw(
+                self.handle, grid.data_ptr(), params.data_ptr(), N.ptr(x_cut), int(seed), seq,
+                int(bins), float(lo), float(hi), hist.data_ptr(), kept.data_ptr(),
+                workspace.data_ptr(), seq_dev, N.stream_of(self.device)),
+                "loits_batch_forward_hist_powerlaw")
+
+    def backward_hist_powerlaw(self, grid, params, x_cut, seed, sequence, bins, lo, hi,
+                               grad_hist, grad_params, workspace) -> None:
+        """VJP of forward_hist_powerlaw: grad_hist -> grad_params (B x 6)."""
+        seq, seq_dev = _sequence_args(sequence)
+        with torch.cuda.device(self.device):
+            N.check(self._lib.loits_batch_backward_hist_powerlaw(
+                self.handle, grid.data_ptr(), params.data_ptr(), N.ptr(x_cut), int(seed), seq,
+                int(bins), float(lo), float(hi), grad_hist.data_ptr(), grad_params.data_ptr(),
+                workspace.data_ptr(), seq_dev, N.stream_of(self.device)),
+                "loits_batch_backward_hist_powerlaw")
+
     def check_status(self, workspace) -> None:
         """Synchronising read of the device status word."""
         N.check(int(self.status_view(workspace).item()), "batched sampler (device)")
@@ -362,6 +386,37 @@ class _HistFunction(torch.autograd.Function):
         return grad_values, None, None, None, None, None, None, None, None
 
 
+class _PowerLawHistFunction(torch.autograd.Function):
+    """Theory parameters -> per-density histograms, the theory evaluated inside
+    the sampler (forward_hist_powerlaw) and its VJP reduced there too."""
+
+    @staticmethod
+    def forward(ctx, params, grid, x_cut, plan: BatchPlan, seed, sequence, bins, lo, hi):
+        hist = torch.empty((plan.n_densities, bins), dtype=torch.float32, device=params.device)
+        kept = torch.empty(plan.n_densities, dtype=torch.int64, device=params.device)
+        ws = plan.new_workspace()
+        plan.forward_hist_powerlaw(grid, params, x_cut, seed, sequence, bins, lo, hi, hist, kept,
+                                   ws)
+        ctx.plan, ctx.seed, ctx.sequence = plan, int(seed), sequence
+        ctx.bins, ctx.lo, ctx.hi, ctx.x_cut = int(bins), float(lo), float(hi), x_cut
+        ctx.save_for_backward(params, grid, ws)
+        ctx.mark_non_differentiable(kept)
+        return hist, kept
+
+    @staticmethod
+    def backward(ctx, grad_hist, grad_kept):
+        params, grid, ws = ctx.saved_tensors
+        grad_params = torch.empty_like(params)
+        if grad_hist is None:
+            grad_params.zero_()
+        else:
+            ctx.plan.backward_hist_powerlaw(grid, params, ctx.x_cut, ctx.seed, ctx.sequence,
+                                            ctx.bins, ctx.lo, ctx.hi,
+                                            grad_hist.to(torch.float32).contiguous(),
+                                            grad_params, ws)
+        return grad_params, None, None, None, None, None, None, None, None
+
+
 class BatchedLOITS:
     """Autograd-facing batched sampler: ``sample(batch) -> (events, row_offsets)``.
 
@@ -463,6 +518,28 @@ class BatchedLOITS:
         x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
         return _HistFunction.apply(batch.values.contiguous(), grid, x_cut, plan, self.seed,
                                    sequence, int(bins), float(lo), float(hi))
+
+    def histogram_powerlaw(self, params: torch.Tensor, batch: DensityBatch, bins: int = 64,
+                           lo: float = 0.0, hi: float = 1.0, sequence=None):
+        """``histogram`` of the densities the two-component power-law theory
+        gives for ``params`` (B x 6 raw parameters, see
+        ``gan.PowerLawTheory``) on ``batch.grid``, the theory evaluated inside
+        the sampler's kernels (its values never stored) and its VJP reduced
+        there: ``(hist, kept)``, hist differentiable w.r.t. ``params``.
+        ``batch.values`` is not read (only its shape)."""
+        counts = batch.event_counts
+        if sequence is None:
+            if self.sequence_dev is not None:
+                sequence = self.sequence_dev.clone()
+                self.sequence_dev.add_(1)
+            else:
+                sequence = self.sequence
+                self.sequence += 1
+        plan = self.plan_for(batch.knot_offsets, counts, batch, (bins, lo, hi))
+        grid = batch.grid.detach().contiguous()
+        x_cut = None if batch.x_cut is None else batch.x_cut.detach().contiguous()
+        return _PowerLawHistFunction.apply(params.to(torch.float32).contiguous(), grid, x_cut, plan,
+                                           self.seed, sequence, int(bins), float(lo), float(hi))
 
 
 class BatchStep:

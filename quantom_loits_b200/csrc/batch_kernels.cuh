@@ -81,6 +81,8 @@ struct BatchArgs {
   // inputs
   const float* grid;
   const float* values;
+  const float* theory;         // B x 6 power-law parameters: knot values are evaluated from
+                               // them (theory.cuh) instead of read from `values`, or null
   const float* x_cut;
   // state (workspace)
   float4* rec;
@@ -121,6 +123,7 @@ struct BatchArgs {
   // backward
   const float* grad;
   float* grad_values;
+  float* grad_theory;          // with `theory`: B x 6 parameter gradient instead of grad_values
   const int32_t* st_intervals; // saved state read instead of replaying the uniforms
   const float* st_offsets;
   // histogram mode (events are binned instead of written; see hist_bin)

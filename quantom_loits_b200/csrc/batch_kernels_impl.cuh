@@ -42,6 +42,7 @@
 
 #include "batch_kernels.cuh"
 #include "lookback.cuh"
+#include "theory.cuh"
 
 namespace loits_dev {
 
@@ -398,13 +399,26 @@ __device__ __forceinline__ bool cdf_tile_fits(const BatchArgs& a, const int32_t*
   return 8 * n <= 4ll * a.fwd_guide_off;
 }
 
-// Knots [s0, s1) of the density at k0 into shared memory (sg, sf): coalesced
-// loads, all in flight at once, instead of each thread's strided chain of
-// dependent loads.  The caller synchronises.
+// Knots [s0, s1) of density b (first knot k0) into shared memory (sg, sf):
+// coalesced loads, all in flight at once, instead of each thread's strided
+// chain of dependent loads.  With theory parameters the values are evaluated
+// here from the knot positions: the densities never round-trip global
+// memory.  The caller synchronises.
 template <int TPB>
-__device__ __forceinline__ void stage_knots(const BatchArgs& a, int64_t k0, int64_t s0,
+__device__ __forceinline__ void stage_knots(const BatchArgs& a, int b, int64_t k0, int64_t s0,
                                             int64_t s1, float* sg, float* sf) {
   const int64_t n = s1 - s0;
+  if (a.theory) {
+    const float* p = a.theory + static_cast<int64_t>(b) * 6;
+    const loits_theory::Comp c0 = loits_theory::component(p, 0);
+    const loits_theory::Comp c1 = loits_theory::component(p, 1);
+    for (int64_t i = threadIdx.x; i < n; i += TPB) {
+      const float x = __ldg(&a.grid[k0 + s0 + i]);
+      sg[i] = x;
+      sf[i] = loits_theory::value(c0, c1, x);
+    }
+    return;
+  }
 #pragma unroll 4
   for (int64_t i = threadIdx.x; i < n; i += TPB) {
     sg[i] = __ldg(&a.grid[k0 + s0 + i]);
@@ -474,7 +488,7 @@ __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, Cd
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
   const Knots kn = tile_knots<kS>(a, k0, G, lo, hi, stage_s);
   if constexpr (kS) {
-    stage_knots<TPB>(a, k0, kn.off, kn.off + (kn.f - kn.g), const_cast<float*>(kn.g),
+    stage_knots<TPB>(a, b, k0, kn.off, kn.off + (kn.f - kn.g), const_cast<float*>(kn.g),
                      const_cast<float*>(kn.f));
     __syncthreads();
   }
@@ -551,7 +565,7 @@ __device__ __forceinline__ void cdf_finalize_item(const BatchArgs& a, int32_t fi
   const int64_t lo = ci * KT, hi = lo + KT < G ? lo + KT : G;
   const Knots kn = tile_knots<kS>(a, k0, G, lo, hi, stage_s);
   if constexpr (kS)  // made visible by the barrier after the lane-0 work below
-    stage_knots<TPB>(a, k0, kn.off, kn.off + (kn.f - kn.g), const_cast<float*>(kn.g),
+    stage_knots<TPB>(a, b, k0, kn.off, kn.off + (kn.f - kn.g), const_cast<float*>(kn.g),
                      const_cast<float*>(kn.f));
   if (threadIdx.x < 32) {
     const int lane = threadIdx.x;
@@ -2194,10 +2208,12 @@ struct FinShared {
   double sfirst[TPB];
   double red[33];
   double carry;
+  float tred[TPB / 32][6];  // per-warp parameter gradients (theory)
 };
 
 // Reverse-mode chain of density b: grad_cdf (sum of chunk partials) ->
-// suffix scan -> grad_rho -> normaliser VJP -> grad_values.
+// suffix scan -> grad_rho -> normaliser VJP -> grad_values (with theory
+// parameters: -> their gradient, the theory's VJP, reduced here).
 template <int TPB>
 __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, double* grho, FinShared<TPB>& sh) {
   const int32_t nch = __ldg(&a.chunk_first[b + 1]) - __ldg(&a.chunk_first[b]);
@@ -2211,7 +2227,14 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
   }
   __syncthreads();
   const float* g = a.grid + k0;
-  const float* f = a.values + k0;
+  const float* f = a.values ? a.values + k0 : nullptr;
+  // with theory parameters: the density's components, to evaluate its values
+  // and to take its parameter gradient here
+  loits_theory::Comp th[2];
+  if (a.theory) {
+    th[0] = loits_theory::component(a.theory + static_cast<int64_t>(b) * 6, 0);
+    th[1] = loits_theory::component(a.theory + static_cast<int64_t>(b) * 6, 1);
+  }
   const double norm = __ldcg(&a.norm[b]);
   const float* part = a.partials + __ldg(&a.part_off[b]);
   constexpr int E = 4;
@@ -2261,7 +2284,8 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
       const double h_n = t + 1 < G ? 0.5 * (static_cast<double>(__ldg(&g[t + 1])) - static_cast<double>(__ldg(&g[t]))) : 0.0;
       const double gr = h_n * s_next + h_t * gc[e];
       grho[k0 + t] = gr;
-      gn_local += gr * static_cast<double>(__ldg(&f[t]));
+      const float ft = a.theory ? loits_theory::value(th[0], th[1], __ldg(&g[t])) : __ldg(&f[t]);
+      gn_local += gr * static_cast<double>(ft);
     }
     __syncthreads();
     if (threadIdx.x == 0) sh.carry = carry + seg_tot;
@@ -2272,11 +2296,31 @@ __device__ __forceinline__ void vjp_finalize_item(const BatchArgs& a, int b, dou
   const double inv_n = 1.0 / norm;
   const double gnorm = -gn_total * inv_n * inv_n;
   __threadfence_block();
+  float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};  // with theory: d loss / d parameters
   for (int64_t t = threadIdx.x; t < G; t += TPB) {
     const double h_t = t >= 1 ? 0.5 * (static_cast<double>(__ldg(&g[t])) - static_cast<double>(__ldg(&g[t - 1]))) : 0.0;
     const double h_n = t + 1 < G ? 0.5 * (static_cast<double>(__ldg(&g[t + 1])) - static_cast<double>(__ldg(&g[t]))) : 0.0;
     const double v = grho[k0 + t] * inv_n + (h_t + h_n) * gnorm;
-    a.grad_values[k0 + t] = __double2float_rn(v);
+    if (a.theory) loits_theory::add_grad(th, __ldg(&g[t]), __double2float_rn(v), acc);
+    else a.grad_values[k0 + t] = __double2float_rn(v);
+  }
+  if (a.theory) {
+    // the density's parameter gradient: warp trees, then the warps in order
+    // (deterministic)
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+      float v = acc[j];
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+      if (lane == 0) sh.tred[warp][j] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+      float v = 0.0f;
+      for (int w = 0; w < TPB / 32; ++w) v += sh.tred[w][threadIdx.x];
+      a.grad_theory[static_cast<int64_t>(b) * 6 + threadIdx.x] = v;
+    }
   }
   __syncthreads();
 }

@@ -971,12 +971,26 @@ extern "C" int loits_batch_backward_state(const loits_batch_plan* p, const float
   return launch_backward(p, a, workspace, p->bwd_smem, static_cast<cudaStream_t>(stream));
 }
 
-extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* grid,
-                                        const float* values, const float* x_cut, uint64_t seed,
-                                        uint64_t sequence, int32_t bins, float lo, float hi,
-                                        float* hist, int64_t* kept, void* workspace,
-                                        const uint64_t* sequence_dev, void* stream) {
-  if (!p || !grid || !values || !hist || !kept || !workspace) return LOITS_ERR_INVALID;
+namespace {
+
+// Whether the densities of plan p can take their values from theory
+// parameters: each CDF is one tile staged in shared memory (the tile load
+// evaluates the theory) and sampled from shared memory.
+bool theory_fits(const loits_batch_plan* p) {
+  for (int64_t b = 0; b < p->nd; ++b) {
+    const int64_t g = p->koff[b + 1] - p->koff[b];
+    const int64_t kt = static_cast<int64_t>(p->tpb) * p->scan_k[b];
+    if (g > p->gcap || g > kt || 8 * (g + 2) > 4 * static_cast<int64_t>(p->fwd_guide_off))
+      return false;
+  }
+  return true;
+}
+
+int forward_hist(const loits_batch_plan* p, const float* grid, const float* values,
+                 const float* theory, const float* x_cut, uint64_t seed, uint64_t sequence,
+                 int32_t bins, float lo, float hi, float* hist, int64_t* kept, void* workspace,
+                 const uint64_t* sequence_dev, void* stream) {
+  if (!p || !grid || !(values || theory) || !hist || !kept || !workspace) return LOITS_ERR_INVALID;
   if (!hist_range_ok(bins, lo, hi) || !aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
   cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -984,6 +998,7 @@ extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* 
       cudaMemsetAsync(kept, 0, static_cast<size_t>(p->nd) * sizeof(int64_t), st) != cudaSuccess)
     return LOITS_ERR_CUDA;
   BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.theory = theory;
   a.seq_dev = sequence_dev;
   a.hist = hist;
   a.kept = reinterpret_cast<unsigned long long*>(kept);
@@ -1005,25 +1020,75 @@ extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* 
   return launch_forward(p, a, workspace, smem, st);
 }
 
-extern "C" int loits_batch_backward_hist(const loits_batch_plan* p, const float* grid,
-                                         const float* values, const float* x_cut, uint64_t seed,
-                                         uint64_t sequence, int32_t bins, float lo, float hi,
-                                         const float* grad_hist, float* grad_values,
-                                         void* workspace, const uint64_t* sequence_dev,
-                                         void* stream) {
-  if (!p || !grid || !values || !grad_hist || !grad_values || !workspace) return LOITS_ERR_INVALID;
+int backward_hist(const loits_batch_plan* p, const float* grid, const float* values,
+                  const float* theory, const float* x_cut, uint64_t seed, uint64_t sequence,
+                  int32_t bins, float lo, float hi, const float* grad_hist, float* grad_values,
+                  float* grad_theory, void* workspace, const uint64_t* sequence_dev,
+                  void* stream) {
+  if (!p || !grid || !(values || theory) || !grad_hist || !(grad_values || grad_theory) ||
+      !workspace)
+    return LOITS_ERR_INVALID;
   if (!hist_range_ok(bins, lo, hi) || !aligned16(workspace)) return LOITS_ERR_INVALID;
   if (sequence > (UINT64_MAX - 1) / 2) return LOITS_ERR_INVALID;
   BatchArgs a = step_args(p, workspace, grid, values, x_cut, seed, sequence);
+  a.theory = theory;
   a.seq_dev = sequence_dev;
   a.grad_hist = grad_hist;
   a.grad_values = grad_values;
+  a.grad_theory = grad_theory;
   a.hist_bins = bins;
   a.hist_lo = lo;
   a.hist_inv_h = static_cast<float>(bins / (static_cast<double>(hi) - lo));
   a.hist_smem_off = static_cast<int32_t>(p->bwd_smem / sizeof(float));
   const size_t smem = p->bwd_smem + static_cast<size_t>(bins) * sizeof(float);
   return launch_backward(p, a, workspace, smem, static_cast<cudaStream_t>(stream));
+}
+
+}  // namespace
+
+extern "C" int loits_batch_forward_hist(const loits_batch_plan* p, const float* grid,
+                                        const float* values, const float* x_cut, uint64_t seed,
+                                        uint64_t sequence, int32_t bins, float lo, float hi,
+                                        float* hist, int64_t* kept, void* workspace,
+                                        const uint64_t* sequence_dev, void* stream) {
+  if (!values) return LOITS_ERR_INVALID;
+  return forward_hist(p, grid, values, nullptr, x_cut, seed, sequence, bins, lo, hi, hist, kept,
+                      workspace, sequence_dev, stream);
+}
+
+extern "C" int loits_batch_backward_hist(const loits_batch_plan* p, const float* grid,
+                                         const float* values, const float* x_cut, uint64_t seed,
+                                         uint64_t sequence, int32_t bins, float lo, float hi,
+                                         const float* grad_hist, float* grad_values,
+                                         void* workspace, const uint64_t* sequence_dev,
+                                         void* stream) {
+  if (!values || !grad_values) return LOITS_ERR_INVALID;
+  return backward_hist(p, grid, values, nullptr, x_cut, seed, sequence, bins, lo, hi, grad_hist,
+                       grad_values, nullptr, workspace, sequence_dev, stream);
+}
+
+extern "C" int loits_batch_forward_hist_powerlaw(const loits_batch_plan* p, const float* grid,
+                                                 const float* params, const float* x_cut,
+                                                 uint64_t seed, uint64_t sequence, int32_t bins,
+                                                 float lo, float hi, float* hist, int64_t* kept,
+                                                 void* workspace, const uint64_t* sequence_dev,
+                                                 void* stream) {
+  if (!p || !params) return LOITS_ERR_INVALID;
+  if (!theory_fits(p)) return LOITS_ERR_UNSUPPORTED;
+  return forward_hist(p, grid, nullptr, params, x_cut, seed, sequence, bins, lo, hi, hist, kept,
+                      workspace, sequence_dev, stream);
+}
+
+extern "C" int loits_batch_backward_hist_powerlaw(const loits_batch_plan* p, const float* grid,
+                                                  const float* params, const float* x_cut,
+                                                  uint64_t seed, uint64_t sequence, int32_t bins,
+                                                  float lo, float hi, const float* grad_hist,
+                                                  float* grad_params, void* workspace,
+                                                  const uint64_t* sequence_dev, void* stream) {
+  if (!p || !params || !grad_params) return LOITS_ERR_INVALID;
+  if (!theory_fits(p)) return LOITS_ERR_UNSUPPORTED;
+  return backward_hist(p, grid, nullptr, params, x_cut, seed, sequence, bins, lo, hi, grad_hist,
+                       nullptr, grad_params, workspace, sequence_dev, stream);
 }
 
 extern "C" int loits_batch_cdf(const loits_batch_plan* p, const void* workspace, double* cdf,

@@ -15,34 +15,12 @@
 #include <cuda_runtime.h>
 
 #include "loits_b200.h"
+#include "theory.cuh"
 
 namespace {
 
-struct Comp {
-  float a, b, w;        // exponents and weight
-  float da, db, dw;     // d a / d p, d b / d p, d w / d p
-};
-
-__device__ __forceinline__ float sigmoid(float z) { return 1.0f / (1.0f + expf(-z)); }
-
-__device__ __forceinline__ Comp component(const float* p, int i) {
-  Comp c;
-  const float sa = sigmoid(p[2 * i]), sb = sigmoid(p[2 * i + 1]), sw = sigmoid(p[4 + i]);
-  c.a = -0.5f + 1.5f * sa;
-  c.b = 1.0f + 4.0f * sb;
-  // softplus, written to stay finite for large arguments
-  const float z = p[4 + i];
-  c.w = z > 20.0f ? z : log1pf(expf(z));
-  c.da = 1.5f * sa * (1.0f - sa);
-  c.db = 4.0f * sb * (1.0f - sb);
-  c.dw = sw;
-  return c;
-}
-
-// x^a (1-x)^b with 0 at x = 1 (b >= 1) and its logs' factors.
-__device__ __forceinline__ float term(float lx, float l1x, float a, float b) {
-  return expf(a * lx + b * l1x);
-}
+using loits_theory::Comp;
+using loits_theory::component;
 
 __global__ void theory_eval_kernel(int64_t nd, int64_t G, const float* __restrict__ params,
                                    const float* __restrict__ grid, float* __restrict__ values) {
@@ -53,8 +31,7 @@ __global__ void theory_eval_kernel(int64_t nd, int64_t G, const float* __restric
     const float x = __ldg(&grid[i - d * G]);
     const float* p = params + d * 6;
     const Comp c0 = component(p, 0), c1 = component(p, 1);
-    const float lx = logf(x), l1x = logf(1.0f - x);  // -inf at x = 1: the term is 0
-    values[i] = c0.w * term(lx, l1x, c0.a, c0.b) + c1.w * term(lx, l1x, c1.a, c1.b);
+    values[i] = loits_theory::value(c0, c1, x);
   }
 }
 
@@ -68,22 +45,8 @@ __global__ void __launch_bounds__(kVjpThreads) theory_vjp_kernel(
   const Comp c[2] = {component(p, 0), component(p, 1)};
   const float* gv = grad_values + d * G;
   float acc[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
-  for (int64_t t = threadIdx.x; t < G; t += kVjpThreads) {
-    const float x = __ldg(&grid[t]);
-    const float g = __ldg(&gv[t]);
-    const float lx = logf(x);
-    const float one_m = 1.0f - x;
-    const float l1x = logf(one_m);
-#pragma unroll
-    for (int i = 0; i < 2; ++i) {
-      const float tv = term(lx, l1x, c[i].a, c[i].b);
-      const float gwt = g * c[i].w * tv;
-      acc[2 * i] += gwt * lx * c[i].da;
-      // (1-x)^b ln(1-x) -> 0 as x -> 1 (b >= 1)
-      acc[2 * i + 1] += one_m > 0.0f ? gwt * l1x * c[i].db : 0.0f;
-      acc[4 + i] += g * tv * c[i].dw;
-    }
-  }
+  for (int64_t t = threadIdx.x; t < G; t += kVjpThreads)
+    loits_theory::add_grad(c, __ldg(&grid[t]), __ldg(&gv[t]), acc);
   // fixed-order reduction: warp tree, then warp 0 over the warps
   __shared__ float red[kVjpThreads / 32][6];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;

@@ -103,12 +103,17 @@ class BatchedGANTrainer:
 
     def __init__(self, device="cuda", batch: int = 256, n_events: int = 200_000,
                  grid_size: int = 2048, bins: int = 64, latent: int = 64, lr: float = 1e-4,
-                 seed: int = 0, config="auto", profile_regions: bool = False):
+                 seed: int = 0, config="auto", profile_regions: bool = False,
+                 fused_theory: bool = True):
         self.device = torch.device(device)
         N.require_device(self.device)
         torch.manual_seed(int(seed))
         self.batch, self.n_events, self.bins, self.latent = batch, int(n_events), bins, latent
         self.profile_regions = profile_regions
+        # the theory evaluated inside the sampler's CDF tiles and its VJP
+        # reduced there (BatchedLOITS.histogram_powerlaw), or as its own
+        # kernels (PowerLawTheory, then BatchedLOITS.histogram)
+        self.fused_theory = bool(fused_theory)
         grid1 = torch.linspace(1e-3, 1.0, grid_size, dtype=torch.float64).to(torch.float32)
         self.theory = PowerLawTheory(grid1).to(self.device)
         self.generator = Generator(latent).to(self.device)
@@ -120,6 +125,8 @@ class BatchedGANTrainer:
         self.grid = self.theory.grid.repeat(batch)
         self.knot_offsets = np.arange(batch + 1, dtype=np.int64) * grid_size
         self.event_counts = np.full(batch, self.n_events, dtype=np.int64)
+        self._shape_values = torch.zeros(batch * grid_size, dtype=torch.float32,
+                                         device=self.device)  # shape only: never read
         self.loss = nn.BCEWithLogitsLoss()
         # one fused multi-tensor kernel per optimizer step instead of one per
         # tensor; step counts on the device so that the step can be captured
@@ -147,8 +154,21 @@ class BatchedGANTrainer:
     def latent_noise(self) -> torch.Tensor:
         return torch.randn((self.batch, self.latent), generator=self.gen, device=self.device)
 
+    def histogram_of_params(self, params: torch.Tensor) -> torch.Tensor:
+        """histogram(theory(params)) with the theory fused into the sampler."""
+        batch = DensityBatch(self.grid, self._shape_values, self.knot_offsets, self.event_counts)
+        hist, _ = self.sampler.histogram_powerlaw(params, batch, self.bins, self.lo, self.hi)
+        return hist * (1.0 / self.n_events)
+
+    def generate_from(self, params: torch.Tensor) -> torch.Tensor:
+        """Normalised histograms of the densities the theory gives for
+        params (B x 6)."""
+        if self.fused_theory:
+            return self.histogram_of_params(params)
+        return self.histogram(self.theory(params))
+
     def generate(self, z: torch.Tensor) -> torch.Tensor:
-        return self.histogram(self.theory(self.generator(z)))
+        return self.generate_from(self.generator(z))
 
     def _step_body(self, z_d: torch.Tensor, z_g: torch.Tensor):
         with self._region("gan::discriminator_step"):

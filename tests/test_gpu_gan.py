@@ -154,6 +154,63 @@ def test_histogram_autograd_path():
     assert torch.isfinite(batch.values.grad).all() and batch.values.grad.abs().max() > 0
 
 
+@pytest.mark.parametrize("knots,threads", [(512, 256), (2048, 1024)])
+def test_powerlaw_theory_fused_into_the_sampler(knots, threads):
+    """histogram_powerlaw (the theory evaluated in the sampler's CDF tile
+    loads, its VJP reduced in the backward's finalize) against the theory's
+    own kernels followed by the tabulated-value histogram: the same values
+    bit for bit, hence the same kept counts and events; histograms and the
+    parameter gradient to fp32 summation order."""
+    from quantom_loits_b200 import batched as B
+    from quantom_loits_b200.gan import PowerLawTheory
+
+    nd = 12
+    grid1 = torch.linspace(1e-3, 1.0, knots, dtype=torch.float64).to(torch.float32)
+    th = PowerLawTheory(grid1).to(DEV)
+    gen = torch.Generator().manual_seed(7)
+    params = (torch.randn((nd, 6), generator=gen) * 0.8).to(DEV)
+    koff = np.arange(nd + 1, dtype=np.int64) * knots
+    counts = np.full(nd, 30_000, dtype=np.int64)
+    grid = th.grid.repeat(nd)
+    cfg = B.make_config(threads=threads, blocks_per_item=4)
+    sampler = B.BatchedLOITS(DEV, seed=5, config=cfg)
+    cot = torch.randn((nd, 32), generator=gen).to(DEV)
+
+    p_a = params.clone().requires_grad_(True)
+    batch = B.DensityBatch(grid, th(p_a).reshape(-1), koff, counts)
+    h_a, k_a = sampler.histogram(batch, 32, 1e-3, 1.0, sequence=9)
+    (g_a,) = torch.autograd.grad((h_a * cot).sum(), p_a)
+
+    p_b = params.clone().requires_grad_(True)
+    shape = B.DensityBatch(grid, torch.zeros(nd * knots, device=DEV), koff, counts)
+    h_b, k_b = sampler.histogram_powerlaw(p_b, shape, 32, 1e-3, 1.0, sequence=9)
+    (g_b,) = torch.autograd.grad((h_b * cot).sum(), p_b)
+
+    assert torch.equal(k_a, k_b)
+    # the same events; the per-tile merges into the global histogram are fp32
+    # additions in arrival order, so the bins agree to fp32 accumulation order
+    torch.testing.assert_close(h_b.detach(), h_a.detach(), rtol=1e-5, atol=1e-3)
+    scale = g_a.abs().max().item()
+    assert scale > 0 and (g_a - g_b).abs().max().item() <= 1e-4 * scale
+
+
+def test_powerlaw_theory_fused_rejects_densities_it_cannot_stage():
+    from quantom_loits_b200 import _native as N
+    from quantom_loits_b200 import batched as B
+
+    knots = 70_001  # above the shared-memory knot count: sampled from global memory
+    koff = np.array([0, knots], dtype=np.int64)
+    plan = B.BatchPlan(koff, np.array([1000]), B.make_config(threads=1024), DEV)
+    grid = torch.linspace(1e-3, 1.0, knots, device=DEV)
+    params = torch.zeros((1, 6), device=DEV)
+    hist = torch.empty((1, 8), device=DEV)
+    kept = torch.empty(1, dtype=torch.int64, device=DEV)
+    ws = plan.new_workspace()
+    with pytest.raises(N.LoitsError) as e:
+        plan.forward_hist_powerlaw(grid, params, None, 1, 0, 8, 0.0, 1.0, hist, kept, ws)
+    assert e.value.code == N.LOITS_ERR_UNSUPPORTED
+
+
 def test_gan_trainer_steps():
     from quantom_loits_b200.gan import BatchedGANTrainer
 

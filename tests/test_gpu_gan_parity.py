@@ -130,6 +130,13 @@ def test_gan_step_matches_fp64_oracle(oracle_lib):
     (gp,) = torch.autograd.grad(bce(logits, torch.ones_like(logits)), p_gpu)
     scale = gp_ref.abs().max().item()
     assert (gp.double().cpu() - gp_ref).abs().max().item() <= 1e-3 * scale
+    # ... and with the theory evaluated inside the sampler (the step's own path)
+    p_f = params_g.detach().clone().requires_grad_(True)
+    h_f, _ = tr.sampler.histogram_powerlaw(p_f, batch_g, bins, lo, hi, sequence=seq0 + 1)
+    torch.testing.assert_close(h_f.detach(), h_g.detach(), rtol=1e-5, atol=1e-3)
+    logits_f = tr.discriminator(h_f * (1.0 / N_EV))
+    (gpf,) = torch.autograd.grad(bce(logits_f, torch.ones_like(logits_f)), p_f)
+    assert (gpf.double().cpu() - gp_ref).abs().max().item() <= 1e-3 * scale
 
     # generator weights: the bf16 generator's backward from either gradient
     z = z_g.clone()
