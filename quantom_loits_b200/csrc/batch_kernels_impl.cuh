@@ -1998,32 +1998,40 @@ __device__ __forceinline__ void vjp_state_chunk_fix(const BatchArgs& a, int64_t 
   acc.lmask = (1u << acc.lbits) - 1u;
   const float4* rec = a.rec + k0;
   const int jmax = G - 2;
-  constexpr int U = 4;  // rows per thread in flight
+  // one row's fixed-point terms (or, above the chunk's cap, fp32 reductions)
+  auto add_row = [&](int j, float t, float g) {
+    j = min(max(j, 0), jmax);
+    const float w = t * invd_s[j];
+    if (!fix_pair(acc, j, g, w)) {
+      const float mg = __ldg(&rec[j].w) * g;
+      atomicAdd(&part[j], mg * (w - 1.0f));  // no return value: reductions
+      atomicAdd(&part[j + 1], -(mg * w));
+    }
+  };
+  // rows up to the first multiple of 4 and past the last one singly; the
+  // rest as 16-byte vectors of 4 rows per array (the three arrays start on
+  // 16-byte boundaries when their base pointers do)
+  const bool vec = ((reinterpret_cast<uintptr_t>(a.st_intervals) |
+                     reinterpret_cast<uintptr_t>(a.st_offsets) |
+                     reinterpret_cast<uintptr_t>(a.grad)) & 15) == 0;
+  const int64_t q0 = vec ? (r0 + 3) >> 2 : r1, q1 = vec ? r1 >> 2 : r1;  // quads [q0, q1)
+  const int64_t body0 = q0 < q1 ? 4 * q0 : r1, body1 = q0 < q1 ? 4 * q1 : r1;
+  for (int64_t r = r0 + threadIdx.x; r < body0; r += TPB)
+    add_row(__ldcs(&a.st_intervals[r]), __ldcs(&a.st_offsets[r]), __ldcs(&a.grad[r]));
+  for (int64_t r = body1 + threadIdx.x; r < r1; r += TPB)
+    add_row(__ldcs(&a.st_intervals[r]), __ldcs(&a.st_offsets[r]), __ldcs(&a.grad[r]));
+  const int4* iv4 = reinterpret_cast<const int4*>(a.st_intervals);
+  const float4* of4 = reinterpret_cast<const float4*>(a.st_offsets);
+  const float4* gr4 = reinterpret_cast<const float4*>(a.grad);
 #pragma unroll 1
-  for (int64_t r_base = r0; r_base < r1; r_base += static_cast<int64_t>(TPB) * U) {
-    int j[U];
-    float t[U], g[U];
-#pragma unroll
-    for (int i = 0; i < U; ++i) {
-      const int64_t r = r_base + i * TPB + threadIdx.x;
-      j[i] = -1;
-      t[i] = g[i] = 0.0f;
-      if (r < r1) {
-        j[i] = min(max(__ldcs(&a.st_intervals[r]), 0), jmax);
-        t[i] = __ldcs(&a.st_offsets[r]);
-        g[i] = __ldcs(&a.grad[r]);
-      }
-    }
-#pragma unroll
-    for (int i = 0; i < U; ++i) {
-      if (j[i] < 0) continue;
-      const float w = t[i] * invd_s[j[i]];
-      if (!fix_pair(acc, j[i], g[i], w)) {
-        const float mg = __ldg(&rec[j[i]].w) * g[i];
-        atomicAdd(&part[j[i]], mg * (w - 1.0f));  // no return value: reductions
-        atomicAdd(&part[j[i] + 1], -(mg * w));
-      }
-    }
+  for (int64_t q = q0 + threadIdx.x; q < q1; q += TPB) {
+    const int4 j4 = __ldcs(&iv4[q]);
+    const float4 t4 = __ldcs(&of4[q]);
+    const float4 g4 = __ldcs(&gr4[q]);
+    add_row(j4.x, t4.x, g4.x);
+    add_row(j4.y, t4.y, g4.y);
+    add_row(j4.z, t4.z, g4.z);
+    add_row(j4.w, t4.w, g4.w);
   }
   __threadfence();
   __syncthreads();
