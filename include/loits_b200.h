@@ -282,7 +282,9 @@ int loits_batch_forward_state(const loits_batch_plan* plan, const float* grid,
  * fp32 accumulation order), reading each kept row's interval, offset and
  * cotangent instead of regenerating its uniform and searching its interval.
  * intervals / offsets: as written by loits_batch_forward_state with this
- * workspace (intervals are clamped to the density's range). */
+ * workspace (intervals are clamped to the density's range).  The rows are
+ * read four at a time when grad_events, like the state, starts on a 16-byte
+ * boundary; otherwise one at a time (same result). */
 int loits_batch_backward_state(const loits_batch_plan* plan, const float* grid,
                                const float* values, const float* x_cut, const int32_t* intervals,
                                const float* offsets, const float* grad_events, float* grad_values,
