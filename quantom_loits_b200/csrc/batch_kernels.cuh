@@ -36,6 +36,9 @@ struct BatchArgs {
   const int64_t* knot_off;     // [B+1]
   const int64_t* n_events;     // [B]
   const int32_t* tile_first;   // [B+1] sampling tiles
+  const int32_t* tile_owner;   // [tiles] density of each sampling tile
+  const int32_t* cdf_owner;    // [CDF scan tiles] density of each
+  const int32_t* chunk_owner;  // [backward chunks] density of each
   const int32_t* cdf_first;    // [B+1] CDF scan tiles
   const int32_t* fin_first;    // [B+1] CDF finalize items (multi-tile densities only)
   const int32_t* chunk_first;  // [B+1] backward chunks

@@ -387,12 +387,10 @@ __device__ __forceinline__ double cdf_lookback(const BatchArgs& a, int32_t first
   return chained_lookback(a.cflag, a.cagg, a.cinc, a.status, first, ct, agg, a.spin_limit);
 }
 
-// Whether CDF item `it` (owner table first[]: scan or finalize items) can
-// stage its knots, 2 floats per knot of [lo - 1, hi + 1), in the dynamic
-// shared memory before the guide.
-__device__ __forceinline__ bool cdf_tile_fits(const BatchArgs& a, const int32_t* first, int32_t it,
-                                              int tpb) {
-  const int b = find_owner(first, a.d_lo, a.d_hi, it);
+// Whether a CDF item (scan or finalize) of density b can stage its knots,
+// 2 floats per knot of [lo - 1, hi + 1), in the dynamic shared memory before
+// the guide.
+__device__ __forceinline__ bool cdf_tile_fits(const BatchArgs& a, int b, int tpb) {
   const int64_t G = __ldg(&a.knot_off[b + 1]) - __ldg(&a.knot_off[b]);
   const int64_t KT = static_cast<int64_t>(tpb) * __ldg(&a.scan_k[b]);
   const int64_t n = (G < KT ? G : KT) + 2;
@@ -478,7 +476,7 @@ __device__ __forceinline__ void publish_density(const BatchArgs& a, int b, int64
 template <int TPB, bool kS>
 __device__ __forceinline__ void cdf_scan_item(const BatchArgs& a, int32_t ct, CdfShared<TPB>& sh,
                                               float* stage_s) {
-  const int b = find_owner(a.cdf_first, a.d_lo, a.d_hi, ct);
+  const int b = __ldg(&a.cdf_owner[ct]);
   const int32_t first = __ldg(&a.cdf_first[b]);
   const int32_t ci = ct - first, nci = __ldg(&a.cdf_first[b + 1]) - first;
   const int64_t k0 = __ldg(&a.knot_off[b]);
@@ -654,7 +652,7 @@ struct TileGeom {
 template <int TPB, int R>
 __device__ __forceinline__ TileGeom tile_geom(const BatchArgs& a, int32_t t) {
   TileGeom tg;
-  tg.b = find_owner(a.tile_first, a.d_lo, a.d_hi, t);
+  tg.b = __ldg(&a.tile_owner[t]);
   const int32_t si = t - __ldg(&a.tile_first[tg.b]);
   tg.rb = min(max(__ldg(&a.tile_r[tg.b]), 1), R);
   tg.k0 = __ldg(&a.knot_off[tg.b]);
@@ -2057,7 +2055,7 @@ template <int TPB, int R, bool kLarge, bool kFix>
 __device__ __forceinline__ void vjp_chunk_item(const BatchArgs& a, int32_t k, float4* rec_s,
                                                uint32_t* guide_s, float* invd_s, float* gacc_s,
                                                SampleShared& sh, int& guide_key, BulkStage bulk) {
-  const int b = find_owner(a.chunk_first, a.d_lo, a.d_hi, k);
+  const int b = __ldg(&a.chunk_owner[k]);
   const int32_t ki = k - __ldg(&a.chunk_first[b]);
   const int32_t tb = __ldg(&a.tile_first[b]);
   const int32_t t_first = tb + ki * a.tiles_per_chunk;
@@ -2495,11 +2493,12 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_forward_kernel(BatchArg
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nC)) {
       const int32_t ct = a.c_lo + static_cast<int32_t>(item);
-      if (cdf_tile_fits(a, a.cdf_first, ct, TPB)) cdf_scan_item<TPB, true>(a, ct, sh.cdf, stage_s);
+      if (cdf_tile_fits(a, __ldg(&a.cdf_owner[ct]), TPB)) cdf_scan_item<TPB, true>(a, ct, sh.cdf, stage_s);
       else cdf_scan_item<TPB, false>(a, ct, sh.cdf, stage_s);
     } else if (item < static_cast<uint32_t>(nC + nF)) {
       const int32_t fi = a.f_lo + static_cast<int32_t>(item) - nC;
-      if (cdf_tile_fits(a, a.fin_first, fi, TPB)) cdf_finalize_item<TPB, true>(a, fi, sh.cdf, stage_s);
+      if (cdf_tile_fits(a, find_owner(a.fin_first, a.d_lo, a.d_hi, fi), TPB))
+        cdf_finalize_item<TPB, true>(a, fi, sh.cdf, stage_s);
       else cdf_finalize_item<TPB, false>(a, fi, sh.cdf, stage_s);
     } else {
       sample_item<TPB, R, kLarge>(a, a.t_lo + static_cast<int32_t>(item) - nC - nF, rec_s,

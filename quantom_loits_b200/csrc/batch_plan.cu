@@ -60,6 +60,7 @@ struct loits_batch_plan {
   int64_t total_partials = 0, total_guide = 0, total_pk = 0, total_gc = 0;
   std::vector<int32_t> tile_first, cdf_first, fin_first, chunk_first, rowfill_lo, gbits;
   std::vector<int32_t> tile_r, scan_k;  // per density: blocks per thread per tile, CDF width
+  std::vector<int32_t> tile_owner, cdf_owner, chunk_owner;  // density of each item
   std::vector<int64_t> part_off, goff, pkoff, gc_off;
   std::vector<int32_t> lfin_first;
   void* dtab = nullptr;
@@ -68,7 +69,8 @@ struct loits_batch_plan {
   const int32_t* d_lfin_first = nullptr;
   const int32_t *d_tile_first = nullptr, *d_cdf_first = nullptr, *d_fin_first = nullptr,
                 *d_chunk_first = nullptr, *d_rowfill_lo = nullptr, *d_gbits = nullptr,
-                *d_tile_r = nullptr, *d_scan_k = nullptr;
+                *d_tile_r = nullptr, *d_scan_k = nullptr, *d_tile_owner = nullptr,
+                *d_cdf_owner = nullptr, *d_chunk_owner = nullptr;
   Layout lay{};
   size_t fwd_smem = 0, bwd_smem = 0;
   // dynamic shared memory already allowed for the kernels (histogram mode
@@ -402,6 +404,9 @@ BatchArgs base_args(const loits_batch_plan* p, void* ws) {
   a.knot_off = p->d_koff;
   a.n_events = p->d_nev;
   a.tile_first = p->d_tile_first;
+  a.tile_owner = p->d_tile_owner;
+  a.cdf_owner = p->d_cdf_owner;
+  a.chunk_owner = p->d_chunk_owner;
   a.cdf_first = p->d_cdf_first;
   a.fin_first = p->d_fin_first;
   a.chunk_first = p->d_chunk_first;
@@ -681,6 +686,16 @@ extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* kn
   }
   p->chunk_first[n_densities] = static_cast<int32_t>(nk);
   p->n_chunks = static_cast<int32_t>(nk);
+  // the density of every tile, CDF scan tile and chunk (one load per item
+  // instead of a search of the first-item tables)
+  auto owners = [&](const std::vector<int32_t>& first, std::vector<int32_t>& out) {
+    out.assign(static_cast<size_t>(first.back()), 0);
+    for (int64_t b = 0; b < n_densities; ++b)
+      for (int32_t i = first[b]; i < first[b + 1]; ++i) out[i] = static_cast<int32_t>(b);
+  };
+  owners(p->tile_first, p->tile_owner);
+  owners(p->cdf_first, p->cdf_owner);
+  owners(p->chunk_first, p->chunk_owner);
   p->total_partials = po;
   const int64_t items_b = nk + n_densities + 2 * static_cast<int64_t>(p->n_lfin);
   p->bwd_grid = static_cast<int>(std::max<int64_t>(1, std::min<int64_t>(items_b, resident_b)));
@@ -742,6 +757,9 @@ extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* kn
   const size_t o_cf = push(p->cdf_first.data(), p->cdf_first.size() * 4);
   const size_t o_ff = push(p->fin_first.data(), p->fin_first.size() * 4);
   const size_t o_kf = push(p->chunk_first.data(), p->chunk_first.size() * 4);
+  const size_t o_to = push(p->tile_owner.data(), p->tile_owner.size() * 4);
+  const size_t o_co = push(p->cdf_owner.data(), p->cdf_owner.size() * 4);
+  const size_t o_ko = push(p->chunk_owner.data(), p->chunk_owner.size() * 4);
   const size_t o_rf = push(p->rowfill_lo.data(), p->rowfill_lo.size() * 4);
   const size_t o_go = push(p->goff.data(), p->goff.size() * 8);
   const size_t o_gb = push(p->gbits.data(), p->gbits.size() * 4);
@@ -764,6 +782,9 @@ extern "C" int loits_batch_plan_create_ex(int64_t n_densities, const int64_t* kn
   p->d_cdf_first = reinterpret_cast<const int32_t*>(d + o_cf);
   p->d_fin_first = reinterpret_cast<const int32_t*>(d + o_ff);
   p->d_chunk_first = reinterpret_cast<const int32_t*>(d + o_kf);
+  p->d_tile_owner = reinterpret_cast<const int32_t*>(d + o_to);
+  p->d_cdf_owner = reinterpret_cast<const int32_t*>(d + o_co);
+  p->d_chunk_owner = reinterpret_cast<const int32_t*>(d + o_ko);
   p->d_rowfill_lo = reinterpret_cast<const int32_t*>(d + o_rf);
   p->d_goff = reinterpret_cast<const int64_t*>(d + o_go);
   p->d_gbits = reinterpret_cast<const int32_t*>(d + o_gb);
