@@ -2518,7 +2518,7 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
     FinShared<TPB> fin;
     SampleShared smp;
   } sh;
-  __shared__ uint32_t s_item;
+  __shared__ uint32_t s_item[2];
   __shared__ int s_guide_key;  // density whose coarse guide guide_s holds
   __shared__ __align__(8) uint64_t s_bar;  // bulk copies of density views
   __shared__ uint32_t s_phase;
@@ -2531,11 +2531,12 @@ __global__ void __launch_bounds__(TPB, 1280 / TPB) batch_backward_kernel(BatchAr
   const BulkStage bulk{&s_bar, &s_phase};
   const int32_t nK = a.k_hi - a.k_lo, nD = a.d_hi - a.d_lo, nL = a.l_hi - a.l_lo;
   const uint32_t n_items = static_cast<uint32_t>(nK + nD + 2 * nL);
-  while (true) {
-    if (threadIdx.x == 0) s_item = atomicAdd(a.ticket, 1u);
+  // two ticket slots used in turn: a slot is written again only after the
+  // next item's barrier, which every thread reaches after reading it
+  for (int par = 0;; par ^= 1) {
+    if (threadIdx.x == 0) s_item[par] = atomicAdd(a.ticket, 1u);
     __syncthreads();
-    const uint32_t item = s_item;
-    __syncthreads();
+    const uint32_t item = s_item[par];
     if (item >= n_items) break;
     if (item < static_cast<uint32_t>(nK)) {
       vjp_chunk_item<TPB, R, kLarge, kFix>(a, a.k_lo + static_cast<int32_t>(item), rec_s, guide_s,
